@@ -1,0 +1,184 @@
+"""ctypes front end of the CPU oracle (psf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of bench.py, never by the photonpy_b200 package.
+
+The FP32 functions restate photonpy's CPU estimator arithmetic
+(cpp/SMLMLib/Estimators/Estimation.h:63-251, SolveMatrix.h:84-452,
+Estimators/Gaussian/GaussianPSFModels.h, Estimators/CSpline/CubicSplinePSFModels.h);
+the FP64 functions are the same algorithm in double precision and serve as the
+"true MLE" yardstick. Parity of the FP32 build with the reference's own C++ CPU
+estimator is pinned by tests/test_oracle.py against tests/golden/*.npz.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD_DIR = os.path.join(HERE, "_build")
+LIB_PATH = os.path.join(BUILD_DIR, "liboracle.so")
+SOURCES = [os.path.join(HERE, "psf_oracle.c"), os.path.join(HERE, "psf_oracle_impl.h")]
+
+XYIBG, XYIBG_CONSTSIGMA, XYIBG_SIGMA, XYIBG_SIGMAXY, XYZIBG, CSPLINE = range(6)
+NUM_PARAMS = {XYIBG: 4, XYIBG_CONSTSIGMA: 4, XYIBG_SIGMA: 5, XYIBG_SIGMAXY: 6, XYZIBG: 5, CSPLINE: 5}
+
+
+class PsoModel(ct.Structure):
+    _fields_ = [
+        ("model", ct.c_int32),
+        ("roisize", ct.c_int32),
+        ("sigma", ct.c_float * 2),
+        ("astig_x", ct.c_float * 5),
+        ("astig_y", ct.c_float * 5),
+        ("minz", ct.c_float),
+        ("maxz", ct.c_float),
+        ("spline_shape", ct.c_int32 * 3),
+        ("spline_zmin", ct.c_float),
+        ("spline_zmax", ct.c_float),
+        ("coefs", ct.c_void_p),
+    ]
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile psf_oracle.c with gcc (no FMA contraction, no fast-math)."""
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    newest = max(os.path.getmtime(s) for s in SOURCES)
+    if not force and os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= newest:
+        return LIB_PATH
+    tmp = LIB_PATH + f".tmp{os.getpid()}"
+    cmd = ["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-std=gnu11",
+           "-o", tmp, SOURCES[0], "-lm", "-lpthread"]
+    subprocess.check_call(cmd)
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = build()
+            L = ct.CDLL(path)
+            fp = ct.POINTER(ct.c_float)
+            ip = ct.POINTER(ct.c_int32)
+            dp = ct.POINTER(ct.c_double)
+            for sfx in ("_f32", "_f64"):
+                f = getattr(L, "pso_fit" + sfx)
+                f.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, ct.c_int, ct.c_double, fp, ip, fp,
+                              ct.c_int, ct.c_int]
+                f = getattr(L, "pso_derivatives" + sfx)
+                f.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, fp]
+                f = getattr(L, "pso_crlb" + sfx)
+                f.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, fp, fp, dp]
+            L.pso_spline_compute.argtypes = [ip, fp, fp, ct.c_int]
+            L.pso_sizeof_model.restype = ct.c_int
+            assert L.pso_sizeof_model() == ct.sizeof(PsoModel), "oracle struct layout mismatch"
+            _lib = L
+    return _lib
+
+
+def _fptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ct.POINTER(ct.c_float))
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Model:
+    """Description of one PSF model instance, mirroring the reference's creation calls."""
+
+    def __init__(self, model: int, roisize: int, sigma=(1.0, 1.0), astig_x=None, astig_y=None, zrange=(0, 0),
+                 coefs=None, spline_zrange=(0, 0)):
+        self.model = model
+        self.roisize = int(roisize)
+        self.K = NUM_PARAMS[model]
+        self.numconst = 2 if model == XYIBG_CONSTSIGMA else 0
+        s = PsoModel()
+        s.model = model
+        s.roisize = self.roisize
+        s.sigma[0], s.sigma[1] = (sigma, sigma) if np.isscalar(sigma) else tuple(sigma)
+        ax = list(astig_x) if astig_x is not None else [1, 0, 1, 0, 0]
+        ay = list(astig_y) if astig_y is not None else [1, 0, 1, 0, 0]
+        ax += [0.0] * (5 - len(ax))
+        ay += [0.0] * (5 - len(ay))
+        for i in range(5):
+            s.astig_x[i] = ax[i]
+            s.astig_y[i] = ay[i]
+        s.minz, s.maxz = zrange
+        self._coefs = None
+        if coefs is not None:
+            self._coefs = np.ascontiguousarray(coefs, dtype=np.float32)
+            nz, ny, nx = self._coefs.shape[:3]
+            s.spline_shape[0], s.spline_shape[1], s.spline_shape[2] = nz, ny, nx
+            s.spline_zmin, s.spline_zmax = spline_zrange
+            s.coefs = self._coefs.ctypes.data
+        self.s = s
+
+    # -- oracle entry points -------------------------------------------------------------
+    def fit(self, samples, constants=None, initial=None, iterations=50, lambda_=1e-18, fp64=False,
+            trace_len=0, nthreads=None):
+        samples = _f32(samples)
+        n = samples.shape[0]
+        constants = _f32(constants)
+        initial = _f32(initial)
+        params = np.zeros((n, self.K), np.float32)
+        its = np.zeros(n, np.int32)
+        trace = np.zeros((n, trace_len, self.K), np.float32) if trace_len > 0 else None
+        f = lib().pso_fit_f64 if fp64 else lib().pso_fit_f32
+        f(ct.byref(self.s), n, _fptr(samples), _fptr(constants), _fptr(initial), int(iterations),
+          float(lambda_), _fptr(params), its.ctypes.data_as(ct.POINTER(ct.c_int32)), _fptr(trace),
+          int(trace_len), int(nthreads or os.cpu_count() or 1))
+        if trace_len > 0:
+            return params, its, trace
+        return params, its
+
+    def derivatives(self, params, constants=None, fp64=False):
+        params = _f32(params)
+        n = params.shape[0]
+        npix = self.roisize * self.roisize
+        ev = np.zeros((n, self.roisize, self.roisize), np.float32)
+        deriv = np.zeros((n, self.K, self.roisize, self.roisize), np.float32)
+        f = lib().pso_derivatives_f64 if fp64 else lib().pso_derivatives_f32
+        f(ct.byref(self.s), n, _fptr(params), _fptr(_f32(constants)), _fptr(deriv), _fptr(ev))
+        del npix
+        return deriv, ev
+
+    def expected_value(self, params, constants=None, fp64=False):
+        return self.derivatives(params, constants, fp64)[1]
+
+    def crlb(self, params, samples=None, constants=None, fp64=False, return_fisher=False):
+        params = _f32(params)
+        n = params.shape[0]
+        crlb = np.zeros((n, self.K), np.float32)
+        chisq = np.zeros(n, np.float32)
+        fisher = np.zeros((n, self.K, self.K), np.float64) if return_fisher else None
+        f = lib().pso_crlb_f64 if fp64 else lib().pso_crlb_f32
+        f(ct.byref(self.s), n, _fptr(params), _fptr(_f32(samples)), _fptr(_f32(constants)), _fptr(crlb),
+          _fptr(chisq), None if fisher is None else fisher.ctypes.data_as(ct.POINTER(ct.c_double)))
+        if return_fisher:
+            return crlb, chisq, fisher
+        return crlb, chisq
+
+
+def spline_compute(data, border=0):
+    """CSpline_Compute restated (double LUP solve per voxel)."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    shape = np.ascontiguousarray(data.shape, dtype=np.int32)
+    out = np.zeros((*(np.array(data.shape) - 3 + 2 * border), 64), np.float32)
+    rc = lib().pso_spline_compute(shape.ctypes.data_as(ct.POINTER(ct.c_int32)), _fptr(data), _fptr(out),
+                                  int(border))
+    if rc != 0:
+        raise RuntimeError("spline basis matrix is singular")
+    return out

@@ -1,0 +1,152 @@
+/* CPU oracle for the batched Poisson-MLE PSF estimator.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is a plain-C restatement of photonpy's
+ * estimator arithmetic (cpp/SMLMLib/Estimators/Estimation.h, SolveMatrix.h,
+ * Estimators/Gaussian/GaussianPSFModels.h, Estimators/CSpline/CubicSplinePSFModels.h,
+ * Estimators/CSpline/CubicSplinePSF.cu). It exists so that tests/, the smoke
+ * check and bench.py's CPU-baseline leg can check the CUDA product against the
+ * reference's algorithm. The product (photonpy_b200) never links or calls it.
+ *
+ * Parity pin: tests/test_oracle.py checks the FP32 build of this file against
+ * golden vectors produced by the reference's own C++ CPU estimator
+ * (tests/golden/make_golden.py, built by oracle/build_ref.sh).
+ *
+ * Build: gcc -O2 -fPIC -shared -ffp-contract=off (no FMA contraction, like the
+ * reference's host -O3 build on x86-64 without -march=native).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PSO_MAXK 6
+
+enum {
+    PSO_XYIBG = 0,            /* Gauss2D_Model_XYIBg            (GaussianPSFModels.h:35-152)  */
+    PSO_XYIBG_CONSTSIGMA = 1, /* Gauss2D_Model_XYIBgConstSigma  (GaussianPSFModels.h:156-227) */
+    PSO_XYIBG_SIGMA = 2,      /* Gauss2D_Model_XYIBgSigma       (GaussianPSFModels.h:308-387) */
+    PSO_XYIBG_SIGMAXY = 3,    /* Gauss2D_Model_XYIBgSigmaXY     (GaussianPSFModels.h:391-471) */
+    PSO_XYZIBG = 4,           /* Gauss2D_Model_XYZIBg (astig)   (GaussianPSFModels.h:636-751) */
+    PSO_CSPLINE = 5           /* CSpline_Model_XYZIBg           (CubicSplinePSFModels.h:14-154) */
+};
+
+typedef struct {
+    int model;
+    int roisize;
+    float sigma[2];         /* fixed sigma (XYIBg) or initial sigma(s) (Sigma, SigmaXY)        */
+    float astig_x[5];       /* s0, gamma, d, A, B   (B = 0 is the reference's 4-term form)    */
+    float astig_y[5];
+    float minz, maxz;
+    int spline_shape[3];    /* coefficient grid (z, y, x)                                      */
+    float spline_zmin, spline_zmax;
+    const float* coefs;     /* [Nz][Ny][Nx][64]                                                */
+} pso_model_t;
+
+int pso_num_params(int model)
+{
+    switch (model) {
+    case PSO_XYIBG: case PSO_XYIBG_CONSTSIGMA: return 4;
+    case PSO_XYIBG_SIGMAXY: return 6;
+    default: return 5;
+    }
+}
+
+int pso_num_constants(int model) { return model == PSO_XYIBG_CONSTSIGMA ? 2 : 0; }
+
+int pso_sizeof_model(void) { return (int)sizeof(pso_model_t); }
+
+/* ---- FP32: the reference's arithmetic ---- */
+#define REAL float
+#define SUFFIX _f32
+#define ERF erff
+#define EXP expf
+#define SQRT sqrtf
+#define FMAX fmaxf
+#define FMIN fminf
+#define FABS fabsf
+#include "psf_oracle_impl.h"
+#undef REAL
+#undef SUFFIX
+#undef ERF
+#undef EXP
+#undef SQRT
+#undef FMAX
+#undef FMIN
+#undef FABS
+
+/* ---- FP64 oracle ---- */
+#define REAL double
+#define SUFFIX _f64
+#define ERF erf
+#define EXP exp
+#define SQRT sqrt
+#define FMAX fmax
+#define FMIN fmin
+#define FABS fabs
+#include "psf_oracle_impl.h"
+
+/* CSpline_Compute (CubicSplinePSF.cu:151-204): per output voxel, the 4x4x4 neighbourhood
+ * (clamped at the border) is solved against the 64x64 power-basis matrix with a double
+ * LUP decomposition. Output shape = shape - 3 + 2*border, 64 coefficients per voxel,
+ * coefficient index = zpow*16 + ypow*4 + xpow. */
+int pso_spline_compute(const int* shape, const float* data, float* coefs, int border)
+{
+    static double A[64 * 64];
+    int P[65];
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            for (int k = 0; k < 4; k++)
+                for (int l = 0; l < 4; l++)
+                    for (int m = 0; m < 4; m++)
+                        for (int n = 0; n < 4; n++)
+                            A[64 * (i * 16 + j * 4 + k) + (l * 16 + m * 4 + n)] =
+                                (double)(powf((float)(i - 1.0), (float)l) * powf((float)(j - 1.0), (float)m) *
+                                         powf((float)(k - 1.0), (float)n));
+    const int N = 64;
+    for (int i = 0; i <= N; i++) P[i] = i;
+    for (int i = 0; i < N; i++) {
+        double maxA = 0, absA;
+        int imax = i;
+        for (int k = i; k < N; k++)
+            if ((absA = fabs(A[k * N + i])) > maxA) { maxA = absA; imax = k; }
+        if (maxA < (double)1e-10f) return -1;
+        if (imax != i) {
+            int j = P[i]; P[i] = P[imax]; P[imax] = j;
+            for (int jj = 0; jj < N; jj++) {
+                double t = A[i * N + jj]; A[i * N + jj] = A[imax * N + jj]; A[imax * N + jj] = t;
+            }
+            P[N]++;
+        }
+        for (int j = i + 1; j < N; j++) {
+            A[j * N + i] /= A[i * N + i];
+            for (int k = i + 1; k < N; k++) A[j * N + k] -= A[j * N + i] * A[i * N + k];
+        }
+    }
+    const int o0 = shape[0] - 3 + border * 2, o1 = shape[1] - 3 + border * 2, o2 = shape[2] - 3 + border * 2;
+    for (int i = 0; i < o0; i++)
+        for (int j = 0; j < o1; j++)
+            for (int k = 0; k < o2; k++) {
+                double b[64], x[64];
+                for (int m = 0; m < 4; m++)
+                    for (int n = 0; n < 4; n++)
+                        for (int o = 0; o < 4; o++) {
+                            int z = i + m - border, y = j + n - border, xx = k + o - border;
+                            z = z < 0 ? 0 : (z > shape[0] - 1 ? shape[0] - 1 : z);
+                            y = y < 0 ? 0 : (y > shape[1] - 1 ? shape[1] - 1 : y);
+                            xx = xx < 0 ? 0 : (xx > shape[2] - 1 ? shape[2] - 1 : xx);
+                            b[m * 16 + n * 4 + o] = data[(size_t)shape[1] * shape[2] * z + (size_t)shape[2] * y + xx];
+                        }
+                for (int r = 0; r < N; r++) {
+                    x[r] = b[P[r]];
+                    for (int q = 0; q < r; q++) x[r] -= A[r * N + q] * x[q];
+                }
+                for (int r = N - 1; r >= 0; r--) {
+                    for (int q = r + 1; q < N; q++) x[r] -= A[r * N + q] * x[q];
+                    x[r] = x[r] / A[r * N + r];
+                }
+                float* dst = coefs + 64 * ((size_t)o1 * o2 * i + (size_t)o2 * j + k);
+                for (int a = 0; a < 64; a++) dst[a] = (float)x[a];
+            }
+    return 0;
+}

@@ -1,0 +1,190 @@
+"""Minimal ctypes binding of the reference photonpy library built by oracle/build_ref.sh.
+
+TEST INFRASTRUCTURE ONLY: used to generate golden vectors, by parity tests when the
+reference build is present, and by bench.py's reference (CPU baseline) arm. It calls
+the reference's unmodified C ABI (cpp/SMLMLib/Estimators/Estimator.h:157-171,
+Estimators/Gaussian/GaussianPSF.h:35-41, Estimators/CSpline/CubicSplinePSF.h:33-40) the
+same way photonpy/cpp/estimator.py does; all arithmetic happens inside the reference.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libphotonpy_ref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+class Gauss3DCalib(ct.Structure):
+    _fields_ = [("x", ct.c_float * 4), ("y", ct.c_float * 4), ("zrange", ct.c_float * 2)]
+
+
+class CSplineCalib(ct.Structure):
+    _fields_ = [("shape", ct.c_int32 * 3), ("z_min", ct.c_float), ("z_max", ct.c_float), ("coefs", ct.c_void_p)]
+
+
+class Props(ct.Structure):
+    _fields_ = [("numParams", ct.c_int), ("sampleCount", ct.c_int), ("numDiag", ct.c_int), ("numConst", ct.c_int),
+                ("sampleIndexDims", ct.c_int)]
+
+
+class LMParams(ct.Structure):
+    _fields_ = [("iterations", ct.c_int32), ("lambda_", ct.c_float), ("factor", ct.c_float)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{REF_LIB} not built (run oracle/build_ref.sh)")
+        L = ct.CDLL(REF_LIB)
+        vp = ct.c_void_p
+        L.Context_Create.restype = vp
+        L.Context_Destroy.argtypes = [vp]
+        for name, args in [
+            ("Gauss2D_CreatePSF_XYIBg", [ct.c_int, ct.c_float, ct.c_float, ct.c_bool, vp]),
+            ("Gauss2D_CreatePSF_XYIBgConstSigma", [ct.c_int, ct.c_bool, vp]),
+            ("Gauss2D_CreatePSF_XYIBgSigma", [ct.c_int, ct.c_float, ct.c_bool, vp]),
+            ("Gauss2D_CreatePSF_XYIBgSigmaXY", [ct.c_int, ct.c_float, ct.c_float, ct.c_bool, vp]),
+            ("Gauss2D_CreatePSF_XYZIBg", [ct.c_int, ct.POINTER(Gauss3DCalib), ct.c_bool, vp]),
+            ("CSpline_CreatePSF", [ct.c_int, ct.POINTER(CSplineCalib), vp, ct.c_int, ct.c_bool, vp]),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = vp
+        L.Estimator_Delete.argtypes = [vp]
+        L.Estimator_GetProperties.argtypes = [vp, ct.POINTER(Props)]
+        L.Estimator_SetLMParams.argtypes = [vp, ct.POINTER(LMParams)]
+        L.Estimator_Estimate.argtypes = [vp, ct.c_int, vp, vp, vp, vp, vp, vp, vp, vp, ct.c_int]
+        L.Estimator_ChiSquareAndCRLB.argtypes = [vp, vp, vp, vp, vp, ct.c_int, vp, vp]
+        L.Estimator_ComputeDerivatives.argtypes = [vp, ct.c_int, vp, vp, vp, vp, vp]
+        L.Estimator_ComputeExpectedValue.argtypes = [vp, ct.c_int, vp, vp, vp, vp]
+        L.CSpline_Compute.argtypes = [vp, vp, vp, ct.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class RefEstimator:
+    """One reference estimator instance (host pointers; cuda selects the reference's GPU kernels)."""
+
+    def __init__(self, kind: str, roisize: int, cuda: bool = False, sigma=(1.5, 1.5), astig=None, zrange=(-1, 1),
+                 coefs=None, spline_zrange=(0, 1)):
+        L = lib()
+        self.ctx = L.Context_Create()
+        self.roisize = roisize
+        if kind == "XYIBg":
+            inst = L.Gauss2D_CreatePSF_XYIBg(roisize, sigma[0], sigma[1], cuda, self.ctx)
+        elif kind == "XYIBgConstSigma":
+            inst = L.Gauss2D_CreatePSF_XYIBgConstSigma(roisize, cuda, self.ctx)
+        elif kind == "XYIBgSigma":
+            inst = L.Gauss2D_CreatePSF_XYIBgSigma(roisize, sigma[0], cuda, self.ctx)
+        elif kind == "XYIBgSigmaXY":
+            inst = L.Gauss2D_CreatePSF_XYIBgSigmaXY(roisize, sigma[0], sigma[1], cuda, self.ctx)
+        elif kind == "XYZIBg":
+            c = Gauss3DCalib()
+            for i in range(4):
+                c.x[i] = astig[0][i]
+                c.y[i] = astig[1][i]
+            c.zrange[0], c.zrange[1] = zrange
+            inst = L.Gauss2D_CreatePSF_XYZIBg(roisize, ct.byref(c), cuda, self.ctx)
+        elif kind == "CSpline":
+            self._coefs = np.ascontiguousarray(coefs, dtype=np.float32)
+            c = CSplineCalib()
+            c.shape[0], c.shape[1], c.shape[2] = self._coefs.shape[:3]
+            c.z_min, c.z_max = spline_zrange
+            c.coefs = self._coefs.ctypes.data
+            inst = L.CSpline_CreatePSF(roisize, ct.byref(c), None, 0, cuda, self.ctx)
+        else:
+            raise ValueError(kind)
+        if not inst:
+            raise RuntimeError(f"reference failed to create {kind}")
+        self.inst = inst
+        p = Props()
+        L.Estimator_GetProperties(inst, ct.byref(p))
+        self.K, self.numconst, self.numdiag = p.numParams, p.numConst, p.numDiag
+        self.set_lm(50, 1e-18)
+
+    def set_lm(self, iterations, lambda_):
+        lmp = LMParams()
+        lmp.iterations, lmp.lambda_, lmp.factor = iterations, lambda_, 0
+        self.iterations = iterations
+        lib().Estimator_SetLMParams(self.inst, ct.byref(lmp))
+
+    def estimate(self, samples, constants=None, initial=None, trace_len=None):
+        L = lib()
+        samples = np.ascontiguousarray(samples, dtype=np.float32)
+        n = samples.shape[0]
+        tl = self.iterations if trace_len is None else trace_len
+        params = np.zeros((n, self.K), np.float32)
+        its = np.zeros(n, np.int32)
+        diag = np.zeros((n, max(self.numdiag, 1)), np.float32)
+        trace = np.zeros((n, max(tl, 1), self.K), np.float32)
+        const = np.ascontiguousarray(constants if constants is not None else np.zeros((n, self.numconst)),
+                                     dtype=np.float32)
+        roipos = np.zeros((n, 2), np.int32)
+        init = None if initial is None else np.ascontiguousarray(initial, dtype=np.float32)
+        L.Estimator_Estimate(self.inst, n, _p(samples), _p(const), _p(roipos), _p(init), _p(params), _p(diag),
+                             _p(its), _p(trace), tl)
+        return params, its, trace
+
+    def crlb_chisq(self, params, samples=None, constants=None):
+        L = lib()
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        n = params.shape[0]
+        crlb = np.zeros((n, self.K), np.float32)
+        chisq = np.zeros(n, np.float32)
+        const = np.ascontiguousarray(constants if constants is not None else np.zeros((n, self.numconst)),
+                                     dtype=np.float32)
+        roipos = np.zeros((n, 2), np.int32)
+        smp = None if samples is None else np.ascontiguousarray(samples, dtype=np.float32)
+        L.Estimator_ChiSquareAndCRLB(self.inst, _p(params), _p(smp), _p(const), _p(roipos), n, _p(crlb),
+                                     _p(chisq))
+        return crlb, chisq
+
+    def derivatives(self, params, constants=None):
+        L = lib()
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        n = params.shape[0]
+        R = self.roisize
+        ev = np.zeros((n, R, R), np.float32)
+        deriv = np.zeros((n, self.K, R, R), np.float32)
+        const = np.ascontiguousarray(constants if constants is not None else np.zeros((n, self.numconst)),
+                                     dtype=np.float32)
+        roipos = np.zeros((n, 2), np.int32)
+        L.Estimator_ComputeDerivatives(self.inst, n, _p(params), _p(const), _p(roipos), _p(deriv), _p(ev))
+        return deriv, ev
+
+    def close(self):
+        if self.inst:
+            lib().Estimator_Delete(self.inst)
+            self.inst = None
+        if self.ctx:
+            lib().Context_Destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spline_compute(data, border=0):
+    L = lib()
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    shape = np.ascontiguousarray(data.shape, dtype=np.int32)
+    out = np.zeros((*(np.array(data.shape) - 3 + 2 * border), 64), np.float32)
+    L.CSpline_Compute(_p(shape), _p(data), _p(out), int(border))
+    return out

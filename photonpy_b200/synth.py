@@ -1,0 +1,218 @@
+"""Seeded synthetic ROI batches for tests and benchmarks.
+
+Ground truth is drawn with ``numpy.random.default_rng(seed)``, the pixel
+expectation is evaluated in FP64 from the pixel-integrated (erf-difference)
+Gaussian PSF that photonpy's models describe (GaussianPSFModels.h:63-98), and
+observed pixels are Poisson draws stored as float32. The same arrays feed the
+CUDA estimator, the reference's CPU estimator and the oracle.
+
+Workloads (distributions as stated in each generator):
+  * ``xyibg``      10x10, sigma 1.5 fixed, x,y~U[4,6], I~U[500,5000], bg~U[2,10]
+  * ``sigmaxy``    16x16 free sigma_x/sigma_y, x,y~U[6.5,8.5], sigma~U[1.2,2.2],
+                   I log-uniform [200,20000], bg~U[1,20], initial sigma 1.7
+  * ``astig``      12x12 astigmatic 3D, z~U[-400,400] nm, s0 1.3 px, c 150 nm,
+                   d 400 nm, A 0.1 (and optional B), I log-uniform [500,1e4], bg~U[2,15]
+  * ``spline``     13x13 cubic-spline PSF built from a z-stack of the astig model
+                   (z in micrometres), z~U[-0.38,0.38] um
+  * ``mixed``      sizes {7,9,11,16} p={.2,.3,.3,.2}; 50% XYIBg, 30% SigmaXY, 20% astig;
+                   x,y re-centred at (R-1)/2 +- 1 px
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+from scipy.special import erf
+
+SQRT2 = math.sqrt(2.0)
+
+
+def _delta(pix, centre, sigma):
+    """Pixel-integrated 1D Gaussian, shape [n, R] (FP64)."""
+    s = SQRT2 * sigma[:, None]
+    a = (pix[None, :] - centre[:, None] + 0.5) / s
+    b = (pix[None, :] - centre[:, None] - 0.5) / s
+    return 0.5 * erf(a) - 0.5 * erf(b)
+
+
+def gauss2d_ev(R, x, y, I, bg, sx, sy):
+    """Expected pixel values [n, R, R] of bg + I * DeltaX * DeltaY (FP64)."""
+    pix = np.arange(R, dtype=np.float64)
+    dx = _delta(pix, np.asarray(x, np.float64), np.asarray(sx, np.float64))
+    dy = _delta(pix, np.asarray(y, np.float64), np.asarray(sy, np.float64))
+    return np.asarray(bg)[:, None, None] + np.asarray(I)[:, None, None] * dy[:, :, None] * dx[:, None, :]
+
+
+def astig_sigma(z, s0, gamma, d, A, B=0.0):
+    """sigma(z) = s0*sqrt(1 + tz^2/d^2 + A*tz^3/d^2 + B*tz^4/d^4), tz = z - gamma (the
+    reference's 4-coefficient form, GaussianPSFModels.h:698-702, plus an optional B term)."""
+    tz = np.asarray(z, np.float64) - gamma
+    return s0 * np.sqrt(1 + tz ** 2 / d ** 2 + A * tz ** 3 / d ** 2 + B * tz ** 4 / d ** 4)
+
+
+def astig_calib_nm(A=0.1, B=0.0, s0=1.3, c=150.0, d=400.0, zrange=(-600.0, 600.0)):
+    """Config-3 calibration expressed in the reference's coefficients (z in nm).
+
+    The workload writes sigma = s0*sqrt(1 + t^2 + A t^3 + B t^4) with t = (z -+ c)/d.
+    In the reference's form A multiplies tz^3/d^2, hence A_ref = A/d.
+    Returns (x[5], y[5], zrange) with (s0, gamma, d, A_ref, B)."""
+    x = [s0, c, d, A / d, B]
+    y = [s0, -c, d, A / d, B]
+    return x, y, tuple(zrange)
+
+
+def _poisson(rng, ev, chunk=1 << 22):
+    out = np.empty(ev.shape, np.float32)
+    flat_in = ev.reshape(-1)
+    flat_out = out.reshape(-1)
+    for s in range(0, flat_in.size, chunk):
+        flat_out[s:s + chunk] = rng.poisson(flat_in[s:s + chunk])
+    return out
+
+
+def _gen_chunks(n, chunk, fn):
+    parts = [fn(s, min(n, s + chunk)) for s in range(0, n, chunk)]
+    return np.concatenate(parts, axis=0) if parts else None
+
+
+def xyibg(n, seed=1, R=10, sigma=1.5, xy=(4.0, 6.0)):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(*xy, n)
+    y = rng.uniform(*xy, n)
+    I = rng.uniform(500, 5000, n)
+    bg = rng.uniform(2, 10, n)
+    truth = np.stack([x, y, I, bg], 1).astype(np.float32)
+    s = np.full(n, sigma)
+    smp = _gen_chunks(n, 65536, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
+                                                                     s[a:b], s[a:b])))
+    return dict(kind="XYIBg", R=R, sigma=(sigma, sigma), samples=smp, truth=truth)
+
+
+def constsigma(n, seed=11, R=9, sig=(1.2, 1.8)):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform((R - 1) / 2 - 1, (R - 1) / 2 + 1, n)
+    y = rng.uniform((R - 1) / 2 - 1, (R - 1) / 2 + 1, n)
+    I = rng.uniform(500, 5000, n)
+    bg = rng.uniform(2, 10, n)
+    sx = rng.uniform(*sig, n)
+    sy = rng.uniform(*sig, n)
+    truth = np.stack([x, y, I, bg], 1).astype(np.float32)
+    consts = np.stack([sx, sy], 1).astype(np.float32)
+    smp = _poisson(rng, gauss2d_ev(R, x, y, I, bg, sx, sy))
+    return dict(kind="XYIBgConstSigma", R=R, samples=smp, truth=truth, constants=consts)
+
+
+def sigma1(n, seed=12, R=11, init_sigma=1.5):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform((R - 1) / 2 - 1, (R - 1) / 2 + 1, n)
+    y = rng.uniform((R - 1) / 2 - 1, (R - 1) / 2 + 1, n)
+    I = rng.uniform(500, 5000, n)
+    bg = rng.uniform(2, 10, n)
+    s = rng.uniform(1.2, 2.0, n)
+    truth = np.stack([x, y, I, bg, s], 1).astype(np.float32)
+    smp = _poisson(rng, gauss2d_ev(R, x, y, I, bg, s, s))
+    return dict(kind="XYIBgSigma", R=R, sigma=(init_sigma, init_sigma), samples=smp, truth=truth)
+
+
+def sigmaxy(n, seed=2, R=16, init_sigma=1.7, xy=(6.5, 8.5)):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(*xy, n)
+    y = rng.uniform(*xy, n)
+    sx = rng.uniform(1.2, 2.2, n)
+    sy = rng.uniform(1.2, 2.2, n)
+    I = np.exp(rng.uniform(math.log(200), math.log(20000), n))
+    bg = rng.uniform(1, 20, n)
+    truth = np.stack([x, y, I, bg, sx, sy], 1).astype(np.float32)
+    smp = _gen_chunks(n, 32768, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
+                                                                     sx[a:b], sy[a:b])))
+    return dict(kind="XYIBgSigmaXY", R=R, sigma=(init_sigma, init_sigma), samples=smp, truth=truth)
+
+
+def astig(n, seed=3, R=12, A=0.1, B=0.0, zr=(-400.0, 400.0), xy=None, zrange=(-600.0, 600.0)):
+    rng = np.random.default_rng(seed)
+    cx, cy, zrange = astig_calib_nm(A=A, B=B, zrange=zrange)
+    lo, hi = xy if xy is not None else ((R - 1) / 2 - 1, (R - 1) / 2 + 1)
+    x = rng.uniform(lo, hi, n)
+    y = rng.uniform(lo, hi, n)
+    z = rng.uniform(*zr, n)
+    I = np.exp(rng.uniform(math.log(500), math.log(1e4), n))
+    bg = rng.uniform(2, 15, n)
+    sx = astig_sigma(z, *cx)
+    sy = astig_sigma(z, *cy)
+    truth = np.stack([x, y, z, I, bg], 1).astype(np.float32)
+    smp = _gen_chunks(n, 65536, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
+                                                                     sx[a:b], sy[a:b])))
+    return dict(kind="XYZIBg", R=R, astig=(cx, cy), zrange=zrange, samples=smp, truth=truth)
+
+
+def astig_zstack(shape_xy=26, nz=41, zrange_um=(-0.4, 0.4), A=0.1, B=0.0, step_px=1.0):
+    """Z-stack [nz, Y, X] of the astig model (z in micrometres), centred at (X-1)/2 in
+    units of the output grid, each slice normalised to sum 1 (in ROI pixel units)."""
+    cx, cy, _ = astig_calib_nm(A=A, B=B)
+    cx = [cx[0], cx[1] * 1e-3, cx[2] * 1e-3, cx[3] * 1e3, cx[4]]
+    cy = [cy[0], cy[1] * 1e-3, cy[2] * 1e-3, cy[3] * 1e3, cy[4]]
+    zs = np.linspace(zrange_um[0], zrange_um[1], nz)
+    X = shape_xy
+    # Grid point g sits at ROI-pixel offset (g - (X-1)/2) * step_px from the PSF centre.
+    offs = (np.arange(X) - (X - 1) / 2) * step_px
+    out = np.zeros((nz, X, X), np.float64)
+    for k, z in enumerate(zs):
+        sx = astig_sigma(z, *cx)
+        sy = astig_sigma(z, *cy)
+        # pixel-integrated over one ROI pixel centred at each grid offset
+        dx = 0.5 * erf((offs + 0.5) / (SQRT2 * sx)) - 0.5 * erf((offs - 0.5) / (SQRT2 * sx))
+        dy = 0.5 * erf((offs + 0.5) / (SQRT2 * sy)) - 0.5 * erf((offs - 0.5) / (SQRT2 * sy))
+        sl = dy[:, None] * dx[None, :]
+        out[k] = sl / sl.sum() * (step_px ** 2 if step_px != 1.0 else 1.0)
+    return out.astype(np.float32), (float(zs[0]), float(zs[-1]))
+
+
+def spline(n, seed=4, R=13, zr=(-0.38, 0.38), A=0.1, B=0.0):
+    """ROIs drawn from the astig model with z in micrometres (the PSF the spline calibrates)."""
+    rng = np.random.default_rng(seed)
+    cx, cy, _ = astig_calib_nm(A=A, B=B)
+    cx = [cx[0], cx[1] * 1e-3, cx[2] * 1e-3, cx[3] * 1e3, cx[4]]
+    cy = [cy[0], cy[1] * 1e-3, cy[2] * 1e-3, cy[3] * 1e3, cy[4]]
+    x = rng.uniform((R - 1) / 2 - 1, (R - 1) / 2 + 1, n)
+    y = rng.uniform((R - 1) / 2 - 1, (R - 1) / 2 + 1, n)
+    z = rng.uniform(*zr, n)
+    I = np.exp(rng.uniform(math.log(500), math.log(1e4), n))
+    bg = rng.uniform(2, 15, n)
+    sx = astig_sigma(z, *cx)
+    sy = astig_sigma(z, *cy)
+    truth = np.stack([x, y, z, I, bg], 1).astype(np.float32)
+    smp = _gen_chunks(n, 65536, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
+                                                                     sx[a:b], sy[a:b])))
+    return dict(kind="CSpline", R=R, samples=smp, truth=truth)
+
+
+MIXED_SIZES = (7, 9, 11, 16)
+MIXED_SIZE_P = (0.2, 0.3, 0.3, 0.2)
+MIXED_MODELS = ("XYIBg", "XYIBgSigmaXY", "XYZIBg")
+MIXED_MODEL_P = (0.5, 0.3, 0.2)
+
+
+def mixed(n, seed=5):
+    """Mixed-size, mixed-model batch. Returns a list of groups, one per (model, size):
+    dict(kind, R, index (positions in the mixed order), samples, truth, ...)."""
+    rng = np.random.default_rng(seed)
+    size_idx = rng.choice(len(MIXED_SIZES), n, p=MIXED_SIZE_P)
+    model_idx = rng.choice(len(MIXED_MODELS), n, p=MIXED_MODEL_P)
+    groups = []
+    sub_seed = seed * 1000
+    for mi, kind in enumerate(MIXED_MODELS):
+        for si, R in enumerate(MIXED_SIZES):
+            sel = np.nonzero((model_idx == mi) & (size_idx == si))[0]
+            if sel.size == 0:
+                continue
+            sub_seed += 1
+            xy = ((R - 1) / 2 - 1, (R - 1) / 2 + 1)
+            if kind == "XYIBg":
+                g = xyibg(sel.size, seed=sub_seed, R=R, xy=xy)
+            elif kind == "XYIBgSigmaXY":
+                g = sigmaxy(sel.size, seed=sub_seed, R=R, xy=xy)
+            else:
+                g = astig(sel.size, seed=sub_seed, R=R, xy=xy)
+            g["index"] = sel
+            groups.append(g)
+    return groups

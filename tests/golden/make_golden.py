@@ -1,0 +1,88 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own CPU estimator.
+
+Run in a container that has the reference sources (the GPU box does not):
+    oracle/build_ref.sh            # builds oracle/_ref/libphotonpy_ref.so from the reference
+    python tests/golden/make_golden.py
+
+Inputs are seeded synthetic ROIs (photonpy_b200.synth). Every output array is what the
+reference's C ABI (Estimator_Estimate, Estimator_ChiSquareAndCRLB,
+Estimator_ComputeDerivatives, CSpline_Compute; cuda=False) returned for them, with the
+Python API's default LM settings (lambda 1e-18, 50 iterations; estimator.py:151).
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ref_lib  # noqa: E402
+from photonpy_b200 import synth  # noqa: E402
+
+N_TRACE = 40
+N_DERIV = 16
+
+
+def _fit_and_save(name, est, data, constants=None, extra=None):
+    smp = data["samples"]
+    params, its, trace = est.estimate(smp, constants=constants, trace_len=50)
+    crlb, chisq = est.crlb_chisq(params, smp, constants=constants)
+    crlb_truth, _ = est.crlb_chisq(data["truth"], None, constants=constants)
+    deriv, ev = est.derivatives(data["truth"][:N_DERIV], constants=None if constants is None else constants[:N_DERIV])
+    out = dict(samples=smp, truth=data["truth"], params=params, iterations=its, trace=trace[:N_TRACE],
+               crlb=crlb, chisq=chisq, crlb_truth=crlb_truth, deriv=deriv, ev=ev, roisize=np.int32(data["R"]))
+    if constants is not None:
+        out["constants"] = constants
+    out.update(extra or {})
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    capped = float(np.mean(its > 50))
+    print(f"{name}: n={len(smp)} mean it={its.mean():.2f} capped={capped:.3f}")
+
+
+def main():
+    if not ref_lib.available():
+        raise SystemExit("build the reference first: oracle/build_ref.sh")
+
+    d = synth.xyibg(400, seed=101)
+    e = ref_lib.RefEstimator("XYIBg", d["R"], sigma=d["sigma"])
+    _fit_and_save("xyibg_r10", e, d, extra=dict(sigma=np.float32(d["sigma"])))
+
+    d = synth.constsigma(300, seed=111)
+    e = ref_lib.RefEstimator("XYIBgConstSigma", d["R"])
+    _fit_and_save("constsigma_r9", e, d, constants=d["constants"])
+
+    d = synth.sigma1(300, seed=112)
+    e = ref_lib.RefEstimator("XYIBgSigma", d["R"], sigma=d["sigma"])
+    _fit_and_save("sigma_r11", e, d, extra=dict(sigma=np.float32(d["sigma"])))
+
+    d = synth.sigmaxy(400, seed=102)
+    e = ref_lib.RefEstimator("XYIBgSigmaXY", d["R"], sigma=d["sigma"])
+    _fit_and_save("sigmaxy_r16", e, d, extra=dict(sigma=np.float32(d["sigma"])))
+
+    d = synth.astig(400, seed=103)
+    cx, cy = d["astig"]
+    zr = d["zrange"]
+    e = ref_lib.RefEstimator("XYZIBg", d["R"], astig=(cx[:4], cy[:4]), zrange=zr)
+    _fit_and_save("astig_r12", e, d, extra=dict(astig_x=np.float32(cx), astig_y=np.float32(cy),
+                                                zrange=np.float32(zr)))
+
+    # Cubic spline: z-stack of the astig model (z in um), coefficients by the reference's
+    # CSpline_Compute with border 1 (one voxel per ROI pixel, one spline segment per z step).
+    zstack, zr = synth.astig_zstack(shape_xy=24, nz=21, zrange_um=(-0.4, 0.4))
+    coefs = ref_lib.spline_compute(zstack, border=1)
+    rng = np.random.default_rng(7)
+    pick = rng.choice(coefs.size, 4096, replace=False)
+    d = synth.spline(300, seed=104)
+    e = ref_lib.RefEstimator("CSpline", d["R"], coefs=coefs, spline_zrange=zr)
+    _fit_and_save("spline_r13", e, d, extra=dict(
+        zstack=zstack, spline_zrange=np.float32(zr), coefs_sha256=np.bytes_(hashlib.sha256(coefs.tobytes()).hexdigest()),
+        coefs_shape=np.int32(coefs.shape), coefs_pick=pick.astype(np.int64), coefs_pick_values=coefs.reshape(-1)[pick]))
+
+
+if __name__ == "__main__":
+    main()
