@@ -1,0 +1,181 @@
+/* photonpy_b200 — C ABI of the B200 (sm_100a) batched Poisson-MLE PSF estimator.
+ *
+ * Drop-in for photonpy's estimator ABI: every function below that carries a
+ * reference citation has the same name, argument order, argument meaning and
+ * error behaviour as the photonpy export it replaces, so photonpy's ctypes
+ * bindings (photonpy/cpp/estimator.py, gaussian.py, cspline.py, context.py) can
+ * bind libphotonpy_b200.so unchanged. Unless stated otherwise all pointers are
+ * HOST memory and the caller allocates every output. Errors never propagate as
+ * C++ exceptions: like the reference, functions return void (factories return
+ * NULL) and report through the debug-print callback; in addition the message is
+ * kept for PB200_GetLastError().
+ *
+ * Citations are paths inside photonpy's cpp/SMLMLib.
+ */
+#ifndef PHOTONPY_B200_H
+#define PHOTONPY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#else
+#include <stdbool.h>
+#endif
+
+typedef struct Estimator Estimator; /* opaque */
+typedef struct Context Context;     /* opaque */
+
+/* LMParams, Estimators/Estimator.h:18-26. `factor` is accepted and unused, as in the reference. */
+typedef struct LMParams {
+    int iterations;
+    float lambda;
+    float factor;
+} LMParams;
+
+/* ParamLimit, Estimators/Estimator.h:28-31. */
+typedef struct ParamLimit {
+    float min, max;
+} ParamLimit;
+
+/* EstimatorProperties, Estimators/Estimator.h:151-154. */
+typedef struct EstimatorProperties {
+    int numParams, sampleCount, numDiag, numConst, sampleIndexDims;
+} EstimatorProperties;
+
+/* Gauss3D_Calibration, Estimators/Gaussian/GaussianPSF.h:27-33:
+ * sigma(z) = s0*sqrt(1 + tz^2/d^2 + A*tz^3/d^2), tz = z - gamma; x/y = {s0, gamma, d, A}. */
+typedef struct Gauss3D_Calibration {
+    float x[4];
+    float y[4];
+    float minz, maxz;
+} Gauss3D_Calibration;
+
+/* Extension (no reference counterpart): astigmatic calibration with a quartic term,
+ * x/y = {s0, gamma, d, A, B}: sigma(z) = s0*sqrt(1 + tz^2/d^2 + A tz^3/d^2 + B tz^4/d^4).
+ * B = 0 gives results identical to Gauss3D_Calibration. */
+typedef struct Gauss3D_CalibrationB {
+    float x[5];
+    float y[5];
+    float minz, maxz;
+} Gauss3D_CalibrationB;
+
+/* CSpline_Calibration, Estimators/CSpline/CubicSplinePSF.h:12-23 (shape = z, y, x). */
+typedef struct CSpline_Calibration {
+    int shape[3];
+    float z_min;
+    float z_max;
+    const float* coefs; /* [shape0][shape1][shape2][64] */
+} CSpline_Calibration;
+
+/* ---- Context (Context.h:43-44) ------------------------------------------------------ */
+Context* Context_Create(void);  /* replaces Context.cpp Context_Create */
+void Context_Destroy(Context* ctx); /* replaces Context_Destroy; deletes every estimator it owns */
+
+/* ---- Estimator factories -------------------------------------------------------------
+ * `cuda` is accepted for ABI compatibility; every estimator of this library runs on the
+ * current CUDA device (there is no CPU path). */
+/* Estimators/Gaussian/GaussianPSF.cu:87-108 */
+Estimator* Gauss2D_CreatePSF_XYIBg(int roisize, float sigmaX, float sigmaY, bool cuda, Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:110-132 (sigma x/y per spot as 2 constants) */
+Estimator* Gauss2D_CreatePSF_XYIBgConstSigma(int roisize, bool cuda, Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:136-158 */
+Estimator* Gauss2D_CreatePSF_XYIBgSigma(int roisize, float initialSigma, bool cuda, Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:162-185 */
+Estimator* Gauss2D_CreatePSF_XYIBgSigmaXY(int roisize, float initialSigmaX, float initialSigmaY, bool cuda,
+                                          Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:36-59 (the calibration is passed by reference in C++,
+ * i.e. as a pointer in the ABI) */
+Estimator* Gauss2D_CreatePSF_XYZIBg(int roisize, const Gauss3D_Calibration* calib, bool cuda, Context* ctx);
+/* Extension (no reference counterpart): astigmatic model with the quartic B term. */
+Estimator* Gauss2D_CreatePSF_XYZIBgB(int roisize, const Gauss3D_CalibrationB* calib, bool cuda, Context* ctx);
+/* Estimators/CSpline/CubicSplinePSF.cu:55-107. Only mode 0 (flat background) is supported;
+ * other modes report an error and return NULL. coefs (nullable) overrides calib->coefs. The
+ * coefficients are copied to the device at creation. */
+Estimator* CSpline_CreatePSF(int roisize, const CSpline_Calibration* calib, const float* coefs, int mode, bool cuda,
+                             Context* ctx);
+/* Estimators/CSpline/CubicSplinePSF.cu:135-146: z-stack file (header v1) -> coefficients (border 0). */
+Estimator* CSpline_CreatePSF_FromFile(int roisize, const char* filename, int mode, bool cuda, Context* ctx);
+/* Estimators/CSpline/CubicSplinePSF.cu:151-204: spline coefficients of a z-stack, computed on the
+ * GPU with the reference's double-precision LUP solve (bit-identical output).
+ * coefs[shape-3+2*border][64]. */
+void CSpline_Compute(const int* shape, const float* data, float* splineCoefs, int border);
+/* Estimators/CSpline/CubicSplinePSF.cu:208-271: value and x/y/z derivatives of the spline at
+ * a shifted position; values[(shape-2*border)][4]. */
+void CSpline_Evaluate(const int* shape, const float* splineCoefs, const float* shift, int border, float* values);
+
+/* ---- Estimator C API (Estimators/Estimator.h:157-171, Estimator.cpp:45-157) ---------- */
+void Estimator_Delete(Estimator* e);
+const char* Estimator_ParamFormat(Estimator* e);
+void Estimator_GetProperties(Estimator* e, EstimatorProperties* props);
+void Estimator_SampleDims(Estimator* e, int* dims);
+void Estimator_GetParamLimits(Estimator* e, ParamLimit* limits);
+void Estimator_SetLMParams(Estimator* e, const LMParams* p);
+void Estimator_GetLMParams(Estimator* e, LMParams* p);
+/* ev[numspots][H][W] */
+void Estimator_ComputeExpectedValue(Estimator* e, int numspots, const float* params, const float* constants,
+                                    const int* spotpos, float* ev);
+/* Fit (centre-of-mass start when initial == NULL). params[n][K], iterations[n] (nullable;
+ * = i+1 at the stop, maxIterations+1 when capped), trace[n][traceBufLen][K] (nullable),
+ * diagnostics: numDiag == 0 floats per spot (untouched). */
+void Estimator_Estimate(Estimator* e, int numspots, const float* sample, const float* constants, const int* spotpos,
+                        const float* initial, float* params, float* diagnostics, int* iterations, float* trace,
+                        int traceBufLen);
+/* deriv[n][K][H][W], ev[n][H][W] */
+void Estimator_ComputeDerivatives(Estimator* e, int numspots, const float* params, const float* constants,
+                                  const int* spotpos, float* psf_deriv, float* ev);
+/* crlb[n][K], chisq[n] (sample nullable: chi-square not computed, written as 0). */
+void Estimator_ChiSquareAndCRLB(Estimator* e, const float* params, const float* sample, const float* constants,
+                                const int* spotpos, int numspots, float* crlb, float* chisq);
+
+/* ---- Loader-time exports bound eagerly by photonpy/cpp/lib.py ------------------------ */
+int CudaGetNumDevices(void);                                                        /* CudaUtils.cu:12 */
+bool CudaSetDevice(int index);                                                      /* CudaUtils.cu:19 */
+bool CudaGetDeviceInfo(int index, int* numMultiprocessors, char* name, int namelen); /* CudaUtils.cu:24 */
+void CudaGetMemoryUse(uint64_t* pinnedBytes, uint64_t* devicePitchedBytes, uint64_t* deviceBytes,
+                      uint64_t* pitchedNumAllocs);                                  /* CudaUtils.cu:38 */
+void SetDebugPrintCallback(int (*cb)(const char* msg));                             /* StringUtils.cpp:45 */
+void SetDebugImageCallback(void (*cb)(int w, int h, int n, const float* d, const char* t)); /* DebugImageCallback.h:9 */
+void ShowDebugImage(int w, int h, int numImg, const float* data, const char* title); /* DebugImageCallback.h:10 */
+/* Out-of-scope exports that lib.py/gaussian.py bind at load time: present so those bindings
+ * load; each reports "not provided by photonpy_b200" and does nothing. */
+void FFT(const void* src, void* dst, int batchsize, int siglen, int forward);
+void FFT2(const void* src, void* dst, int batchsize, int sigw, int sigh, int forward);
+void DrawROIs(float* image, int width, int height, const float* rois, int numrois, int roisize, const int* roiposYX);
+void Gauss2D_Draw(double* image, int imgw, int imgh, float* spotList, int nspots, float addSigma);
+void Gauss2D_EstimateIntensityBg(const float* imageData, float* IBg, float* IBg_crlb, int numspots, const float* xy,
+                                 const int* roipos, const float* sigma, int imgw, int maxIterations, int cuda);
+Estimator* Gauss2D_CreatePSF_XYITiltedBg(int roisize, bool cuda, Context* ctx);
+Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int roisize, float sx, float sy, bool cuda, Context* ctx);
+
+/* ---- Extensions (no reference counterpart) ------------------------------------------ */
+/* Message of the last error on this thread ("" if none); cleared by PB200_ClearError. */
+const char* PB200_GetLastError(void);
+void PB200_ClearError(void);
+/* Fused localization: LM fit + Fisher/CRLB + chi-square in one launch (what photonpy's
+ * EstimationQueue runs as Estimate followed by ChiSquareAndCRLB, EstimationQueue.cpp:285-289).
+ * Host pointers; large batches are pipelined in chunks over two CUDA streams. */
+void PB200_EstimateCRLB(Estimator* e, int numspots, const float* sample, const float* constants,
+                        const float* initial, float* params, int* iterations, float* crlb, float* chisq);
+/* Device-pointer variants on a caller stream (cudaStream_t as void*; NULL = legacy default).
+ * No host synchronisation; all pointers are device memory. crlb/chisq/iterations/trace nullable. */
+void PB200_EstimateDevice(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                          const float* d_initial, float* d_params, int* d_iterations, float* d_trace, int traceBufLen,
+                          float* d_crlb, float* d_chisq, void* stream);
+void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
+                               float* d_ev, float* d_deriv, void* stream);
+void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_params, const float* d_sample,
+                                  const float* d_constants, float* d_crlb, float* d_chisq, void* stream);
+/* Kernel configuration used for this estimator: lanes per ROI (4, 8, 16, 32; 0 = automatic)
+ * and threads per block (64..256). Returns 0 on success. */
+int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
+void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock);
+/* Number of fit-kernel launches issued by this library since load (for launch accounting). */
+uint64_t PB200_LaunchCount(void);
+/* Model id (0 XYIBg, 1 XYIBgConstSigma, 2 XYIBgSigma, 3 XYIBgSigmaXY, 4 XYZIBg, 5 CSpline) and ROI size. */
+int PB200_ModelInfo(Estimator* e, int* roisize);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHOTONPY_B200_H */

@@ -1,0 +1,85 @@
+"""Build libphotonpy_b200.so (sm_100a) in-tree with nvcc.
+
+    python -m photonpy_b200.csrc.build [--verbose]
+
+Output: photonpy_b200/lib/libphotonpy_b200.so. The library statically links the CUDA
+runtime so that it does not depend on which libcudart other modules of the process load.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+LIB_DIR = os.path.join(PKG, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libphotonpy_b200.so")
+OBJ_DIR = os.path.join(PKG, "_build")
+
+UNITS = ["estimator.cu"]
+HEADERS = ["models.cuh", "fit_kernels.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def sources():
+    return [os.path.join(HERE, u) for u in UNITS] + [os.path.join(HERE, h) for h in HEADERS] + [
+        os.path.join(ROOT, "include", "photonpy_b200.h")]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB_PATH):
+        return False
+    t = os.path.getmtime(LIB_PATH)
+    return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB_PATH
+    os.makedirs(LIB_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    common = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-O3", "-I", os.path.join(ROOT, "include")]
+    if verbose:
+        common += ["-Xptxas", "-v"]
+
+    def compile_unit(u):
+        src = os.path.join(HERE, u)
+        obj = os.path.join(OBJ_DIR, os.path.splitext(u)[0] + ".o")
+        cmd = [nvcc(), *common, "-c", src, "-o", obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {u}:\n{r.stdout}\n{r.stderr}")
+        return obj, r.stderr
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(len(UNITS), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_unit, UNITS))
+    if verbose:
+        for _, log in results:
+            sys.stderr.write(log)
+    tmp = LIB_PATH + f".tmp{os.getpid()}"
+    cmd = [nvcc(), "-shared", *ARCH, "-o", tmp, *[o for o, _ in results], "-cudart", "static", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    args = ap.parse_args()
+    print(build(force=args.force, verbose=args.verbose))

@@ -1,0 +1,996 @@
+// C ABI of the photonpy_b200 estimator: estimator objects, context, host<->device staging,
+// kernel dispatch and the spline-coefficient kernels.
+//
+// Replaces (paths inside photonpy's cpp/SMLMLib):
+//   Estimators/Estimator.cpp:45-157         Estimator_* C API
+//   Estimators/EstimatorImpl.cu:225-300     cuEstimatorWrapper (host pointers -> device)
+//   Estimators/EstimatorImpl.h:58-105       cuPSFImpl kernels (one thread per ROI)
+//   Estimators/Gaussian/GaussianPSF.cu      Gauss2D_CreatePSF_* factories and exported limits
+//   Estimators/CSpline/CubicSplinePSF.cu    CSpline_CreatePSF / _FromFile / _Compute / _Evaluate
+//   Context.cpp, StringUtils.cpp, CudaUtils.cu, DebugImageCallback.cpp (loader-time exports)
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "../../include/photonpy_b200.h"
+#include "fit_kernels.cuh"
+
+using namespace pb200;
+
+// ------------------------------------------------------------------------------------
+// errors and debug output
+// ------------------------------------------------------------------------------------
+namespace {
+thread_local std::string t_lastError;
+int (*g_debugPrint)(const char*) = nullptr;
+void (*g_debugImage)(int, int, int, const float*, const char*) = nullptr;
+std::atomic<uint64_t> g_launches{0};
+
+void debug_printf(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (g_debugPrint) g_debugPrint(buf);
+    else fputs(buf, stderr);
+}
+
+void report(const std::exception& e) {
+    t_lastError = e.what();
+    debug_printf("%s\n", e.what());
+}
+
+struct Error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define PB_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t err_ = (call);                                                                     \
+        if (err_ != cudaSuccess)                                                                       \
+            throw Error(std::string("CUDA error: ") + cudaGetErrorString(err_) + " in " #call);       \
+    } while (0)
+
+// ------------------------------------------------------------------------------------
+// device buffers
+// ------------------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+    void ensure(size_t nbytes) {
+        if (nbytes <= bytes) return;
+        release();
+        size_t want = nbytes < 256 ? 256 : nbytes;
+        PB_CUDA(cudaGetDevice(&device));
+        PB_CUDA(cudaMalloc(&p, want));
+        bytes = want;
+    }
+    void release() {
+        if (p) {
+            int cur = -1;
+            cudaGetDevice(&cur);
+            if (device >= 0 && device != cur) cudaSetDevice(device);
+            cudaFree(p);
+            if (device >= 0 && device != cur) cudaSetDevice(cur);
+        }
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+    ~DevBuf() { release(); }
+};
+
+int num_sms() {
+    static int sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) {
+        cudaDeviceProp prop;
+        PB_CUDA(cudaGetDeviceProperties(&prop, dev));
+        sms[dev] = prop.multiProcessorCount;
+    }
+    return sms[dev];
+}
+
+// ------------------------------------------------------------------------------------
+// kernel dispatch over (model, lanes per ROI)
+// ------------------------------------------------------------------------------------
+using FitLaunch = void (*)(const ModelDesc&, FitArgs, int threads, cudaStream_t);
+using EvalLaunch = void (*)(const ModelDesc&, const float*, const float*, float*, float*, int, int threads,
+                            cudaStream_t);
+
+constexpr int kMaxSmemPerBlock = 200 * 1024;
+
+template <class M, int G>
+void launch_fit(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
+    if (a.n <= 0) return;
+    auto kern = fit_kernel<M, G>;
+    a.smemStride = group_smem_floats<M>(d.roisize);
+    int gpb = threads / G;
+    size_t smem = (size_t)gpb * a.smemStride * sizeof(float);
+    while (smem > (size_t)kMaxSmemPerBlock && threads > 32) {
+        threads /= 2;
+        gpb = threads / G;
+        smem = (size_t)gpb * a.smemStride * sizeof(float);
+    }
+    if (smem > (size_t)kMaxSmemPerBlock || gpb < 1) throw Error("ROI too large for the fit kernel's shared memory");
+    static std::once_flag once;
+    std::call_once(once, [&] { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerBlock); });
+    int perSM = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem));
+    if (perSM < 1) perSM = 1;
+    const long long needed = (a.n + gpb - 1) / gpb;
+    const long long cap = (long long)num_sms() * perSM;
+    const int grid = (int)(needed < cap ? needed : cap);
+    kern<<<grid, threads, smem, s>>>(d, a);
+    PB_CUDA(cudaGetLastError());
+    g_launches++;
+}
+
+template <class M, int G>
+void launch_eval(const ModelDesc& d, const float* params, const float* consts, float* ev, float* deriv, int n,
+                 int threads, cudaStream_t s) {
+    if (n <= 0) return;
+    auto kern = eval_kernel<M, G>;
+    const int stride = round_up(M::table_floats(d.roisize), 32) + 8;
+    const int gpb = threads / G;
+    const size_t smem = (size_t)gpb * stride * sizeof(float);
+    int perSM = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem));
+    if (perSM < 1) perSM = 1;
+    const long long needed = (n + gpb - 1) / gpb;
+    const long long cap = (long long)num_sms() * perSM * 4;
+    const int grid = (int)(needed < cap ? needed : cap);
+    kern<<<grid, threads, smem, s>>>(d, params, consts, ev, deriv, n, stride);
+    PB_CUDA(cudaGetLastError());
+    g_launches++;
+}
+
+template <class M>
+struct ModelTable {
+    static FitLaunch fit(int G) {
+        switch (G) {
+        case 4: return launch_fit<M, 4>;
+        case 8: return launch_fit<M, 8>;
+        case 16: return launch_fit<M, 16>;
+        default: return launch_fit<M, 32>;
+        }
+    }
+    static EvalLaunch eval(int G) {
+        switch (G) {
+        case 8: return launch_eval<M, 8>;
+        case 16: return launch_eval<M, 16>;
+        default: return launch_eval<M, 32>;
+        }
+    }
+};
+
+FitLaunch fit_launcher(int model, int G) {
+    switch (model) {
+    case MODEL_XYIBG: return ModelTable<GaussModel<MODEL_XYIBG>>::fit(G);
+    case MODEL_XYIBG_CONSTSIGMA: return ModelTable<GaussModel<MODEL_XYIBG_CONSTSIGMA>>::fit(G);
+    case MODEL_XYIBG_SIGMA: return ModelTable<GaussModel<MODEL_XYIBG_SIGMA>>::fit(G);
+    case MODEL_XYIBG_SIGMAXY: return ModelTable<GaussModel<MODEL_XYIBG_SIGMAXY>>::fit(G);
+    case MODEL_XYZIBG: return ModelTable<GaussModel<MODEL_XYZIBG>>::fit(G);
+    case MODEL_CSPLINE: return ModelTable<SplineModel>::fit(G);
+    }
+    throw Error("unknown model");
+}
+
+EvalLaunch eval_launcher(int model, int G) {
+    switch (model) {
+    case MODEL_XYIBG: return ModelTable<GaussModel<MODEL_XYIBG>>::eval(G);
+    case MODEL_XYIBG_CONSTSIGMA: return ModelTable<GaussModel<MODEL_XYIBG_CONSTSIGMA>>::eval(G);
+    case MODEL_XYIBG_SIGMA: return ModelTable<GaussModel<MODEL_XYIBG_SIGMA>>::eval(G);
+    case MODEL_XYIBG_SIGMAXY: return ModelTable<GaussModel<MODEL_XYIBG_SIGMAXY>>::eval(G);
+    case MODEL_XYZIBG: return ModelTable<GaussModel<MODEL_XYZIBG>>::eval(G);
+    case MODEL_CSPLINE: return ModelTable<SplineModel>::eval(G);
+    }
+    throw Error("unknown model");
+}
+
+// Lanes per ROI when no tuned value is set: enough ROIs per warp to amortise the redundant
+// K x K solve for small ROIs, enough lanes to keep per-lane pixel loops short for large ones.
+int default_lanes(int model, int R) {
+    const int npix = R * R;
+    if (model == MODEL_CSPLINE) return npix <= 100 ? 8 : 16;
+    if (npix <= 64) return 4;
+    if (npix <= 324) return 8;
+    if (npix <= 784) return 16;
+    return 32;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// Context and Estimator objects
+// ------------------------------------------------------------------------------------
+struct Estimator;
+
+struct Context {
+    std::mutex mtx;
+    std::unordered_set<Estimator*> objects;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    DevBuf smp, consts, initial, params, iters, trace, crlb, chisq;
+};
+
+struct Estimator {
+    ModelDesc desc{};
+    int K = 0, numconst = 0;
+    std::string format;
+    std::vector<ParamLimit> limits;
+    LMParams lm{30, 1e-15f, 0.0f};  // C++ default of the reference (Estimator.cpp:24)
+    Context* ctx = nullptr;
+    DevBuf coefs;
+    int lanes = 0, threads = 256;
+    int device = 0;
+    std::mutex mtx;
+    Slot slots[2];
+
+    Estimator() { PB_CUDA(cudaGetDevice(&device)); }
+    ~Estimator() {
+        for (auto& s : slots)
+            if (s.stream) cudaStreamDestroy(s.stream);
+    }
+    int lanes_for() const { return lanes ? lanes : default_lanes(desc.model, desc.roisize); }
+    int npix() const { return desc.roisize * desc.roisize; }
+    Slot& slot(int i) {
+        if (!slots[i].stream) PB_CUDA(cudaStreamCreateWithFlags(&slots[i].stream, cudaStreamNonBlocking));
+        return slots[i];
+    }
+};
+
+namespace {
+
+void attach(Estimator* e, Context* ctx) {
+    if (!ctx) return;
+    std::lock_guard<std::mutex> g(ctx->mtx);
+    ctx->objects.insert(e);
+    e->ctx = ctx;
+}
+
+void detach(Estimator* e) {
+    if (!e->ctx) return;
+    std::lock_guard<std::mutex> g(e->ctx->mtx);
+    e->ctx->objects.erase(e);
+    e->ctx = nullptr;
+}
+
+Estimator* make_gauss(int model, int roisize, float s0, float s1, const float* ax, const float* ay, float minz,
+                      float maxz, Context* ctx) {
+    if (roisize < 3 || roisize > 64) throw Error("roisize must be in [3, 64]");
+    auto* e = new Estimator();
+    e->desc.model = model;
+    e->desc.roisize = roisize;
+    e->desc.sigma[0] = s0;
+    e->desc.sigma[1] = s1;
+    for (int i = 0; i < 5; i++) {
+        e->desc.astig_x[i] = ax ? ax[i] : 0.0f;
+        e->desc.astig_y[i] = ay ? ay[i] : 0.0f;
+    }
+    e->desc.minz = minz;
+    e->desc.maxz = maxz;
+    e->K = model_num_params(model);
+    e->numconst = model_num_consts(model);
+    // Exported limits (GaussianPSF.cu:42-48, 92-97, 115-120, 141-147, 168-175).
+    const float border = 1.5f;
+    const float xyhi = (float)(roisize - 1) - border;
+    switch (model) {
+    case MODEL_XYIBG:
+    case MODEL_XYIBG_CONSTSIGMA:
+        e->format = "x,y,I,bg";
+        e->limits = {{border, xyhi}, {border, xyhi}, {10.0f, 1e9f}, {1e-6f, 1e9f}};
+        break;
+    case MODEL_XYIBG_SIGMA:
+        e->format = "x,y,\tI,bg,sigma";  // the reference's format string has this tab
+        e->limits = {{border, xyhi}, {border, xyhi}, {10.0f, 1e9f}, {1e-6f, 1e9f}, {1.0f, roisize * 2.0f}};
+        break;
+    case MODEL_XYIBG_SIGMAXY:
+        e->format = "x,y,I,bg,sx,sy";
+        e->limits = {{border, xyhi}, {border, xyhi}, {10.0f, 1e9f}, {1e-6f, 1e9f},
+                     {1.0f, roisize * 2.0f}, {1.0f, roisize * 2.0f}};
+        break;
+    case MODEL_XYZIBG:
+        e->format = "x,y,z,I,bg";
+        e->limits = {{border, xyhi}, {border, xyhi}, {minz, maxz}, {10.0f, 1e9f}, {1e-6f, 1e9f}};
+        break;
+    }
+    attach(e, ctx);
+    return e;
+}
+
+struct Chunking {
+    int chunk;
+};
+
+// Host-pointer fit through the two-slot pipeline: H2D(c) + kernel(c) on slot c%2 are issued
+// before D2H(c-1), so copies of one chunk overlap the fit of the other.
+void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, const float* h_initial,
+              float* h_params, int* h_iters, float* h_trace, int traceLen, float* h_crlb, float* h_chisq,
+              int flags) {
+    std::lock_guard<std::mutex> g(e->mtx);
+    PB_CUDA(cudaSetDevice(e->device));
+    const int K = e->K, NC = e->numconst, npix = e->npix();
+    const bool fisherOnly = (flags & FIT_CRLB_ONLY) != 0;
+    int chunk = n;
+    if (n > 65536) chunk = std::max(32768, (n + 7) / 8);
+    const int nchunks = (n + chunk - 1) / chunk;
+    FitLaunch fl = fit_launcher(e->desc.model, e->lanes_for());
+    struct Pending {
+        int slot, start, count;
+    };
+    std::vector<Pending> pend;
+    auto d2h = [&](const Pending& p) {
+        Slot& s = e->slot(p.slot);
+        if (h_params && !fisherOnly)
+            PB_CUDA(cudaMemcpyAsync(h_params + (size_t)p.start * K, s.params.as<float>(), sizeof(float) * K * p.count,
+                                    cudaMemcpyDeviceToHost, s.stream));
+        if (h_iters)
+            PB_CUDA(cudaMemcpyAsync(h_iters + p.start, s.iters.as<int>(), sizeof(int) * p.count,
+                                    cudaMemcpyDeviceToHost, s.stream));
+        if (h_trace && traceLen > 0)
+            PB_CUDA(cudaMemcpyAsync(h_trace + (size_t)p.start * traceLen * K, s.trace.as<float>(),
+                                    sizeof(float) * (size_t)traceLen * K * p.count, cudaMemcpyDeviceToHost,
+                                    s.stream));
+        if (h_crlb)
+            PB_CUDA(cudaMemcpyAsync(h_crlb + (size_t)p.start * K, s.crlb.as<float>(), sizeof(float) * K * p.count,
+                                    cudaMemcpyDeviceToHost, s.stream));
+        if (h_chisq)
+            PB_CUDA(cudaMemcpyAsync(h_chisq + p.start, s.chisq.as<float>(), sizeof(float) * p.count,
+                                    cudaMemcpyDeviceToHost, s.stream));
+    };
+    for (int c = 0; c < nchunks; c++) {
+        const int start = c * chunk, count = std::min(chunk, n - start);
+        Slot& s = e->slot(c & 1);
+        if (h_smp) {
+            s.smp.ensure(sizeof(float) * (size_t)npix * count);
+            PB_CUDA(cudaMemcpyAsync(s.smp.p, h_smp + (size_t)start * npix, sizeof(float) * (size_t)npix * count,
+                                    cudaMemcpyHostToDevice, s.stream));
+        }
+        if (NC) {
+            if (!h_consts) throw Error("this estimator needs per-spot constants");
+            s.consts.ensure(sizeof(float) * NC * count);
+            PB_CUDA(cudaMemcpyAsync(s.consts.p, h_consts + (size_t)start * NC, sizeof(float) * NC * count,
+                                    cudaMemcpyHostToDevice, s.stream));
+        }
+        if (h_initial) {
+            s.initial.ensure(sizeof(float) * K * count);
+            PB_CUDA(cudaMemcpyAsync(s.initial.p, h_initial + (size_t)start * K, sizeof(float) * K * count,
+                                    cudaMemcpyHostToDevice, s.stream));
+        }
+        s.params.ensure(sizeof(float) * K * count);
+        if (h_iters) s.iters.ensure(sizeof(int) * count);
+        if (h_trace && traceLen > 0) {
+            s.trace.ensure(sizeof(float) * (size_t)traceLen * K * count);
+            PB_CUDA(cudaMemsetAsync(s.trace.p, 0, sizeof(float) * (size_t)traceLen * K * count, s.stream));
+        }
+        if (h_crlb) s.crlb.ensure(sizeof(float) * K * count);
+        if (h_chisq || h_crlb) s.chisq.ensure(sizeof(float) * count);
+        FitArgs a{};
+        a.smp = h_smp ? s.smp.as<float>() : nullptr;
+        a.consts = NC ? s.consts.as<float>() : nullptr;
+        a.initial = h_initial ? s.initial.as<float>() : nullptr;
+        a.params = s.params.as<float>();
+        a.iterations = h_iters ? s.iters.as<int>() : nullptr;
+        a.trace = (h_trace && traceLen > 0) ? s.trace.as<float>() : nullptr;
+        a.traceLen = (h_trace && traceLen > 0) ? traceLen : 0;
+        a.crlb = h_crlb ? s.crlb.as<float>() : nullptr;
+        a.chisq = (h_chisq || h_crlb) ? s.chisq.as<float>() : nullptr;
+        a.n = count;
+        a.maxIter = e->lm.iterations;
+        a.lambda = e->lm.lambda;
+        a.flags = flags;
+        fl(e->desc, a, e->threads, s.stream);
+        pend.push_back({c & 1, start, count});
+        if (pend.size() == 2) {
+            d2h(pend.front());
+            pend.erase(pend.begin());
+        }
+    }
+    for (auto& p : pend) d2h(p);
+    for (int i = 0; i < 2; i++)
+        if (e->slots[i].stream) PB_CUDA(cudaStreamSynchronize(e->slots[i].stream));
+}
+
+void host_eval(Estimator* e, int n, const float* h_params, const float* h_consts, float* h_ev, float* h_deriv) {
+    std::lock_guard<std::mutex> g(e->mtx);
+    PB_CUDA(cudaSetDevice(e->device));
+    const int K = e->K, NC = e->numconst, npix = e->npix();
+    Slot& s = e->slot(0);
+    s.initial.ensure(sizeof(float) * K * n);
+    PB_CUDA(cudaMemcpyAsync(s.initial.p, h_params, sizeof(float) * K * n, cudaMemcpyHostToDevice, s.stream));
+    if (NC) {
+        if (!h_consts) throw Error("this estimator needs per-spot constants");
+        s.consts.ensure(sizeof(float) * NC * n);
+        PB_CUDA(cudaMemcpyAsync(s.consts.p, h_consts, sizeof(float) * NC * n, cudaMemcpyHostToDevice, s.stream));
+    }
+    if (h_ev) s.smp.ensure(sizeof(float) * (size_t)npix * n);
+    if (h_deriv) s.trace.ensure(sizeof(float) * (size_t)npix * K * n);
+    int G = e->lanes_for();
+    if (G < 8) G = 8;
+    eval_launcher(e->desc.model, G)(e->desc, s.initial.as<float>(), NC ? s.consts.as<float>() : nullptr,
+                                    h_ev ? s.smp.as<float>() : nullptr, h_deriv ? s.trace.as<float>() : nullptr, n,
+                                    256, s.stream);
+    if (h_ev)
+        PB_CUDA(cudaMemcpyAsync(h_ev, s.smp.p, sizeof(float) * (size_t)npix * n, cudaMemcpyDeviceToHost, s.stream));
+    if (h_deriv)
+        PB_CUDA(cudaMemcpyAsync(h_deriv, s.trace.p, sizeof(float) * (size_t)npix * K * n, cudaMemcpyDeviceToHost,
+                                s.stream));
+    PB_CUDA(cudaStreamSynchronize(s.stream));
+}
+
+// ------------------------------------------------------------------------------------
+// Spline coefficients (CubicSplinePSF.cu:151-204) on the GPU.
+// The 64x64 power-basis matrix is LUP-factored once on the host in double precision with the
+// reference's algorithm; one thread per output voxel runs the reference's forward/backward
+// substitution with non-fused double arithmetic, so results are bit-identical.
+// ------------------------------------------------------------------------------------
+__constant__ double c_splineLU[64 * 64];
+__constant__ int c_splineP[65];
+
+__global__ void spline_compute_kernel(const float* __restrict__ data, int s0, int s1, int s2, int border,
+                                      float* __restrict__ coefs, int o0, int o1, int o2) {
+    const long long total = (long long)o0 * o1 * o2;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(v % o2);
+        const int j = (int)((v / o2) % o1);
+        const int i = (int)(v / ((long long)o1 * o2));
+        double b[64], x[64];
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+#pragma unroll
+            for (int n = 0; n < 4; n++)
+#pragma unroll
+                for (int o = 0; o < 4; o++) {
+                    int z = min(max(i + m - border, 0), s0 - 1);
+                    int y = min(max(j + n - border, 0), s1 - 1);
+                    int xx = min(max(k + o - border, 0), s2 - 1);
+                    b[m * 16 + n * 4 + o] = (double)data[((size_t)z * s1 + y) * s2 + xx];
+                }
+        for (int r = 0; r < 64; r++) {
+            double t = b[c_splineP[r]];
+            for (int q = 0; q < r; q++) t = __dsub_rn(t, __dmul_rn(c_splineLU[r * 64 + q], x[q]));
+            x[r] = t;
+        }
+        for (int r = 63; r >= 0; r--) {
+            double t = x[r];
+            for (int q = r + 1; q < 64; q++) t = __dsub_rn(t, __dmul_rn(c_splineLU[r * 64 + q], x[q]));
+            x[r] = __ddiv_rn(t, c_splineLU[r * 64 + r]);
+        }
+        float* dst = coefs + 64 * v;
+#pragma unroll
+        for (int a = 0; a < 64; a++) dst[a] = (float)x[a];
+    }
+}
+
+void spline_lu_once() {
+    static std::once_flag once;
+    static int dev_done[64] = {0};
+    static double LU[64 * 64];
+    static int P[65];
+    std::call_once(once, [] {
+        const int N = 64;
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++)
+                for (int k = 0; k < 4; k++)
+                    for (int l = 0; l < 4; l++)
+                        for (int m = 0; m < 4; m++)
+                            for (int n = 0; n < 4; n++)
+                                LU[64 * (i * 16 + j * 4 + k) + (l * 16 + m * 4 + n)] =
+                                    (double)(powf((float)(i - 1.0), (float)l) * powf((float)(j - 1.0), (float)m) *
+                                             powf((float)(k - 1.0), (float)n));
+        for (int i = 0; i <= N; i++) P[i] = i;
+        for (int i = 0; i < N; i++) {
+            double maxA = 0.0, absA;
+            int imax = i;
+            for (int k = i; k < N; k++)
+                if ((absA = std::fabs(LU[k * N + i])) > maxA) { maxA = absA; imax = k; }
+            if (imax != i) {
+                std::swap(P[i], P[imax]);
+                for (int jj = 0; jj < N; jj++) std::swap(LU[i * N + jj], LU[imax * N + jj]);
+                P[N]++;
+            }
+            for (int j = i + 1; j < N; j++) {
+                LU[j * N + i] /= LU[i * N + i];
+                for (int k = i + 1; k < N; k++) LU[j * N + k] -= LU[j * N + i] * LU[i * N + k];
+            }
+        }
+    });
+    int dev = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !dev_done[dev]) {
+        PB_CUDA(cudaMemcpyToSymbol(c_splineLU, LU, sizeof(LU)));
+        PB_CUDA(cudaMemcpyToSymbol(c_splineP, P, sizeof(P)));
+        dev_done[dev] = 1;
+    }
+}
+
+void spline_compute_device(const int* shape, const float* d_data, float* d_coefs, int border, cudaStream_t s) {
+    spline_lu_once();
+    const int o0 = shape[0] - 3 + 2 * border, o1 = shape[1] - 3 + 2 * border, o2 = shape[2] - 3 + 2 * border;
+    if (o0 <= 0 || o1 <= 0 || o2 <= 0) throw Error("z-stack too small for a cubic spline");
+    const long long total = (long long)o0 * o1 * o2;
+    const int threads = 128;
+    const int grid = (int)std::min<long long>((total + threads - 1) / threads, 65535);
+    spline_compute_kernel<<<grid, threads, 0, s>>>(d_data, shape[0], shape[1], shape[2], border, d_coefs, o0, o1, o2);
+    PB_CUDA(cudaGetLastError());
+    g_launches++;
+}
+
+// CSpline_Evaluate (CubicSplinePSF.cu:208-271): values[z][y][x][4] = val, dx, dy, dz.
+__global__ void spline_evaluate_kernel(const float* __restrict__ coefs, int s0, int s1, int s2, float d0, float d1,
+                                       float d2, float sh0, float sh1, float sh2, int border, float* values) {
+    const int n0 = s0 - 2 * border, n1 = s1 - 2 * border, n2 = s2 - 2 * border;
+    const long long total = (long long)n0 * n1 * n2;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % n2) + border;
+        const int y = (int)((v / n2) % n1) + border;
+        const int z = (int)(v / ((long long)n1 * n2)) + border;
+        float df[64], dxf[64], dyf[64], dzf[64];
+        for (int q = 0; q < 64; q++) df[q] = dxf[q] = dyf[q] = dzf[q] = 0.0f;
+        float zzz = 1.0f;
+        for (int m = 0; m <= 3; m++) {
+            float yyy = 1.0f;
+            for (int n = 0; n <= 3; n++) {
+                float xxx = 1.0f;
+                for (int o = 0; o <= 3; o++) {
+                    const float xyz = MUL(MUL(xxx, yyy), zzz);
+                    df[m * 16 + n * 4 + o] = xyz;
+                    if (o < 3) dxf[m * 16 + n * 4 + o + 1] = MUL((float)o + 1.0f, xyz);
+                    if (n < 3) dyf[m * 16 + (n + 1) * 4 + o] = MUL((float)n + 1.0f, xyz);
+                    if (m < 3) dzf[(m + 1) * 16 + n * 4 + o] = MUL((float)m + 1.0f, xyz);
+                    xxx = MUL(xxx, d2);
+                }
+                yyy = MUL(yyy, d1);
+            }
+            zzz = MUL(zzz, d0);
+        }
+        const float zz = SUB((float)z, sh0);
+        const int k = min(max((int)zz, 0), s0 - 1);
+        const float yy = SUB((float)y, sh1);
+        const int j = min(max((int)yy, 0), s1 - 1);
+        const float xx = SUB((float)x, sh2);
+        const int i = min(max((int)xx, 0), s2 - 1);
+        float val = 0.0f, dx = 0.0f, dy = 0.0f, dz = 0.0f;
+        const float* c = coefs + 64 * (((size_t)k * s1 + j) * s2 + i);
+        for (int idx = 0; idx < 64; idx++) {
+            const float cf = c[idx];
+            val = ADD(val, MUL(df[idx], cf));
+            dx = ADD(dx, MUL(dxf[idx], cf));
+            dy = ADD(dy, MUL(dyf[idx], cf));
+            dz = ADD(dz, MUL(dzf[idx], cf));
+        }
+        float* out = values + 4 * v;
+        out[0] = val;
+        out[1] = dx;
+        out[2] = dy;
+        out[3] = dz;
+    }
+}
+
+Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const float* h_coefs, int mode, Context* ctx,
+                       const float* d_coefs_src) {
+    if (mode != 0) throw Error("CSpline_CreatePSF: only mode 0 (flat background) is provided by photonpy_b200");
+    if (roisize < 3 || roisize > 64) throw Error("roisize must be in [3, 64]");
+    if (!calib) throw Error("CSpline_CreatePSF: calibration is null");
+    const int nz = calib->shape[0], ny = calib->shape[1], nx = calib->shape[2];
+    if (nz <= 0 || ny <= 0 || nx <= 0) throw Error("CSpline_CreatePSF: empty coefficient grid");
+    auto* e = new Estimator();
+    try {
+        e->desc.model = MODEL_CSPLINE;
+        e->desc.roisize = roisize;
+        e->desc.spline_shape[0] = nz;
+        e->desc.spline_shape[1] = ny;
+        e->desc.spline_shape[2] = nx;
+        e->desc.spline_zmin = calib->z_min;
+        e->desc.spline_zmax = calib->z_max;
+        const size_t ncoef = (size_t)nz * ny * nx * 64;
+        e->coefs.ensure(sizeof(float) * ncoef);
+        if (d_coefs_src)
+            PB_CUDA(cudaMemcpy(e->coefs.p, d_coefs_src, sizeof(float) * ncoef, cudaMemcpyDeviceToDevice));
+        else {
+            const float* src = h_coefs ? h_coefs : calib->coefs;
+            if (!src) throw Error("CSpline_CreatePSF: no coefficients");
+            PB_CUDA(cudaMemcpy(e->coefs.p, src, sizeof(float) * ncoef, cudaMemcpyHostToDevice));
+        }
+        e->desc.coefs = e->coefs.as<float>();
+        e->K = 5;
+        e->numconst = 0;
+        e->format = "x,y,z,I,bg";
+        const float border = 1.5f;
+        const float xyhi = (float)(roisize - 1) - border;
+        e->limits = {{border, xyhi}, {border, xyhi}, {calib->z_min, calib->z_max}, {10.0f, 1e9f}, {1e-6f, 1e9f}};
+    } catch (...) {
+        delete e;
+        throw;
+    }
+    attach(e, ctx);
+    return e;
+}
+
+void check_estimator(Estimator* e) {
+    if (!e) throw Error("estimator is null");
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------
+template <class F>
+auto guarded(F&& f, decltype(f()) onerr) -> decltype(f()) {
+    try {
+        return f();
+    } catch (const std::exception& ex) {
+        report(ex);
+        return onerr;
+    }
+}
+
+template <class F>
+void guarded_void(F&& f) {
+    try {
+        f();
+    } catch (const std::exception& ex) {
+        report(ex);
+    }
+}
+
+extern "C" {
+
+const char* PB200_GetLastError(void) { return t_lastError.c_str(); }
+void PB200_ClearError(void) { t_lastError.clear(); }
+uint64_t PB200_LaunchCount(void) { return g_launches.load(); }
+
+Context* Context_Create(void) { return new Context(); }
+
+void Context_Destroy(Context* ctx) {
+    if (!ctx) return;
+    std::vector<Estimator*> objs;
+    {
+        std::lock_guard<std::mutex> g(ctx->mtx);
+        objs.assign(ctx->objects.begin(), ctx->objects.end());
+        ctx->objects.clear();
+    }
+    for (auto* e : objs) {
+        e->ctx = nullptr;
+        delete e;
+    }
+    delete ctx;
+}
+
+Estimator* Gauss2D_CreatePSF_XYIBg(int roisize, float sigmaX, float sigmaY, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {return make_gauss(MODEL_XYIBG, roisize, sigmaX, sigmaY, nullptr, nullptr, 0, 0, ctx);}, (Estimator*)nullptr);
+}
+
+Estimator* Gauss2D_CreatePSF_XYIBgConstSigma(int roisize, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {return make_gauss(MODEL_XYIBG_CONSTSIGMA, roisize, 0, 0, nullptr, nullptr, 0, 0, ctx);}, (Estimator*)nullptr);
+}
+
+Estimator* Gauss2D_CreatePSF_XYIBgSigma(int roisize, float initialSigma, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {return make_gauss(MODEL_XYIBG_SIGMA, roisize, initialSigma, initialSigma, nullptr, nullptr, 0, 0, ctx);
+           }, (Estimator*)nullptr);
+}
+
+Estimator* Gauss2D_CreatePSF_XYIBgSigmaXY(int roisize, float sx, float sy, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {return make_gauss(MODEL_XYIBG_SIGMAXY, roisize, sx, sy, nullptr, nullptr, 0, 0, ctx);}, (Estimator*)nullptr);
+}
+
+Estimator* Gauss2D_CreatePSF_XYZIBg(int roisize, const Gauss3D_Calibration* calib, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {
+        if (!calib) throw Error("Gauss2D_CreatePSF_XYZIBg: calibration is null");
+        float ax[5] = {calib->x[0], calib->x[1], calib->x[2], calib->x[3], 0.0f};
+        float ay[5] = {calib->y[0], calib->y[1], calib->y[2], calib->y[3], 0.0f};
+        return make_gauss(MODEL_XYZIBG, roisize, 0, 0, ax, ay, calib->minz, calib->maxz, ctx);
+        }, (Estimator*)nullptr);
+}
+
+Estimator* Gauss2D_CreatePSF_XYZIBgB(int roisize, const Gauss3D_CalibrationB* calib, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {
+        if (!calib) throw Error("Gauss2D_CreatePSF_XYZIBgB: calibration is null");
+        return make_gauss(MODEL_XYZIBG, roisize, 0, 0, calib->x, calib->y, calib->minz, calib->maxz, ctx);
+        }, (Estimator*)nullptr);
+}
+
+Estimator* CSpline_CreatePSF(int roisize, const CSpline_Calibration* calib, const float* coefs, int mode, bool,
+                             Context* ctx) {
+    return guarded([&]() -> Estimator* {return make_spline(roisize, calib, coefs, mode, ctx, nullptr);}, (Estimator*)nullptr);
+}
+
+Estimator* CSpline_CreatePSF_FromFile(int roisize, const char* filename, int mode, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {
+        FILE* f = fopen(filename, "rb");
+        if (!f) throw Error(std::string("Can't open file ") + (filename ? filename : "(null)"));
+        struct {
+            int version;
+            int shape[3];
+            float zmin, zmax;
+        } h;
+        size_t got = fread(&h, sizeof(h), 1, f);
+        if (got != 1 || h.version != 1) {
+            fclose(f);
+            throw Error("Wrong ZStack file version (should be 1)");
+        }
+        const size_t nvox = (size_t)h.shape[0] * h.shape[1] * h.shape[2];
+        std::vector<float> data(nvox);
+        got = fread(data.data(), sizeof(float), nvox, f);
+        fclose(f);
+        if (got != nvox) throw Error("ZStack file is truncated");
+        DevBuf dd, dc;
+        dd.ensure(sizeof(float) * nvox);
+        PB_CUDA(cudaMemcpy(dd.p, data.data(), sizeof(float) * nvox, cudaMemcpyHostToDevice));
+        const int border = 0;
+        int os[3] = {h.shape[0] - 3 + 2 * border, h.shape[1] - 3 + 2 * border, h.shape[2] - 3 + 2 * border};
+        dc.ensure(sizeof(float) * 64 * (size_t)os[0] * os[1] * os[2]);
+        spline_compute_device(h.shape, dd.as<float>(), dc.as<float>(), border, 0);
+        PB_CUDA(cudaDeviceSynchronize());
+        CSpline_Calibration c;
+        c.shape[0] = os[0];
+        c.shape[1] = os[1];
+        c.shape[2] = os[2];
+        c.z_min = h.zmin;
+        c.z_max = h.zmax;
+        c.coefs = nullptr;
+        return make_spline(roisize, &c, nullptr, mode, ctx, dc.as<float>());
+        }, (Estimator*)nullptr);
+}
+
+void CSpline_Compute(const int* shape, const float* data, float* splineCoefs, int border) {
+    guarded_void([&]() {
+        if (!shape || !data || !splineCoefs) throw Error("CSpline_Compute: null argument");
+        const size_t nvox = (size_t)shape[0] * shape[1] * shape[2];
+        const int o0 = shape[0] - 3 + 2 * border, o1 = shape[1] - 3 + 2 * border, o2 = shape[2] - 3 + 2 * border;
+        if (o0 <= 0 || o1 <= 0 || o2 <= 0) throw Error("CSpline_Compute: z-stack too small");
+        const size_t nout = (size_t)o0 * o1 * o2 * 64;
+        DevBuf dd, dc;
+        dd.ensure(sizeof(float) * nvox);
+        dc.ensure(sizeof(float) * nout);
+        PB_CUDA(cudaMemcpy(dd.p, data, sizeof(float) * nvox, cudaMemcpyHostToDevice));
+        spline_compute_device(shape, dd.as<float>(), dc.as<float>(), border, 0);
+        PB_CUDA(cudaMemcpy(splineCoefs, dc.p, sizeof(float) * nout, cudaMemcpyDeviceToHost));
+        });
+}
+
+void CSpline_Evaluate(const int* shape, const float* splineCoefs, const float* shift, int border, float* values) {
+    guarded_void([&]() {
+        if (!shape || !splineCoefs || !shift || !values) throw Error("CSpline_Evaluate: null argument");
+        const size_t ncoef = (size_t)shape[0] * shape[1] * shape[2] * 64;
+        const int n0 = shape[0] - 2 * border, n1 = shape[1] - 2 * border, n2 = shape[2] - 2 * border;
+        if (n0 <= 0 || n1 <= 0 || n2 <= 0) throw Error("CSpline_Evaluate: border too large");
+        const size_t nout = (size_t)n0 * n1 * n2 * 4;
+        // subpixel position: d = -shift - int(-shift)  (CubicSplinePSF.cu:215)
+        float d[3];
+        for (int i = 0; i < 3; i++) {
+            const float ms = -shift[i];
+            d[i] = ms - (float)(int)ms;
+        }
+        DevBuf dc, dv;
+        dc.ensure(sizeof(float) * ncoef);
+        dv.ensure(sizeof(float) * nout);
+        PB_CUDA(cudaMemcpy(dc.p, splineCoefs, sizeof(float) * ncoef, cudaMemcpyHostToDevice));
+        const long long total = (long long)n0 * n1 * n2;
+        const int grid = (int)std::min<long long>((total + 127) / 128, 65535);
+        spline_evaluate_kernel<<<grid, 128>>>(dc.as<float>(), shape[0], shape[1], shape[2], d[0], d[1], d[2],
+                                              shift[0], shift[1], shift[2], border, dv.as<float>());
+        PB_CUDA(cudaGetLastError());
+        g_launches++;
+        PB_CUDA(cudaMemcpy(values, dv.p, sizeof(float) * nout, cudaMemcpyDeviceToHost));
+        });
+}
+
+void Estimator_Delete(Estimator* e) {
+    if (!e) return;
+    detach(e);
+    delete e;
+}
+
+const char* Estimator_ParamFormat(Estimator* e) { return e ? e->format.c_str() : ""; }
+
+void Estimator_GetProperties(Estimator* e, EstimatorProperties* p) {
+    if (!e || !p) return;
+    p->numParams = e->K;
+    p->sampleCount = e->npix();
+    p->numDiag = 0;
+    p->numConst = e->numconst;
+    p->sampleIndexDims = 2;
+}
+
+void Estimator_SampleDims(Estimator* e, int* dims) {
+    if (!e || !dims) return;
+    dims[0] = e->desc.roisize;
+    dims[1] = e->desc.roisize;
+}
+
+void Estimator_GetParamLimits(Estimator* e, ParamLimit* limits) {
+    if (!e || !limits) return;
+    for (int i = 0; i < e->K; i++) limits[i] = e->limits[i];
+}
+
+void Estimator_SetLMParams(Estimator* e, const LMParams* p) {
+    if (!e || !p) return;
+    std::lock_guard<std::mutex> g(e->mtx);
+    e->lm = *p;
+}
+
+void Estimator_GetLMParams(Estimator* e, LMParams* p) {
+    if (!e || !p) return;
+    *p = e->lm;
+}
+
+void Estimator_ComputeExpectedValue(Estimator* e, int numspots, const float* params, const float* constants,
+                                    const int*, float* ev) {
+    if (numspots == 0) return;
+    guarded_void([&]() {check_estimator(e); if (numspots < 0 || !params || !ev) throw Error("ExpectedValue: bad arguments");
+           host_eval(e, numspots, params, constants, ev, nullptr);});
+}
+
+void Estimator_ComputeDerivatives(Estimator* e, int numspots, const float* params, const float* constants,
+                                  const int*, float* psf_deriv, float* ev) {
+    if (numspots == 0) return;
+    guarded_void([&]() {check_estimator(e); if (numspots < 0 || !params) throw Error("Derivatives: bad arguments");
+           host_eval(e, numspots, params, constants, ev, psf_deriv);});
+}
+
+void Estimator_Estimate(Estimator* e, int numspots, const float* sample, const float* constants, const int*,
+                        const float* initial, float* params, float* diagnostics, int* iterations, float* trace,
+                        int traceBufLen) {
+    (void)diagnostics;
+    if (numspots == 0) return;
+    guarded_void([&]() {check_estimator(e); if (numspots < 0 || !sample || !params) throw Error("Estimate: bad arguments");
+           host_fit(e, numspots, sample, constants, initial, params, iterations, trace, traceBufLen, nullptr, nullptr,
+                    0);
+           });
+}
+
+void Estimator_ChiSquareAndCRLB(Estimator* e, const float* params, const float* sample, const float* constants,
+                                const int*, int numspots, float* crlb, float* chisq) {
+    if (numspots == 0) return;
+    guarded_void([&]() {check_estimator(e); if (numspots < 0 || !params || !crlb) throw Error("ChiSquareAndCRLB: bad arguments");
+           host_fit(e, numspots, sample, constants, params, nullptr, nullptr, nullptr, 0, crlb, chisq,
+                    FIT_CRLB_ONLY);
+           });
+}
+
+void PB200_EstimateCRLB(Estimator* e, int numspots, const float* sample, const float* constants,
+                        const float* initial, float* params, int* iterations, float* crlb, float* chisq) {
+    if (numspots == 0) return;
+    guarded_void([&]() {check_estimator(e); if (numspots < 0 || !sample || !params) throw Error("EstimateCRLB: bad arguments");
+           host_fit(e, numspots, sample, constants, initial, params, iterations, nullptr, 0, crlb, chisq, 0);
+           });
+}
+
+void PB200_EstimateDevice(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                          const float* d_initial, float* d_params, int* d_iterations, float* d_trace,
+                          int traceBufLen, float* d_crlb, float* d_chisq, void* stream) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e); if (numspots < 0 || !d_sample || !d_params) throw Error("EstimateDevice: bad arguments");
+        if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+        FitArgs a{}; a.smp = d_sample; a.consts = d_constants; a.initial = d_initial; a.params = d_params;
+        a.iterations = d_iterations; a.trace = traceBufLen > 0 ? d_trace : nullptr;
+        a.traceLen = traceBufLen > 0 && d_trace ? traceBufLen : 0; a.crlb = d_crlb; a.chisq = d_chisq;
+        a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda; a.flags = 0;
+        fit_launcher(e->desc.model, e->lanes_for())(e->desc, a, e->threads, (cudaStream_t)stream);});
+}
+
+void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
+                               float* d_ev, float* d_deriv, void* stream) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e); if (numspots < 0 || !d_params) throw Error("ExpectedValueDevice: bad arguments");
+        if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+        int G = e->lanes_for(); if (G < 8) G = 8;
+        eval_launcher(e->desc.model, G)(e->desc, d_params, d_constants, d_ev, d_deriv, numspots, 256,
+                                        (cudaStream_t)stream);});
+}
+
+void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_params, const float* d_sample,
+                                  const float* d_constants, float* d_crlb, float* d_chisq, void* stream) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e); if (numspots < 0 || !d_params || !d_crlb) throw Error("ChiSquareAndCRLBDevice: bad arguments");
+        if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+        FitArgs a{}; a.smp = d_sample; a.consts = d_constants; a.initial = d_params; a.params = nullptr;
+        a.crlb = d_crlb; a.chisq = d_chisq; a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda;
+        a.flags = FIT_CRLB_ONLY;
+        fit_launcher(e->desc.model, e->lanes_for())(e->desc, a, e->threads, (cudaStream_t)stream);});
+}
+
+int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {
+    if (!e) return -1;
+    if (lanesPerRoi != 0 && lanesPerRoi != 4 && lanesPerRoi != 8 && lanesPerRoi != 16 && lanesPerRoi != 32) return -1;
+    if (threadsPerBlock < 64 || threadsPerBlock > 256 || (threadsPerBlock & 31)) return -1;
+    std::lock_guard<std::mutex> g(e->mtx);
+    e->lanes = lanesPerRoi;
+    e->threads = threadsPerBlock;
+    return 0;
+}
+
+void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock) {
+    if (!e) return;
+    if (lanesPerRoi) *lanesPerRoi = e->lanes_for();
+    if (threadsPerBlock) *threadsPerBlock = e->threads;
+}
+
+int PB200_ModelInfo(Estimator* e, int* roisize) {
+    if (!e) return -1;
+    if (roisize) *roisize = e->desc.roisize;
+    return e->desc.model;
+}
+
+// ---- loader-time exports ----
+int CudaGetNumDevices(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+bool CudaSetDevice(int index) { return cudaSetDevice(index) == cudaSuccess; }
+
+bool CudaGetDeviceInfo(int index, int* numMultiprocessors, char* name, int namelen) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, index) != cudaSuccess) return false;
+    if (numMultiprocessors) *numMultiprocessors = prop.multiProcessorCount;
+    if (name && namelen > 0) {
+        strncpy(name, prop.name, namelen - 1);
+        name[namelen - 1] = 0;
+    }
+    return true;
+}
+
+void CudaGetMemoryUse(uint64_t* pinnedBytes, uint64_t* devicePitchedBytes, uint64_t* deviceBytes,
+                      uint64_t* pitchedNumAllocs) {
+    size_t freeB = 0, totalB = 0;
+    cudaMemGetInfo(&freeB, &totalB);
+    if (pinnedBytes) *pinnedBytes = 0;
+    if (devicePitchedBytes) *devicePitchedBytes = 0;
+    if (deviceBytes) *deviceBytes = totalB - freeB;
+    if (pitchedNumAllocs) *pitchedNumAllocs = 0;
+}
+
+void SetDebugPrintCallback(int (*cb)(const char* msg)) { g_debugPrint = cb; }
+void SetDebugImageCallback(void (*cb)(int, int, int, const float*, const char*)) { g_debugImage = cb; }
+void ShowDebugImage(int w, int h, int numImg, const float* data, const char* title) {
+    if (g_debugImage) g_debugImage(w, h, numImg, data, title);
+}
+
+static void not_provided(const char* fn) {
+    t_lastError = std::string(fn) + " is not provided by photonpy_b200";
+    debug_printf("%s\n", t_lastError.c_str());
+}
+void FFT(const void*, void*, int, int, int) { not_provided("FFT"); }
+void FFT2(const void*, void*, int, int, int, int) { not_provided("FFT2"); }
+void DrawROIs(float*, int, int, const float*, int, int, const int*) { not_provided("DrawROIs"); }
+void Gauss2D_Draw(double*, int, int, float*, int, float) { not_provided("Gauss2D_Draw"); }
+void Gauss2D_EstimateIntensityBg(const float*, float*, float*, int, const float*, const int*, const float*, int, int,
+                                 int) {
+    not_provided("Gauss2D_EstimateIntensityBg");
+}
+Estimator* Gauss2D_CreatePSF_XYITiltedBg(int, bool, Context*) {
+    not_provided("Gauss2D_CreatePSF_XYITiltedBg");
+    return nullptr;
+}
+Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int, float, float, bool, Context*) {
+    not_provided("Gauss2D_CreatePSF_XYITiltedBgSigmaXY");
+    return nullptr;
+}
+
+}  // extern "C"

@@ -1,0 +1,486 @@
+// Batched Levenberg-Marquardt Poisson-MLE fit, Fisher/CRLB and model-evaluation kernels.
+//
+// Work decomposition (sm_100a): a group of G lanes (G = 4, 8, 16 or 32; several groups
+// per warp for small ROIs) owns one ROI at a time. The ROI's pixels are staged in shared
+// memory with coalesced loads, the separable per-iteration table is built cooperatively,
+// each lane accumulates the Poisson gradient/Hessian terms of its pixels in registers and
+// a register butterfly (shfl.xor inside the group) reduces them. Every lane of the group
+// then runs the tiny damped K x K Cholesky solve redundantly, so the decision to stop is
+// identical on all lanes without a broadcast.
+//
+// The loop is flat: one trip = one LM iteration (or the Fisher pass) for every group of
+// the warp, and a group whose ROI has finished loads its next ROI at the top of the next
+// trip. Groups never wait for their warp-mates' ROIs to converge.
+//
+// Reference semantics kept (Estimators/Estimation.h:104-134, 194-251):
+//  * sample clamped at 1e-6, mu clamped at 1e-6, x_f2 = (x*invmu)*invmu, beta -= (1 - x*invmu)*J;
+//  * damping lambda>0: alpha_kk += lambda * sum_j alpha_jk^2; lambda<0: alpha_kk -= lambda;
+//  * Cholesky fails (LM stops) only on an exactly-zero pivot (SolveMatrix.h:107-125);
+//  * theta += step, model CheckLimits, stop when i > 0 and every |delta_k| <= StopLimit(k);
+//  * iterations = i + 1 (maxIterations + 1 when the cap is hit); trace[i] = theta at the
+//    start of iteration i for i < traceBufLen.
+// Changes by design: pixel sums are reduced in a tree instead of sequentially; a Cholesky
+// pivot that loses more than 6 decimal digits (0 < v < 1e-6 * a_kk, or v < 0) is re-solved in
+// FP64; the Fisher matrix is accumulated in FP32 and inverted in FP64 (LUP with partial
+// pivoting and the reference's 1e-9 tolerance, Estimation.h:63-102, SolveMatrix.h:411-452).
+#pragma once
+#include "models.cuh"
+
+namespace pb200 {
+
+enum FitFlags : int {
+    FIT_CRLB_ONLY = 1,  // skip LM: params come from `initial`, compute Fisher/CRLB/chi^2 only
+};
+
+struct FitArgs {
+    const float* smp;      // [n][npix] (may be null with FIT_CRLB_ONLY: no chi-square)
+    const float* consts;   // [n][numconst] or null
+    const float* initial;  // [n][K] or null (centre-of-mass start)
+    float* params;         // [n][K]
+    int* iterations;       // [n] or null
+    float* trace;          // [n][traceLen][K] or null
+    int traceLen;
+    float* crlb;           // [n][K] or null (no Fisher pass)
+    float* chisq;          // [n] or null
+    int* diag;             // [n] or null: bit 0 = an FP64 re-solve happened
+    int n;
+    int maxIter;
+    float lambda;
+    int smemStride;        // floats of shared memory per group
+    int flags;
+};
+
+__host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+    if (G == 32) return 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    return ((1u << (G & 31)) - 1u) << (lane & ~(unsigned)(G - 1));
+}
+
+template <int G>
+__device__ __forceinline__ float group_sum(float v, unsigned mask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+// Shared-memory scratch a group needs besides its pixels: the model table, or the FP64
+// Fisher/LM work area (2*K*K doubles + K doubles), whichever is larger.
+template <class M>
+__host__ __device__ constexpr int group_scratch_floats(int R) {
+    return M::table_floats(R) > (4 * M::K * M::K + 2 * M::K + 4) ? M::table_floats(R)
+                                                                   : (4 * M::K * M::K + 2 * M::K + 4);
+}
+
+template <class M>
+__host__ __device__ constexpr int group_smem_floats(int R) {
+    return round_up(round_up(R * R, 4) + group_scratch_floats<M>(R), 32) + 8;
+}
+
+// FP64 LUP inverse with the reference's 1e-9 tolerance (SolveMatrix.h:219-318, 344-392),
+// run by one lane on a shared-memory work area. A[K*K] is overwritten, IA[K*K] receives the
+// inverse. Returns false when the matrix is degenerate (the reference then reports Inf).
+__device__ __noinline__ bool invert_fp64_smem(int K, double* A, double* IA) {
+    int P[8];
+    for (int i = 0; i <= K; i++) P[i] = i;
+    for (int i = 0; i < K; i++) {
+        double maxA = 0.0;
+        int imax = i;
+        for (int k = i; k < K; k++) {
+            const double v = fabs(A[k * K + i]);
+            if (v > maxA) { maxA = v; imax = k; }
+        }
+        if (maxA < (double)1e-9f) return false;
+        if (imax != i) {
+            const int tp = P[i]; P[i] = P[imax]; P[imax] = tp;
+            for (int j = 0; j < K; j++) {
+                const double t = A[i * K + j]; A[i * K + j] = A[imax * K + j]; A[imax * K + j] = t;
+            }
+            P[K]++;
+        }
+        for (int j = i + 1; j < K; j++) {
+            A[j * K + i] /= A[i * K + i];
+            for (int k = i + 1; k < K; k++) A[j * K + k] -= A[j * K + i] * A[i * K + k];
+        }
+    }
+    for (int j = 0; j < K; j++) {
+        for (int i = 0; i < K; i++) {
+            double v = (P[i] == j) ? 1.0 : 0.0;
+            for (int k = 0; k < i; k++) v -= A[i * K + k] * IA[k * K + j];
+            IA[i * K + j] = v;
+        }
+        for (int i = K - 1; i >= 0; i--) {
+            double v = IA[i * K + j];
+            for (int k = i + 1; k < K; k++) v -= A[i * K + k] * IA[k * K + j];
+            IA[i * K + j] = v / A[i * K + i];
+        }
+    }
+    return true;
+}
+
+// FP64 Cholesky solve of the damped system S x = b (lower triangle of S used), one lane,
+// shared-memory work area. Returns false on an exactly-zero pivot.
+__device__ __noinline__ bool cholesky_solve_fp64_smem(int K, const float* S, const float* b, double* D, double* y,
+                                                      float* x) {
+    for (int k = 0; k < K; ++k) {
+        double sum = 0.0;
+        for (int p = 0; p < k; ++p) sum += D[k * K + p] * D[k * K + p];
+        const double v = (double)S[k * K + k] - sum;
+        if (v == 0.0) return false;
+        D[k * K + k] = sqrt(v);
+        for (int i = k + 1; i < K; ++i) {
+            double s2 = 0.0;
+            for (int p = 0; p < k; ++p) s2 += D[i * K + p] * D[k * K + p];
+            D[i * K + k] = ((double)S[i * K + k] - s2) / D[k * K + k];
+        }
+    }
+    for (int i = 0; i < K; ++i) {
+        double sum = 0.0;
+        for (int k = 0; k < i; ++k) sum += D[i * K + k] * y[k];
+        y[i] = ((double)b[i] - sum) / D[i * K + i];
+    }
+    for (int i = K - 1; i >= 0; --i) {
+        double sum = 0.0;
+        for (int k = i + 1; k < K; ++k) sum += D[k * K + i] * (double)x[k];
+        // keep the double solution in y[] while x[] still holds float copies for later rows
+        const double xi = (y[i] - sum) / D[i * K + i];
+        y[i] = xi;
+        x[i] = (float)xi;
+    }
+    // recompute with full double precision for rows that used float copies
+    for (int i = K - 1; i >= 0; --i) x[i] = (float)y[i];
+    return true;
+}
+
+// Damped LM step in FP32 (reference algorithm, Estimation.h:213-228, SolveMatrix.h:107-163).
+// Returns 0 on an exactly-zero pivot (reference failure: LM stops), 1 on success, 2 when a
+// pivot lost more than six decimal digits (0 < v <= 1e-6 a_kk, or v < 0): the caller then
+// re-solves in FP64. On return S holds the damped matrix (full, row-major).
+template <int K>
+__device__ __forceinline__ int lm_solve_fp32(const float (&acc)[K * (K + 1) / 2 + K + 1], float lambda,
+                                             float (&S)[K * K], float (&step)[K]) {
+    {
+        int q = 0;
+#pragma unroll
+        for (int i = 0; i < K; i++)
+#pragma unroll
+            for (int j = i; j < K; j++) {
+                S[i * K + j] = acc[q];
+                S[j * K + i] = acc[q];
+                q++;
+            }
+    }
+    float diag[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        if (lambda < 0.0f) {
+            diag[k] = S[k * K + k] - lambda;
+        } else {
+            float s = 0.0f;
+#pragma unroll
+            for (int j = 0; j < K; j++) s += S[j * K + k] * S[j * K + k];
+            diag[k] = S[k * K + k] + s * lambda;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) S[k * K + k] = diag[k];
+    float D[K * K];
+    bool weak = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int p = 0; p < k; ++p) sum += D[k * K + p] * D[k * K + p];
+        const float v = S[k * K + k] - sum;
+        if (v == 0.0f) return 0;
+        if (!(v > 1e-6f * S[k * K + k])) weak = true;  // also catches v < 0 and NaN
+        D[k * K + k] = sqrtf(v);
+#pragma unroll
+        for (int i = k + 1; i < K; ++i) {
+            float s2 = 0.0f;
+#pragma unroll
+            for (int p = 0; p < k; ++p) s2 += D[i * K + p] * D[k * K + p];
+            D[i * K + k] = (S[i * K + k] - s2) / D[k * K + k];
+        }
+    }
+    if (weak) return 2;
+    float y[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = 0; k < i; ++k) sum += D[i * K + k] * y[k];
+        y[i] = (acc[K * (K + 1) / 2 + i] - sum) / D[i * K + i];
+    }
+#pragma unroll
+    for (int i = K - 1; i >= 0; --i) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = i + 1; k < K; ++k) sum += D[k * K + i] * step[k];
+        step[i] = (y[i] - sum) / D[i * K + i];
+    }
+    return 1;
+}
+
+template <class M, int G>
+__global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitArgs a) {
+    constexpr int K = M::K;
+    constexpr int NA = K * (K + 1) / 2;
+    constexpr int NACC = NA + K + 1;
+    constexpr int NC = model_num_consts(M::kId);
+    enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3 };
+    extern __shared__ __align__(16) float sm[];
+
+    const int lane = threadIdx.x & (G - 1);
+    const int gib = threadIdx.x / G;
+    const int gpb = blockDim.x / G;
+    const unsigned mask = group_mask<G>();
+    const int R = d.roisize;
+    const int npix = R * R;
+    float* spix = sm + gib * a.smemStride;
+    float* tab = spix + round_up(npix, 4);  // model table, or FP64 work area after a reduction
+    const int gstride = gridDim.x * gpb;
+    const int dx = G % R, dy = G / R;
+    const int x0 = lane % R, y0 = lane / R;
+    const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
+    const bool haveSmp = a.smp != nullptr;
+    const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
+
+    int roi = blockIdx.x * gpb + gib;
+    float th[K];
+    float cs[NC > 0 ? NC : 1];
+    int it = 0;
+    int mode = MODE_LOAD;
+    bool rescuedAny = false;
+
+    while (true) {
+        if (mode == MODE_LOAD) {
+            // ---- load the next ROI into shared memory and set the start parameters ----
+            if (roi >= a.n) break;
+            __syncwarp(mask);  // previous ROI's readers are done with spix/tab
+            const float* src = haveSmp ? a.smp + (size_t)roi * npix : nullptr;
+            if (haveSmp) {
+                if (vec4) {
+                    const float4* s4 = reinterpret_cast<const float4*>(src);
+                    float4* d4 = reinterpret_cast<float4*>(spix);
+                    for (int i = lane; i < (npix >> 2); i += G) d4[i] = __ldcs(s4 + i);
+                } else {
+                    for (int i = lane; i < npix; i += G) spix[i] = __ldcs(src + i);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NC; c++) cs[c] = a.consts[(size_t)roi * NC + c];
+            if (a.initial) {
+#pragma unroll
+                for (int k = 0; k < K; k++) th[k] = a.initial[(size_t)roi * K + k];
+            } else {
+                __syncwarp(mask);
+                // centre of mass (Estimation.h:336-352); exact for integer-valued samples
+                float sx = 0.0f, sy = 0.0f, s = 0.0f;
+                int x = x0, y = y0;
+                for (int p = lane; p < npix; p += G) {
+                    const float v = spix[p];
+                    sx += (float)x * v;
+                    sy += (float)y * v;
+                    s += v;
+                    x += dx;
+                    y += dy;
+                    if (x >= R) { x -= R; y++; }
+                }
+                sx = group_sum<G>(sx, mask);
+                sy = group_sum<G>(sy, mask);
+                s = group_sum<G>(s, mask);
+                M::initial(d, __fdiv_rn(sx, s), __fdiv_rn(sy, s), s, th);
+            }
+            it = 0;
+            rescuedAny = false;
+            if (fisherOnly) mode = MODE_FISHER;
+            else if (a.maxIter <= 0) mode = a.crlb ? MODE_FISHER : MODE_SKIP;  // start value, iterations = 1
+            else mode = MODE_LM;
+        }
+
+        if (mode != MODE_SKIP) {
+            if (mode == MODE_LM && a.trace && lane == 0 && it < a.traceLen) {
+#pragma unroll
+                for (int k = 0; k < K; k++) a.trace[((size_t)roi * a.traceLen + it) * K + k] = th[k];
+            }
+            // ---- per-iteration table, then the pixel pass ----
+            M m;
+            m.begin(d, th, cs);
+            __syncwarp(mask);
+            m.build_table(d, tab, lane, G);
+            __syncwarp(mask);
+
+            float acc[NACC];
+#pragma unroll
+            for (int q = 0; q < NACC; q++) acc[q] = 0.0f;
+            const bool lm = (mode == MODE_LM);
+            int x = x0, y = y0;
+            for (int p = lane; p < npix; p += G) {
+                float mu, J[K];
+                m.pixel(d, tab, x, y, mu, J);
+                const float s = haveSmp ? spix[p] : 0.0f;
+                float w;
+                if (lm) {
+                    // ComputeLevMarAlphaBeta (Estimation.h:109-128)
+                    const float sv = s < 1e-6f ? 1e-6f : s;
+                    const float muc = mu > 1e-6f ? mu : 1e-6f;
+                    const float invmu = __frcp_rn(muc);
+                    const float t = __fmul_rn(sv, invmu);
+                    w = __fmul_rn(t, invmu);
+                    const float bf = __fsub_rn(1.0f, t);
+#pragma unroll
+                    for (int k = 0; k < K; k++) acc[NA + k] -= bf * J[k];
+                } else {
+                    // ComputeChiSquareAndCRLB (Estimation.h:76-95)
+                    const float mu8 = fmaxf(1e-8f, mu);
+                    w = __frcp_rn(mu8);
+                    if (haveSmp) {
+                        const float e = s - mu8;
+                        acc[NACC - 1] += __fdiv_rn(e * e, mu8);
+                    }
+                }
+                int q = 0;
+#pragma unroll
+                for (int i = 0; i < K; i++) {
+                    const float wi = J[i] * w;
+#pragma unroll
+                    for (int j = i; j < K; j++) acc[q++] += wi * J[j];
+                }
+                x += dx;
+                y += dy;
+                if (x >= R) { x -= R; y++; }
+            }
+#pragma unroll
+            for (int q = 0; q < NACC; q++) acc[q] = group_sum<G>(acc[q], mask);
+
+            if (lm) {
+                float S[K * K], step[K];
+                int rc = lm_solve_fp32<K>(acc, a.lambda, S, step);
+                if (rc == 2) {
+                    // FP64 re-solve of the same damped system on lane 0, broadcast via smem
+                    __syncwarp(mask);
+                    double* D = reinterpret_cast<double*>(tab);
+                    double* yv = D + K * K;
+                    float* xs = reinterpret_cast<float*>(yv + K);
+                    float* Ss = xs + K;
+                    float* bs = Ss + K * K;
+                    if (lane == 0) {
+#pragma unroll
+                        for (int q = 0; q < K * K; q++) Ss[q] = S[q];
+#pragma unroll
+                        for (int q = 0; q < K; q++) bs[q] = acc[NA + q];
+                        const bool ok = cholesky_solve_fp64_smem(K, Ss, bs, D, yv, xs);
+                        Ss[0] = ok ? 1.0f : 0.0f;
+                    }
+                    __syncwarp(mask);
+                    rc = Ss[0] != 0.0f ? 1 : 0;
+#pragma unroll
+                    for (int q = 0; q < K; q++) step[q] = xs[q];
+                    if (rc) rescuedAny = true;
+                    __syncwarp(mask);
+                }
+                bool done;
+                if (rc == 0) {
+                    done = true;  // the reference breaks out with iterations = i + 1
+                } else {
+                    float last[K];
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        last[k] = th[k];
+                        th[k] = th[k] + step[k];
+                    }
+                    M::check_limits(d, th);
+                    bool small = true;
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        if (fabsf(last[k] - th[k]) > M::stop_limit(k)) small = false;
+                    done = (it > 0 && small);
+                    if (!done) {
+                        it++;
+                        if (it >= a.maxIter) {
+                            done = true;
+                            it = a.maxIter;  // iterations = maxIterations + 1
+                        }
+                    }
+                }
+                if (!done) continue;
+                if (a.crlb) {
+                    mode = MODE_FISHER;
+                    continue;
+                }
+            } else {
+                // ---- Fisher pass: FP64 LUP inverse on lane 0 ----
+                __syncwarp(mask);
+                if (lane == 0) {
+                    double* F = reinterpret_cast<double*>(tab);
+                    double* IF = F + K * K;
+                    int q = 0;
+#pragma unroll
+                    for (int i = 0; i < K; i++)
+#pragma unroll
+                        for (int j = i; j < K; j++) {
+                            F[i * K + j] = (double)acc[q];
+                            F[j * K + i] = (double)acc[q];
+                            q++;
+                        }
+                    const bool okInv = invert_fp64_smem(K, F, IF);
+                    for (int k = 0; k < K; k++)
+                        a.crlb[(size_t)roi * K + k] =
+                            okInv ? (float)sqrt(IF[k * (K + 1)]) : __int_as_float(0x7f800000);
+                    if (a.chisq) a.chisq[roi] = acc[NACC - 1];
+                }
+            }
+        }
+        // ---- ROI finished: write results, move to the next ROI ----
+        if (lane == 0 && !fisherOnly) {
+#pragma unroll
+            for (int k = 0; k < K; k++) a.params[(size_t)roi * K + k] = th[k];
+            if (a.iterations) a.iterations[roi] = it + 1;
+            if (a.diag) a.diag[roi] = rescuedAny ? 1 : 0;
+        }
+        roi += gstride;
+        mode = MODE_LOAD;
+    }
+}
+
+// ExpectedValue / Derivatives (Estimation.h:159-181; layouts ev[n][H][W], deriv[n][K][H][W]).
+template <class M, int G>
+__global__ void __launch_bounds__(256) eval_kernel(const ModelDesc d, const float* __restrict__ params,
+                                                   const float* __restrict__ consts, float* __restrict__ ev,
+                                                   float* __restrict__ deriv, int n, int smemStride) {
+    constexpr int K = M::K;
+    constexpr int NC = model_num_consts(M::kId);
+    extern __shared__ __align__(16) float sm[];
+    const int lane = threadIdx.x & (G - 1);
+    const int gib = threadIdx.x / G;
+    const int gpb = blockDim.x / G;
+    const unsigned mask = group_mask<G>();
+    const int R = d.roisize, npix = R * R;
+    float* tab = sm + gib * smemStride;
+    for (int roi = blockIdx.x * gpb + gib; roi < n; roi += gridDim.x * gpb) {
+        float th[K], cs[NC > 0 ? NC : 1];
+#pragma unroll
+        for (int k = 0; k < K; k++) th[k] = params[(size_t)roi * K + k];
+#pragma unroll
+        for (int c = 0; c < NC; c++) cs[c] = consts[(size_t)roi * NC + c];
+        M m;
+        m.begin(d, th, cs);
+        __syncwarp(mask);
+        m.build_table(d, tab, lane, G);
+        __syncwarp(mask);
+        for (int p = lane; p < npix; p += G) {
+            float mu, J[K];
+            m.pixel(d, tab, p % R, p / R, mu, J);
+            if (ev) __stcs(ev + (size_t)roi * npix + p, mu);
+            if (deriv) {
+#pragma unroll
+                for (int k = 0; k < K; k++) __stcs(deriv + ((size_t)roi * K + k) * npix + p, J[k]);
+            }
+        }
+    }
+}
+
+}  // namespace pb200

@@ -1,0 +1,377 @@
+// Device-side PSF models for the batched Poisson-MLE estimator.
+//
+// Each model follows the per-pixel arithmetic of photonpy's models, operation by
+// operation, with explicit round-to-nearest intrinsics so nvcc does not fuse the
+// reference's separate multiplies and adds:
+//   Gauss2D XYIBg / ConstSigma   Estimators/Gaussian/GaussianPSFModels.h:35-227
+//   Gauss2D XYIBgSigma           Estimators/Gaussian/GaussianPSFModels.h:308-387
+//   Gauss2D XYIBgSigmaXY         Estimators/Gaussian/GaussianPSFModels.h:391-471
+//   Gauss2D XYZIBg (astigmatic)  Estimators/Gaussian/GaussianPSFModels.h:636-751
+//   CSpline XYZIBg (flat bg)     Estimators/CSpline/CubicSplinePSFModels.h:14-154
+//
+// B200 layout: the reference recomputes erf/exp for every pixel although they depend
+// only on the column (x) or the row (y). Here a group of lanes first builds a small
+// per-ROI-iteration table in shared memory (2R entries of 4 floats for the Gaussians,
+// the 4x64 power-basis vectors for the spline), then each lane evaluates its pixels
+// from the table. Table values are bit-identical to what the reference computes per
+// pixel, so the per-pixel mu and Jacobian keep the reference's rounding (up to the
+// last-ulp differences between CUDA's and glibc's erff/expf).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pb200 {
+
+enum ModelId : int {
+    MODEL_XYIBG = 0,
+    MODEL_XYIBG_CONSTSIGMA = 1,
+    MODEL_XYIBG_SIGMA = 2,
+    MODEL_XYIBG_SIGMAXY = 3,
+    MODEL_XYZIBG = 4,
+    MODEL_CSPLINE = 5,
+    MODEL_COUNT = 6
+};
+
+// Plain-old-data description of one estimator instance, passed by value to kernels.
+struct ModelDesc {
+    int model;
+    int roisize;
+    float sigma[2];       // fixed sigma (XYIBg) or initial sigma(s) (Sigma / SigmaXY)
+    float astig_x[5];     // s0, gamma, d, A, B  (B = 0 reproduces the reference's 4-term form)
+    float astig_y[5];
+    float minz, maxz;     // astig z clamp
+    int spline_shape[3];  // Nz, Ny, Nx of the coefficient grid
+    float spline_zmin, spline_zmax;
+    const float* coefs;   // device, [Nz][Ny][Nx][64]
+};
+
+__host__ __device__ constexpr int model_num_params(int m) {
+    return (m == MODEL_XYIBG || m == MODEL_XYIBG_CONSTSIGMA) ? 4 : (m == MODEL_XYIBG_SIGMAXY ? 6 : 5);
+}
+__host__ __device__ constexpr int model_num_consts(int m) { return m == MODEL_XYIBG_CONSTSIGMA ? 2 : 0; }
+
+// MATH_PI in the reference is the float literal 3.141592653589793f (MathUtils.h:95).
+#define PB_PI 3.141592653589793f
+#define MUL(a, b) __fmul_rn((a), (b))
+#define ADD(a, b) __fadd_rn((a), (b))
+#define SUB(a, b) __fsub_rn((a), (b))
+#define DIV(a, b) __fdiv_rn((a), (b))
+
+// clamp(f,a,b) = fmaxf(a, fminf(f, b)), CudaMath.h:1152-1155 (NaN maps to b).
+__device__ __forceinline__ float pb_clamp(float f, float a, float b) { return fmaxf(a, fminf(f, b)); }
+
+// Gauss2D_Border = 1.5f; upper x/y limit = (R - 1.5f) - 1 (GaussianPSFModels.h:55-56).
+__device__ __forceinline__ float gauss_xy_max(int R) { return SUB(SUB((float)R, 1.5f), 1.0f); }
+
+// ---------------------------------------------------------------------------------------
+// Gaussian models: table = x-terms [R][4] then y-terms [R][4].
+// ---------------------------------------------------------------------------------------
+template <int MID>
+struct GaussModel {
+    static constexpr int K = model_num_params(MID);
+    static constexpr int kId = MID;
+    static __host__ __device__ constexpr int table_floats(int R) { return 8 * R; }
+
+    // per ROI-iteration scalars
+    float tx, ty, tI, tbg;
+    float cx1, cx2, cy1, cy2;  // OneOverSqrt2SigmaX, OneOverSqrt2PiSigmaX, ... (Y)
+    float invSqrtPi;
+    float sigx, sigy;          // astig: sigma_x(z), sigma_y(z)
+    float dsxz, dsyz;          // astig: dsigma/dz
+
+    __device__ __forceinline__ void begin(const ModelDesc& d, const float* th, const float* consts) {
+        tx = th[0];
+        ty = th[1];
+        const float s2pi = __fsqrt_rn(MUL(2.0f, PB_PI));
+        const float s2 = __fsqrt_rn(2.0f);
+        if (MID == MODEL_XYZIBG) {
+            tI = th[3];
+            tbg = th[4];
+            const float tz = th[2];
+            const float s0x = d.astig_x[0], gx = d.astig_x[1], dx = d.astig_x[2], Ax = d.astig_x[3], Bx = d.astig_x[4];
+            const float s0y = d.astig_y[0], gy = d.astig_y[1], dy = d.astig_y[2], Ay = d.astig_y[3], By = d.astig_y[4];
+            const float dy2 = MUL(dy, dy), dx2 = MUL(dx, dx);
+            const float dy4 = MUL(dy2, dy2), dx4 = MUL(dx2, dx2);
+            const float tzx = SUB(tz, gx), tzx2 = MUL(tzx, tzx), tzx3 = MUL(tzx2, tzx), tzx4 = MUL(tzx2, tzx2);
+            const float tzy = SUB(tz, gy), tzy2 = MUL(tzy, tzy), tzy3 = MUL(tzy2, tzy), tzy4 = MUL(tzy2, tzy2);
+            // 1 + tz^2/d^2 + A tz^3/d^2 (+ B tz^4/d^4, which adds exactly 0 when B == 0)
+            const float qx = ADD(ADD(ADD(1.0f, DIV(tzx2, dx2)), DIV(MUL(Ax, tzx3), dx2)), DIV(MUL(Bx, tzx4), dx4));
+            const float qy = ADD(ADD(ADD(1.0f, DIV(tzy2, dy2)), DIV(MUL(Ay, tzy3), dy2)), DIV(MUL(By, tzy4), dy4));
+            const float sqx = __fsqrt_rn(qx), sqy = __fsqrt_rn(qy);
+            sigx = MUL(s0x, sqx);
+            sigy = MUL(s0y, sqy);
+            cx2 = DIV(1.0f, MUL(s2pi, sigx));
+            cx1 = DIV(1.0f, MUL(s2, sigx));
+            cy2 = DIV(1.0f, MUL(s2pi, sigy));
+            cy1 = DIV(1.0f, MUL(s2, sigy));
+            // s0 * (2 tz/d^2 + A*3*tz^2/d^2 + B*4*tz^3/d^4) / (2 sqrt(q))
+            const float nx = ADD(ADD(DIV(MUL(2.0f, tzx), dx2), DIV(MUL(MUL(Ax, 3.0f), tzx2), dx2)),
+                                 DIV(MUL(MUL(Bx, 4.0f), tzx3), dx4));
+            const float ny = ADD(ADD(DIV(MUL(2.0f, tzy), dy2), DIV(MUL(MUL(Ay, 3.0f), tzy2), dy2)),
+                                 DIV(MUL(MUL(By, 4.0f), tzy3), dy4));
+            dsxz = DIV(MUL(s0x, nx), MUL(2.0f, sqx));
+            dsyz = DIV(MUL(s0y, ny), MUL(2.0f, sqy));
+        } else {
+            tI = th[2];
+            tbg = th[3];
+            float sx, sy;
+            if (MID == MODEL_XYIBG) { sx = d.sigma[0]; sy = d.sigma[1]; }
+            else if (MID == MODEL_XYIBG_CONSTSIGMA) { sx = consts[0]; sy = consts[1]; }
+            else if (MID == MODEL_XYIBG_SIGMA) { sx = th[4]; sy = th[4]; }
+            else { sx = th[4]; sy = th[5]; }
+            invSqrtPi = DIV(1.0f, __fsqrt_rn(PB_PI));
+            cx2 = DIV(1.0f, MUL(s2pi, sx));
+            cy2 = DIV(1.0f, MUL(s2pi, sy));
+            cx1 = DIV(1.0f, MUL(s2, sx));
+            cy1 = DIV(1.0f, MUL(s2, sy));
+            sigx = sx;
+            sigy = sy;
+        }
+    }
+
+    // One 1D term for coordinate c (pixel index) along an axis with centre t.
+    // Output slots: [0]=Delta, [1]=tI*Delta, [2]=tI*dE, [3]=model-specific.
+    __device__ __forceinline__ void term(int c, float t, float c1, float c2, float sig, bool isx, float4* out) const {
+        const float d0 = SUB((float)c, t);
+        const float e0 = MUL(ADD(d0, 0.5f), c1);
+        const float e1 = MUL(SUB(d0, 0.5f), c1);
+        const float delta = SUB(MUL(0.5f, erff(e0)), MUL(0.5f, erff(e1)));
+        const float ex1 = expf(MUL(-e1, e1));
+        const float ex0 = expf(MUL(-e0, e0));
+        const float dE = MUL(c2, SUB(ex1, ex0));
+        float4 r;
+        r.x = delta;
+        r.y = MUL(tI, delta);
+        if (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA) {
+            r.z = MUL(tI, dE);
+            r.w = 0.0f;
+        } else if (MID == MODEL_XYIBG_SIGMA || MID == MODEL_XYIBG_SIGMAXY) {
+            const float dDs = MUL(SUB(MUL(ex1, e1), MUL(ex0, e0)), invSqrtPi);
+            r.z = MUL(tI, dE);
+            r.w = (MID == MODEL_XYIBG_SIGMAXY) ? MUL(tI, dDs) : dDs;
+        } else {
+            // G21 = 1/(sqrt(2 pi) s s) * ((c-t-.5) exp(-(c-t-.5)^2/(2 s s)) - (c-t+.5) exp(-(c-t+.5)^2/(2 s s)))
+            const float m = SUB(d0, 0.5f), p = ADD(d0, 0.5f);
+            const float ss2 = MUL(MUL(2.0f, sig), sig);
+            const float a = DIV(1.0f, MUL(MUL(__fsqrt_rn(MUL(2.0f, PB_PI)), sig), sig));
+            const float g = MUL(a, SUB(MUL(m, expf(DIV(MUL(-m, m), ss2))), MUL(p, expf(DIV(MUL(-p, p), ss2)))));
+            r.z = MUL(tI, dE);
+            r.w = g;
+        }
+        (void)isx;
+        *out = r;
+    }
+
+    __device__ __forceinline__ void build_table(const ModelDesc& d, float* tab, int lane, int G) const {
+        const int R = d.roisize;
+        float4* t4 = reinterpret_cast<float4*>(tab);
+        for (int i = lane; i < 2 * R; i += G) {
+            if (i < R) term(i, tx, cx1, cx2, sigx, true, &t4[i]);
+            else term(i - R, ty, cy1, cy2, sigy, false, &t4[i]);
+        }
+    }
+
+    // mu and Jacobian for pixel (x, y) from the table.
+    __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
+                                          float (&J)[K]) const {
+        const float4 X = reinterpret_cast<const float4*>(tab)[x];
+        const float4 Y = reinterpret_cast<const float4*>(tab)[d.roisize + y];
+        // mu = tbg + (tI*DeltaX)*DeltaY
+        mu = ADD(tbg, MUL(X.y, Y.x));
+        const float dmx = MUL(X.z, Y.x);  // (tI*dEx)*DeltaY
+        const float dmy = MUL(Y.z, X.x);  // (tI*dEy)*DeltaX
+        const float dI = MUL(X.x, Y.x);
+        if (MID == MODEL_XYZIBG) {
+            // dmu/dz = ((tI*DeltaY)*G21x)*dsx/dz + ((tI*DeltaX)*G21y)*dsy/dz
+            const float dMsx = MUL(Y.y, X.w);
+            const float dMsy = MUL(X.y, Y.w);
+            J[0] = dmx;
+            J[1] = dmy;
+            J[2] = ADD(MUL(dMsx, dsxz), MUL(dMsy, dsyz));
+            J[3] = dI;
+            J[4] = 1.0f;
+        } else {
+            J[0] = dmx;
+            J[1] = dmy;
+            J[2] = dI;
+            J[3] = 1.0f;
+            if (MID == MODEL_XYIBG_SIGMA) {
+                // tI * (dDeltaX_dsigma*DeltaY + dDeltaY_dsigma*DeltaX)
+                J[4 % K] = MUL(tI, ADD(MUL(X.w, Y.x), MUL(Y.w, X.x)));
+            } else if (MID == MODEL_XYIBG_SIGMAXY) {
+                J[4 % K] = MUL(X.w, Y.x);
+                J[5 % K] = MUL(Y.w, X.x);
+            }
+        }
+    }
+
+    // CheckLimits (GaussianPSFModels.h:54-61, 327-337, 410-419, 654-661)
+    __device__ __forceinline__ static void check_limits(const ModelDesc& d, float (&t)[K]) {
+        const int R = d.roisize;
+        const float hi = gauss_xy_max(R);
+        t[0] = pb_clamp(t[0], 1.5f, hi);
+        t[1] = pb_clamp(t[1], 1.5f, hi);
+        if (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA) {
+            if (t[2] < 25.0f) t[2] = 25.0f;
+            if (t[3] < 0.0f) t[3] = 0.0f;
+        } else if (MID == MODEL_XYIBG_SIGMA) {
+            if (t[2] < 10.0f) t[2] = 10.0f;
+            if (t[3] < 0.0f) t[3] = 0.0f;
+            if (t[4 % K] < 1.0f) t[4 % K] = 1.0f;
+            const float smax = MUL((float)R, 0.5f);
+            if (t[4 % K] > smax) t[4 % K] = smax;
+        } else if (MID == MODEL_XYIBG_SIGMAXY) {
+            if (t[2] < 10.0f) t[2] = 10.0f;
+            if (t[3] < 0.0f) t[3] = 0.0f;
+            const float smax = MUL((float)R, 0.5f);
+            t[4 % K] = pb_clamp(t[4 % K], 1.0f, smax);
+            t[5 % K] = pb_clamp(t[5 % K], 1.0f, smax);
+        } else {
+            t[2] = pb_clamp(t[2], d.minz, d.maxz);
+            t[3] = fmaxf(t[3], 10.0f);
+            t[4 % K] = fmaxf(t[4 % K], 0.0f);
+        }
+    }
+
+    __device__ __forceinline__ static float stop_limit(int k) {
+        if (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA) return k == 2 ? 1e-1f : 1e-5f;
+        if (MID == MODEL_XYIBG_SIGMA) return k == 2 ? 1e-1f : (k == 3 ? 1e-4f : 1e-5f);
+        if (MID == MODEL_XYIBG_SIGMAXY) return k == 2 ? 1e-1f : (k == 3 ? 1e-4f : 1e-5f);
+        return k == 2 ? 1e-1f : 1e-4f;  // astig {x,y,z,I,bg} = {1e-4,1e-4,1e-1,1e-4,1e-4}
+    }
+
+    // Initial value from the centre of mass (GaussianPSFModels.h:147-151, 382-386, 466-470, 664-674)
+    __device__ __forceinline__ static void initial(const ModelDesc& d, float comx, float comy, float sum,
+                                                   float (&t)[K]) {
+        t[0] = comx;
+        t[1] = comy;
+        if (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA) {
+            t[2] = MUL(sum, 0.7f);
+            t[3] = 0.0f;
+        } else if (MID == MODEL_XYIBG_SIGMA) {
+            t[2] = sum;
+            t[3] = 0.0f;
+            t[4 % K] = d.sigma[0];
+        } else if (MID == MODEL_XYIBG_SIGMAXY) {
+            t[2] = sum;
+            t[3] = 0.0f;
+            t[4 % K] = d.sigma[0];
+            t[5 % K] = d.sigma[1];
+        } else {
+            t[2] = 0.0f;
+            t[3] = sum;
+            t[4 % K] = 0.01f;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------------
+// Cubic spline (flat background): table = delta_f, delta_dxf, delta_dyf, delta_dzf [4][64].
+// ---------------------------------------------------------------------------------------
+struct SplineModel {
+    static constexpr int K = 5;
+    static constexpr int kId = MODEL_CSPLINE;
+    static __host__ __device__ constexpr int table_floats(int) { return 256; }
+
+    float tx, ty, tI, tbg, du;
+    float spx, spy, spz;
+    int k;  // z slice
+    int Nx, Ny;
+
+    __device__ __forceinline__ void begin(const ModelDesc& d, const float* th, const float*) {
+        const int Nz = d.spline_shape[0];
+        Ny = d.spline_shape[1];
+        Nx = d.spline_shape[2];
+        du = DIV(SUB(d.spline_zmax, d.spline_zmin), (float)Nz);
+        tx = SUB(th[0], MUL((float)Nx, 0.5f));
+        ty = SUB(th[1], MUL((float)Ny, 0.5f));
+        tI = th[3];
+        tbg = th[4];
+        float sx = -tx;
+        spx = SUB(sx, (float)(int)sx);
+        float sy = -ty;
+        spy = SUB(sy, (float)(int)sy);
+        float sz = DIV(SUB(th[2], d.spline_zmin), du);
+        int kk = (int)sz;
+        kk = max(0, min(kk, Nz - 1));
+        k = kk;
+        spz = pb_clamp(SUB(sz, (float)kk), 0.0f, 1.0f);
+    }
+
+    // Power-basis tables (CubicSplinePSFModels.h:101-118): entry idx = m*16 + n*4 + o,
+    // xyz = (spx^o * spy^n) * spz^m built by repeated multiplication as in the reference.
+    __device__ __forceinline__ void build_table(const ModelDesc&, float* tab, int lane, int G) const {
+        for (int idx = lane; idx < 64; idx += G) {
+            const int m = idx >> 4, n = (idx >> 2) & 3, o = idx & 3;
+            float xxx = 1.0f, yyy = 1.0f, zzz = 1.0f;
+            for (int q = 0; q < o; q++) xxx = MUL(xxx, spx);
+            for (int q = 0; q < n; q++) yyy = MUL(yyy, spy);
+            for (int q = 0; q < m; q++) zzz = MUL(zzz, spz);
+            const float xyz = MUL(MUL(xxx, yyy), zzz);
+            tab[idx] = xyz;
+            // delta_dxf[m,n,o+1] = (o+1)*xyz(m,n,o); entries with o == 0 stay 0
+            float xo = 1.0f;
+            for (int q = 0; q < o - 1; q++) xo = MUL(xo, spx);
+            tab[64 + idx] = (o > 0) ? MUL((float)o, MUL(MUL(xo, yyy), zzz)) : 0.0f;
+            float yn = 1.0f;
+            for (int q = 0; q < n - 1; q++) yn = MUL(yn, spy);
+            tab[128 + idx] = (n > 0) ? MUL((float)n, MUL(MUL(xxx, yn), zzz)) : 0.0f;
+            float zm = 1.0f;
+            for (int q = 0; q < m - 1; q++) zm = MUL(zm, spz);
+            tab[192 + idx] = (m > 0) ? MUL((float)m, MUL(MUL(xxx, yyy), zm)) : 0.0f;
+        }
+    }
+
+    __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
+                                          float (&J)[5]) const {
+        const float yy = SUB((float)y, ty);
+        const int j = max(0, min((int)yy, Ny - 1));
+        const float xx = SUB((float)x, tx);
+        const int i = max(0, min((int)xx, Nx - 1));
+        const float4* c4 = reinterpret_cast<const float4*>(d.coefs + 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i));
+        const float4* f4 = reinterpret_cast<const float4*>(tab);
+        float psf = 0.0f, dx = 0.0f, dy = 0.0f, dz = 0.0f;
+#pragma unroll 4
+        for (int q = 0; q < 16; q++) {
+            const float4 c = __ldg(c4 + q);
+            const float4 a = f4[q], b = f4[16 + q], e = f4[32 + q], g = f4[48 + q];
+            psf = ADD(ADD(ADD(ADD(psf, MUL(a.x, c.x)), MUL(a.y, c.y)), MUL(a.z, c.z)), MUL(a.w, c.w));
+            dx = ADD(ADD(ADD(ADD(dx, MUL(b.x, c.x)), MUL(b.y, c.y)), MUL(b.z, c.z)), MUL(b.w, c.w));
+            dy = ADD(ADD(ADD(ADD(dy, MUL(e.x, c.x)), MUL(e.y, c.y)), MUL(e.z, c.z)), MUL(e.w, c.w));
+            dz = ADD(ADD(ADD(ADD(dz, MUL(g.x, c.x)), MUL(g.y, c.y)), MUL(g.z, c.z)), MUL(g.w, c.w));
+        }
+        dx = MUL(dx, -tI);
+        dy = MUL(dy, -tI);
+        dz = MUL(dz, DIV(tI, du));
+        if (psf < 0.0f) psf = 0.0f;
+        mu = ADD(MUL(tI, psf), tbg);
+        J[0] = dx;
+        J[1] = dy;
+        J[2] = dz;
+        J[3] = psf;
+        J[4] = 1.0f;
+    }
+
+    // CheckLimits (CubicSplinePSFModels.h:44-50)
+    __device__ __forceinline__ static void check_limits(const ModelDesc& d, float (&t)[5]) {
+        const float hi = SUB(SUB((float)d.roisize, 1.0f), 1.5f);
+        t[0] = pb_clamp(t[0], 1.5f, hi);
+        t[1] = pb_clamp(t[1], 1.5f, hi);
+        t[2] = pb_clamp(t[2], ADD(d.spline_zmin, 1e-3f), SUB(d.spline_zmax, 1e-3f));
+        t[3] = fmaxf(t[3], 10.0f);
+        t[4] = fmaxf(t[4], 0.0f);
+    }
+
+    __device__ __forceinline__ static float stop_limit(int k) { return k == 2 ? 1e-7f : 1e-4f; }
+
+    __device__ __forceinline__ static void initial(const ModelDesc&, float comx, float comy, float sum,
+                                                   float (&t)[5]) {
+        t[0] = comx;
+        t[1] = comy;
+        t[2] = 0.0f;
+        t[3] = sum;
+        t[4] = 0.0f;
+    }
+};
+
+}  // namespace pb200

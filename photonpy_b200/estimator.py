@@ -1,0 +1,366 @@
+"""Estimator — the drop-in Python surface of photonpy/cpp/estimator.py (lines 27-397).
+
+Same constructor, method names, argument order, shapes, defaults (LM lambda 1e-18,
+50 iterations) and error behaviour (the native side reports through the debug-print
+callback and leaves outputs zero). Everything computes on the GPU through
+libphotonpy_b200.so. Extensions: ``Estimate(..., return_iterations=True)``,
+``EstimateWithCRLB`` (fused fit + CRLB + chi-square), ``EstimateDevice`` /
+``ExpectedValueDevice`` (torch CUDA tensors, no host round trip) and ``SetKernelConfig``.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import numpy.ctypeslib as ctl
+
+from .context import Context
+from .lib import NullableFloatArrayType, NullableIntArrayType
+
+
+class EstimatorProperties(ct.Structure):
+    _fields_ = [
+        ("numParams", ct.c_int),
+        ("sampleCount", ct.c_int),
+        ("numDiag", ct.c_int),
+        ("numConst", ct.c_int),
+        ("sampleIndexDims", ct.c_int),
+    ]
+
+
+class LevMarParams(ct.Structure):
+    _fields_ = [("iterations", ct.c_int32), ("lambda_", ct.c_float), ("factor", ct.c_float)]
+
+
+_F32 = ctl.ndpointer(np.float32, flags="aligned, c_contiguous")
+_I32 = ctl.ndpointer(np.int32, flags="aligned, c_contiguous")
+
+
+def _ptr(t):
+    """Device pointer of a torch tensor (or None)."""
+    return None if t is None else ct.c_void_p(t.data_ptr())
+
+
+class Estimator:
+    def __init__(self, ctx: Context, psfInst, calib=None):
+        if not psfInst:
+            raise RuntimeError("native estimator creation failed: " + _last_error(ctx))
+        self.inst = psfInst
+        self.ctx = ctx
+        self.calib = calib
+        lib = ctx.smlm.lib
+        self._lib = lib
+        Inst = ct.c_void_p
+        self._Estimator_Delete = lib.Estimator_Delete
+        self._Estimator_Delete.argtypes = [Inst]
+        self._Estimator_ParamFormat = lib.Estimator_ParamFormat
+        self._Estimator_ParamFormat.restype = ct.c_char_p
+        self._Estimator_ParamFormat.argtypes = [Inst]
+        self._Estimator_GetProperties = lib.Estimator_GetProperties
+        self._Estimator_GetProperties.argtypes = [Inst, ct.POINTER(EstimatorProperties)]
+        self._Estimator_SampleDims = lib.Estimator_SampleDims
+        self._Estimator_SampleDims.argtypes = [Inst, _I32]
+        self._Estimator_GetParamLimits = lib.Estimator_GetParamLimits
+        self._Estimator_GetParamLimits.argtypes = [Inst, _F32]
+        self._Estimator_ChiSquareAndCRLB = lib.Estimator_ChiSquareAndCRLB
+        self._Estimator_ChiSquareAndCRLB.argtypes = [Inst, _F32, NullableFloatArrayType, _F32, _I32, ct.c_int32, _F32,
+                                                     _F32]
+        self._Estimator_ComputeExpectedValue = lib.Estimator_ComputeExpectedValue
+        self._Estimator_ComputeExpectedValue.argtypes = [Inst, ct.c_int32, _F32, _F32, _I32, _F32]
+        self._Estimator_ComputeDerivatives = lib.Estimator_ComputeDerivatives
+        self._Estimator_ComputeDerivatives.argtypes = [Inst, ct.c_int32, _F32, _F32, _I32, _F32, _F32]
+        self._Estimator_Estimate = lib.Estimator_Estimate
+        self._Estimator_Estimate.argtypes = [Inst, ct.c_int32, _F32, _F32, _I32, NullableFloatArrayType, _F32, _F32,
+                                             NullableIntArrayType, NullableFloatArrayType, ct.c_int32]
+        self._Estimator_SetLMParams = lib.Estimator_SetLMParams
+        self._Estimator_SetLMParams.argtypes = [Inst, ct.POINTER(LevMarParams)]
+        self._Estimator_GetLMParams = lib.Estimator_GetLMParams
+        self._Estimator_GetLMParams.argtypes = [Inst, ct.POINTER(LevMarParams)]
+        self._EstimateCRLB = lib.PB200_EstimateCRLB
+        self._EstimateCRLB.argtypes = [Inst, ct.c_int32, _F32, NullableFloatArrayType, NullableFloatArrayType, _F32,
+                                       NullableIntArrayType, NullableFloatArrayType, NullableFloatArrayType]
+
+        props = EstimatorProperties()
+        self._Estimator_GetProperties(self.inst, props)
+        self.numparams = props.numParams
+        self.numconst = props.numConst
+        self.samplecount = props.sampleCount
+        self.indexdims = props.sampleIndexDims
+        self.sampleshape = np.zeros(self.indexdims, dtype=np.int32)
+        self._Estimator_SampleDims(self.inst, self.sampleshape)
+        self.numdiag = props.numDiag
+        self.fmt = self.ParamFormat()
+        self.param_names = [s.strip() for s in self.fmt.split(",")]
+        self.limits = np.zeros((self.numparams, 2), dtype=np.float32)
+        self._Estimator_GetParamLimits(self.inst, self.limits)
+        self.SetLevMarParams(1e-18, 50)
+
+    # ------------------------------------------------------------------ helpers
+    def _checkparams(self, params, constants, roipos):
+        params = np.array(params)
+        if len(params.shape) == 1:
+            params = [params]
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        numspots = len(params)
+        if constants is None:
+            if self.numconst != 0:
+                raise ValueError(f"Estimator is expecting constant array with shape {[len(params), self.numconst]} "
+                                 f"(None given) ")
+            constants = np.zeros((numspots, self.numconst), dtype=np.float32)
+        else:
+            constants = np.ascontiguousarray(constants, dtype=np.float32)
+            if constants.size != numspots * self.numconst:
+                try:
+                    constants_ = np.zeros([numspots, self.numconst], dtype=np.float32)
+                    constants_[:, :] = constants
+                    constants = constants_
+                except Exception:
+                    raise ValueError(f"Provided constants with shape {constants.shape}, expecting "
+                                     f"{[numspots, self.numconst]}")
+        if roipos is None:
+            roipos = np.zeros((numspots, self.indexdims), dtype=np.int32)
+        else:
+            roipos = np.ascontiguousarray(roipos, dtype=np.int32)
+            if not np.array_equal(roipos.shape, [numspots, self.indexdims]):
+                raise ValueError(f"Provided roi positions have incorrect shape: {roipos.shape} should be "
+                                 f"{[numspots, self.indexdims]}")
+        if params.shape[1] != self.numparams:
+            raise ValueError(f"{self.fmt} expected, {params.shape[1]} parameters given")
+        return params, constants, roipos
+
+    # ------------------------------------------------------------------ reference API
+    def ExpectedValue(self, params, roipos=None, constants=None):
+        """Expected value of each pixel of the ROIs, shape [len(params), *sampleshape]."""
+        params, constants, roipos = self._checkparams(params, constants, roipos)
+        ev = np.zeros((len(params), *self.sampleshape), dtype=np.float32)
+        if len(params) > 0:
+            self._Estimator_ComputeExpectedValue(self.inst, len(params), params, constants, roipos, ev)
+        return ev
+
+    def GenerateSample(self, params, roipos=None, constants=None):
+        ev = self.ExpectedValue(params, roipos, constants)
+        return np.random.poisson(ev)
+
+    def FisherMatrix(self, params, roipos=None, constants=None):
+        params, constants, roipos = self._checkparams(params, constants, roipos)
+        fi = np.zeros((len(params), self.numparams, self.numparams), dtype=np.float32)
+        if len(params) > 0:
+            deriv, ev = self.Derivatives(params, roipos, constants)
+            K = self.numparams
+            ev = np.reshape(ev, (len(params), self.samplecount))
+            deriv = np.reshape(deriv, (len(params), K, self.samplecount))
+            ev[ev < 1e-9] = 1e-9
+            for i in range(K):
+                for j in range(K):
+                    fi[:, i, j] = np.sum(1 / ev * (deriv[:, i] * deriv[:, j]), axis=1)
+        return fi
+
+    def CRLBAndChiSquare(self, params, samples=None, roipos=None, constants=None):
+        """(crlb, chisq) if samples are given, otherwise crlb."""
+        params, constants, roipos = self._checkparams(params, constants, roipos)
+        crlb = np.zeros((len(params), self.numparams), dtype=np.float32)
+        chisq = np.zeros(len(params), dtype=np.float32)
+        if samples is not None:
+            samples = np.ascontiguousarray(samples, dtype=np.float32)
+            if not np.array_equal(samples.shape, [len(params), *self.sampleshape]):
+                raise ValueError(f"Sample data was expected to have shape {[len(params), *self.sampleshape]}. "
+                                 f"Given: {samples.shape}")
+        if len(params) > 0:
+            self._Estimator_ChiSquareAndCRLB(self.inst, params, samples, constants, roipos, len(params), crlb, chisq)
+        if samples is not None:
+            return crlb, chisq
+        return crlb
+
+    def ChiSquare(self, params, samples, roipos=None, constants=None):
+        return self.CRLBAndChiSquare(params, samples, roipos, constants)[1]
+
+    def CRLB(self, params, roipos=None, constants=None):
+        fisher = self.FisherMatrix(params, roipos, constants)
+        var = np.linalg.pinv(fisher)
+        return np.sqrt(np.abs(var[:, np.arange(self.numparams), np.arange(self.numparams)]))
+
+    def Derivatives(self, params, roipos=None, constants=None):
+        """(deriv, ev) with deriv shaped [numspots, numparams, *roishape]."""
+        params, constants, roipos = self._checkparams(params, constants, roipos)
+        deriv = np.zeros((len(params), self.numparams, *self.sampleshape), dtype=np.float32)
+        ev = np.zeros((len(params), *self.sampleshape), dtype=np.float32)
+        if len(params) > 0:
+            self._Estimator_ComputeDerivatives(self.inst, len(params), params, constants, roipos, deriv, ev)
+        return deriv, ev
+
+    def NumDeriv(self, params, roipos=None, constants=None, eps=1e-6):
+        """Central-difference derivative of ExpectedValue."""
+        params, constants, roipos = self._checkparams(params, constants, roipos)
+        ev = self.ExpectedValue(params, roipos, constants)
+        deriv = np.zeros((len(params), self.numparams, *self.sampleshape), dtype=np.float32)
+        for k in range(self.numparams):
+            params_min = params * 1
+            params_min[:, k] -= eps
+            params_max = params * 1
+            params_max[:, k] += eps
+            ev_min = self.ExpectedValue(params_min, roipos, constants)
+            ev_max = self.ExpectedValue(params_max, roipos, constants)
+            deriv[:, k] = (ev_max - ev_min) / (2 * eps)
+        return deriv, ev
+
+    def NumCRLB(self, params, roipos=None, constants=None, eps=1e-4, useNumDeriv=True):
+        if useNumDeriv:
+            deriv, ev = self.NumDeriv(params, roipos, constants, eps)
+        else:
+            deriv, ev = self.Derivatives(params, roipos, constants)
+        K = self.numparams
+        deriv = np.reshape(deriv, (len(params), K, self.samplecount))
+        ev = np.reshape(ev, (len(params), self.samplecount))
+        ev[ev < 1e-9] = 1e-9
+        fi = np.zeros((len(params), K, K))
+        for i in range(K):
+            for j in range(K):
+                fi[:, i, j] = np.sum(1 / ev * (deriv[:, i] * deriv[:, j]), axis=1)
+        var = np.linalg.inv(fi)
+        return np.sqrt(np.abs(var[:, np.arange(self.numparams), np.arange(self.numparams)]))
+
+    def GetLevMarParams(self):
+        lmp = LevMarParams()
+        self._Estimator_GetLMParams(self.inst, lmp)
+        self.lmparams = lmp
+        return lmp
+
+    def SetLevMarParams(self, lambda_=1e-15, iterations=50, lmFactor=0.0):
+        self.lmparams = LevMarParams()
+        self.lmparams.lambda_ = lambda_
+        self.lmparams.iterations = iterations
+        self.lmparams.factor = lmFactor
+        self._Estimator_SetLMParams(self.inst, self.lmparams)
+
+    def Estimate(self, imgs, roipos=None, constants=None, initial=None, return_iterations=False):
+        """Fit every ROI. Returns (params, diag, traces) like the reference; with
+        return_iterations=True also the per-spot iteration counts (i+1 at the stop,
+        maxIterations+1 when capped)."""
+        numspots = len(imgs)
+        traceBufLen = self.lmparams.iterations
+        imgs = np.ascontiguousarray(imgs, dtype=np.float32)
+        if not np.array_equal(imgs.shape[1:], self.sampleshape):
+            raise ValueError(f"Sample images are expected to have shape {self.sampleshape}. Given: {imgs.shape[1:]}")
+        iterations = np.zeros(numspots, np.int32)
+        params = np.zeros((numspots, self.numparams), dtype=np.float32)
+        trace = np.zeros((numspots, traceBufLen, self.numparams), dtype=np.float32)
+        diag = np.zeros((numspots, self.numdiag), dtype=np.float32)
+        params, constants, roipos = self._checkparams(params, constants, roipos)
+        if initial is not None:
+            initial = np.ascontiguousarray(initial, dtype=np.float32)
+            if not np.array_equal(initial.shape, [numspots, self.numparams]):
+                raise ValueError(f"Initial value array is expected to have shape {[numspots, self.numparams]}. "
+                                 f"Given: {initial.shape}")
+        if numspots > 0:
+            self._Estimator_Estimate(self.inst, numspots, imgs, constants, roipos, initial, params,
+                                     np.zeros(max(1, diag.size), np.float32), iterations, trace, traceBufLen)
+        traces = [trace[k, 0:iterations[k], :] for k in range(numspots)]
+        if return_iterations:
+            return params, diag, traces, iterations
+        return params, diag, traces
+
+    # ------------------------------------------------------------------ extensions
+    def EstimateWithCRLB(self, imgs, constants=None, initial=None):
+        """Fused fit + Fisher/CRLB + chi-square (one kernel). Returns (params, iterations, crlb, chisq)."""
+        imgs = np.ascontiguousarray(imgs, dtype=np.float32)
+        n = len(imgs)
+        if not np.array_equal(imgs.shape[1:], self.sampleshape):
+            raise ValueError(f"Sample images are expected to have shape {self.sampleshape}. Given: {imgs.shape[1:]}")
+        params = np.zeros((n, self.numparams), np.float32)
+        its = np.zeros(n, np.int32)
+        crlb = np.zeros((n, self.numparams), np.float32)
+        chisq = np.zeros(n, np.float32)
+        _, constants, _ = self._checkparams(params, constants, None)
+        if initial is not None:
+            initial = np.ascontiguousarray(initial, dtype=np.float32)
+        if n > 0:
+            self._EstimateCRLB(self.inst, n, imgs, constants if self.numconst else None, initial, params, its, crlb,
+                               chisq)
+        return params, its, crlb, chisq
+
+    def EstimateDevice(self, imgs, constants=None, initial=None, with_crlb=True, trace_len=0, stream=None):
+        """Fit torch CUDA tensors in place on the device (no host copies, no synchronisation).
+        Returns dict(params, iterations, crlb, chisq[, trace]) of torch tensors."""
+        import torch
+        n = imgs.shape[0]
+        dev = imgs.device
+        assert imgs.is_cuda and imgs.dtype == torch.float32 and imgs.is_contiguous()
+        out = dict(params=torch.empty((n, self.numparams), device=dev, dtype=torch.float32),
+                   iterations=torch.empty(n, device=dev, dtype=torch.int32))
+        if with_crlb:
+            out["crlb"] = torch.empty((n, self.numparams), device=dev, dtype=torch.float32)
+            out["chisq"] = torch.empty(n, device=dev, dtype=torch.float32)
+        if trace_len > 0:
+            out["trace"] = torch.zeros((n, trace_len, self.numparams), device=dev, dtype=torch.float32)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        self._lib.PB200_EstimateDevice(self.inst, n, _ptr(imgs), _ptr(constants), _ptr(initial), _ptr(out["params"]),
+                                       _ptr(out["iterations"]), _ptr(out.get("trace")), int(trace_len),
+                                       _ptr(out.get("crlb")), _ptr(out.get("chisq")), ct.c_void_p(s.cuda_stream))
+        return out
+
+    def ExpectedValueDevice(self, params, constants=None, derivatives=False, stream=None):
+        """ExpectedValue (and Derivatives) of torch CUDA tensors on the device."""
+        import torch
+        n = params.shape[0]
+        R = int(self.sampleshape[0])
+        ev = torch.empty((n, R, R), device=params.device, dtype=torch.float32)
+        deriv = torch.empty((n, self.numparams, R, R), device=params.device, dtype=torch.float32) if derivatives \
+            else None
+        s = stream if stream is not None else torch.cuda.current_stream(params.device)
+        self._lib.PB200_ExpectedValueDevice(self.inst, n, _ptr(params), _ptr(constants), _ptr(ev), _ptr(deriv),
+                                            ct.c_void_p(s.cuda_stream))
+        return (deriv, ev) if derivatives else ev
+
+    def SetKernelConfig(self, lanes_per_roi=0, threads_per_block=256):
+        rc = self._lib.PB200_SetKernelConfig(self.inst, int(lanes_per_roi), int(threads_per_block))
+        if rc != 0:
+            raise ValueError("invalid kernel configuration")
+
+    def GetKernelConfig(self):
+        g, t = ct.c_int(), ct.c_int()
+        self._lib.PB200_GetKernelConfig(self.inst, ct.byref(g), ct.byref(t))
+        return g.value, t.value
+
+    # ------------------------------------------------------------------ misc
+    def Destroy(self):
+        if self.inst is not None:
+            self._Estimator_Delete(self.inst)
+            self.inst = None
+
+    def NumConstants(self):
+        return self.numconst
+
+    def ParamFormat(self):
+        return self._Estimator_ParamFormat(self.inst).decode("utf-8")
+
+    def ParamIndex(self, paramName):
+        if type(paramName) == list:
+            return [self.param_names.index(n) for n in paramName]
+        return self.param_names.index(paramName)
+
+    def NumParams(self):
+        return self.numparams
+
+    def SampleCount(self):
+        return self.samplecount
+
+    def NumDiag(self):
+        return self.numdiag
+
+    def ParamLimits(self):
+        """(min[NumParams], max[NumParams])"""
+        return self.limits[:, 0], self.limits[:, 1]
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *args):
+        self.Destroy()
+
+
+def _last_error(ctx) -> str:
+    try:
+        ctx.smlm.lib.PB200_GetLastError.restype = ct.c_char_p
+        return (ctx.smlm.lib.PB200_GetLastError() or b"").decode()
+    except Exception:
+        return "unknown error"

@@ -1,0 +1,92 @@
+"""Shared test helpers: build the CUDA estimator and the oracle model for a golden set."""
+import hashlib
+
+import numpy as np
+
+from oracle import oracle as O
+
+
+def oracle_model(name, g):
+    R = int(g["roisize"])
+    if name.startswith("xyibg"):
+        return O.Model(O.XYIBG, R, sigma=tuple(g["sigma"]))
+    if name.startswith("constsigma"):
+        return O.Model(O.XYIBG_CONSTSIGMA, R)
+    if name.startswith("sigma_"):
+        return O.Model(O.XYIBG_SIGMA, R, sigma=tuple(g["sigma"]))
+    if name.startswith("sigmaxy"):
+        return O.Model(O.XYIBG_SIGMAXY, R, sigma=tuple(g["sigma"]))
+    if name.startswith("astig"):
+        return O.Model(O.XYZIBG, R, astig_x=g["astig_x"], astig_y=g["astig_y"], zrange=tuple(g["zrange"]))
+    if name.startswith("spline"):
+        coefs = O.spline_compute(g["zstack"], border=1)
+        return O.Model(O.CSPLINE, R, coefs=coefs, spline_zrange=tuple(g["spline_zrange"]))
+    raise KeyError(name)
+
+
+def cuda_estimator(name, g, ctx):
+    import photonpy_b200 as pb
+    R = int(g["roisize"])
+    if name.startswith("xyibg"):
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYIBg(R, tuple(g["sigma"]), True)
+    if name.startswith("constsigma"):
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYIBg(R, None, True)
+    if name.startswith("sigma_"):
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYIBgSigma(R, float(g["sigma"][0]), True)
+    if name.startswith("sigmaxy"):
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYIBgSigmaXY(R, tuple(g["sigma"]), True)
+    if name.startswith("astig"):
+        c = pb.Gauss3D_Calibration(list(g["astig_x"][:4]), list(g["astig_y"][:4]), list(g["zrange"]))
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYZIBg(R, c, True)
+    if name.startswith("spline"):
+        sm = pb.CSplineMethods(ctx)
+        coefs = sm.ComputeSplineCoeff(g["zstack"], border=1)
+        calib = pb.CSplineCalibration(float(g["spline_zrange"][0]), float(g["spline_zrange"][1]), coefs)
+        est = sm.CreatePSF_XYZIBg(R, calib, sm.FlatBg, True)
+        est._keep = calib
+        return est
+    raise KeyError(name)
+
+
+def coefs_sha(coefs):
+    return hashlib.sha256(np.ascontiguousarray(coefs, dtype=np.float32).tobytes()).hexdigest()
+
+
+def pos_tol(name):
+    """Position tolerance: 1e-3 px for x/y; z: 1 nm (astig, z in nm) or 1e-3 um (spline)."""
+    if name.startswith("astig"):
+        return np.array([1e-3, 1e-3, 1.0])
+    if name.startswith("spline"):
+        return np.array([1e-3, 1e-3, 1e-3])
+    return np.array([1e-3, 1e-3])
+
+
+def split_params(name, K):
+    """indices of (position params, photometric params I/bg)"""
+    if name.startswith("astig") or name.startswith("spline"):
+        return [0, 1, 2], [3, 4]
+    return [0, 1], [2, 3]
+
+
+def parity_stats(name, ref_params, ref_its, params, its, maxit=50):
+    """Agreement of one result set with the reference, stratified by converged/capped."""
+    pos, phot = split_params(name, ref_params.shape[1])
+    tol = pos_tol(name)
+    dpos = np.abs(params[:, pos] - ref_params[:, pos])
+    pos_ok = np.all(dpos <= tol[None, :], axis=1)
+    rel = np.abs(params[:, phot] - ref_params[:, phot]) / np.maximum(np.abs(ref_params[:, phot]), 1e-6)
+    phot_ok = np.all(rel <= 1e-4, axis=1)
+    conv_ref = ref_its <= maxit
+    conv = its <= maxit
+    both = conv_ref & conv
+    return dict(
+        n=len(its),
+        it_match=float(np.mean(its == ref_its)),
+        conv_flag_match=float(np.mean(conv == conv_ref)),
+        pos_ok=float(np.mean(pos_ok)),
+        phot_ok=float(np.mean(phot_ok)),
+        pos_ok_converged=float(np.mean(pos_ok[both])) if both.any() else 1.0,
+        phot_ok_converged=float(np.mean(phot_ok[both])) if both.any() else 1.0,
+        frac_capped_ref=float(np.mean(~conv_ref)),
+        max_dpos_converged=float(dpos[both].max()) if both.any() else 0.0,
+    )
