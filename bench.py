@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""Localizations/s of the batched Poisson-MLE PSF estimator on B200.
+
+One step = one pass of the hot path over one batch: LM fit (centre-of-mass start) +
+Fisher/CRLB + chi-square for every ROI of the batch, which is what photonpy's
+EstimationQueue runs per batch (Estimate then ChiSquareAndCRLB).
+
+Default workload: 2D Gaussian free-sigma MLE (XYIBgSigmaXY), 1,000,000 float32 ROIs of
+16x16 px per GPU, photonpy's Python defaults (LM lambda 1e-18, 50 iterations), seeded
+synthetic Poisson data. The inputs (1.02 GB) exceed the 126 MB L2, so no L2 flush is needed
+between steps.
+
+  value   device-resident throughput (inputs already in HBM), CUDA events on the launch stream
+  e2e     the same through the C ABI (PB200_EstimateCRLB) with pinned HOST buffers; the
+          host->device copy of the ROIs and the device->host copy of the results are inside
+          the timed region (wall clock around the synchronous call)
+  roofline  the fit kernel is bound by the FP32 FMA pipe (not tensor cores, not HBM):
+          achieved = algorithmic FLOPs (photonpy_b200/roofline.py) / kernel time, peak =
+          FP32 FMA throughput measured in the same run by PB200_Fp32ProbeLaunch
+  cpu_baseline  photonpy's own C++ CPU estimator (oracle/_ref, built from the reference
+          sources) on a bounded sample of the same ROIs, all host cores
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
+Multi-GPU: one process per GPU (torchrun); each rank fits its own batch (weak scaling, no
+collective on the data path); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "localizations/s (1 B200, fused vs plain GPU vs host CPU) at CPU-oracle tolerance"
+UNIT = "localizations/s"
+MAX_IT = 50
+LAMBDA = 1e-18
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sigmaxy", choices=["sigmaxy", "xyibg", "astig", "spline"])
+    ap.add_argument("--n", type=int, default=None, help="ROIs per GPU (default: the workload's size)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+WORKLOADS = {
+    "sigmaxy": dict(n=1_000_000, desc="XYIBgSigmaXY 16x16 free-sigma 2D Gaussian MLE + CRLB"),
+    "xyibg": dict(n=1_000_000, desc="XYIBg 10x10 fixed-sigma 2D Gaussian MLE + CRLB"),
+    "astig": dict(n=1_000_000, desc="XYZIBg 12x12 astigmatic 3D Gaussian MLE + CRLB (reference 4-term form)"),
+    "spline": dict(n=500_000, desc="CSpline XYZIBg 13x13 cubic-spline 3D MLE + CRLB"),
+}
+
+
+def make_data(workload, n, seed, device=None):
+    from photonpy_b200 import synth
+    synth.use_torch(device, seed)
+    if workload == "sigmaxy":
+        return synth.sigmaxy(n, seed=seed)
+    if workload == "xyibg":
+        return synth.xyibg(n, seed=seed)
+    if workload == "astig":
+        return synth.astig(n, seed=seed)
+    if workload == "spline":
+        d = synth.spline(n, seed=seed)
+        zstack, zr = synth.astig_zstack(shape_xy=26, nz=41, zrange_um=(-0.4, 0.4))
+        d["zstack"], d["spline_zrange"] = zstack, zr
+        return d
+    raise ValueError(workload)
+
+
+def make_estimator(pb, ctx, d):
+    G = pb.GaussianPSFMethods(ctx)
+    k = d["kind"]
+    if k == "XYIBg":
+        return G.CreatePSF_XYIBg(d["R"], d["sigma"], True)
+    if k == "XYIBgSigmaXY":
+        return G.CreatePSF_XYIBgSigmaXY(d["R"], d["sigma"], True)
+    if k == "XYZIBg":
+        cx, cy = d["astig"]
+        return G.CreatePSF_XYZIBg(d["R"], pb.Gauss3D_Calibration(cx[:4], cy[:4], d["zrange"]), True)
+    if k == "CSpline":
+        sm = pb.CSplineMethods(ctx)
+        coefs = sm.ComputeSplineCoeff(d["zstack"], border=1)
+        calib = pb.CSplineCalibration(d["spline_zrange"][0], d["spline_zrange"][1], coefs)
+        e = sm.CreatePSF_XYZIBg(d["R"], calib, sm.FlatBg, True)
+        e._calib = calib
+        return e
+    raise ValueError(k)
+
+
+def ref_estimator(d):
+    from oracle import ref_lib
+    k = d["kind"]
+    if k in ("XYIBg", "XYIBgSigmaXY"):
+        return ref_lib.RefEstimator(k, d["R"], sigma=d["sigma"])
+    if k == "XYZIBg":
+        cx, cy = d["astig"]
+        return ref_lib.RefEstimator(k, d["R"], astig=(cx[:4], cy[:4]), zrange=d["zrange"])
+    if k == "CSpline":
+        coefs = ref_lib.spline_compute(d["zstack"], border=1)
+        return ref_lib.RefEstimator(k, d["R"], coefs=coefs, spline_zrange=d["spline_zrange"])
+    raise ValueError(k)
+
+
+def oracle_model(d):
+    from oracle import oracle as O
+    k = d["kind"]
+    if k == "XYIBg":
+        return O.Model(O.XYIBG, d["R"], sigma=d["sigma"])
+    if k == "XYIBgSigmaXY":
+        return O.Model(O.XYIBG_SIGMAXY, d["R"], sigma=d["sigma"])
+    if k == "XYZIBg":
+        cx, cy = d["astig"]
+        return O.Model(O.XYZIBG, d["R"], astig_x=cx, astig_y=cy, zrange=d["zrange"])
+    if k == "CSpline":
+        return O.Model(O.CSPLINE, d["R"], coefs=O.spline_compute(d["zstack"], border=1),
+                       spline_zrange=d["spline_zrange"])
+    raise ValueError(k)
+
+
+def cpu_localize(d, samples):
+    """photonpy's CPU estimator (reference build) — or the oracle port when it is absent —
+    on `samples`: Estimate + ChiSquareAndCRLB, in chunks of 20k spots (the reference starts one
+    thread per spot). Returns (seconds, kind)."""
+    from oracle import ref_lib
+    t0 = time.perf_counter()
+    if ref_lib.available():
+        est = ref_estimator(d)
+        for s in range(0, len(samples), 20000):
+            chunk = samples[s:s + 20000]
+            p, _, _ = est.estimate(chunk, trace_len=0)
+            est.crlb_chisq(p, chunk)
+        est.close()
+        kind = "reference"
+    else:
+        m = oracle_model(d)
+        for s in range(0, len(samples), 20000):
+            chunk = samples[s:s + 20000]
+            p, _ = m.fit(chunk)
+            m.crlb(p, chunk)
+        kind = "port"
+    return time.perf_counter() - t0, kind
+
+
+def cpu_baseline(d, budget_s):
+    samples = d["samples"]
+    n0 = min(len(samples), 2000)
+    t, kind = cpu_localize(d, samples[:n0])
+    rate = n0 / max(t, 1e-6)
+    n = int(min(len(samples), max(n0, rate * budget_s)))
+    t, kind = cpu_localize(d, samples[:n])
+    return dict(value=n / t, unit=UNIT, cores=os.cpu_count(), kind=kind,
+                sample=f"first {n} ROIs of the same batch ({d['kind']} {d['R']}x{d['R']}), "
+                       f"Estimate + ChiSquareAndCRLB, {t:.1f} s")
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.f:
+            return None
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smmax=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwth=parts[6], swth=parts[7], swpc=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        load = [r for r in rows if r["power"] > 200] or rows
+        reasons = set()
+        for r in load:
+            for key, name in (("hw", "hw_slowdown"), ("hwth", "hw_thermal_slowdown"), ("swth", "sw_thermal_slowdown"),
+                              ("swpc", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return dict(sm_mhz=statistics.median(r["sm"] for r in load), sm_max_mhz=max(r["smmax"] for r in rows),
+                     power_w_max=max(r["power"] for r in rows), samples=len(rows), reasons=sorted(reasons))
+
+
+def fp32_peak(pb, torch):
+    """Measured FP32 FMA throughput (TFLOP/s) on this GPU: best of 3 probe launches."""
+    L = pb.load_library()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    out = torch.zeros(sms * 8, device="cuda")
+    stream = torch.cuda.current_stream()
+    best = 0.0
+    for it in (2000, 8000, 8000, 8000):
+        s, e = torch.cuda.Event(True), torch.cuda.Event(True)
+        s.record()
+        flops = L.PB200_Fp32ProbeLaunch(sms * 8, 256, it, out.data_ptr(), stream.cuda_stream)
+        e.record()
+        torch.cuda.synchronize()
+        if flops > 0:
+            best = max(best, flops / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def traffic_from_profile(workload):
+    """DRAM bytes per fit launch from the committed ncu summary, scaled to the batch."""
+    p = os.path.join(ROOT, "profiles", f"fit_{workload}_traffic.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return None
+
+
+def run_reference(args):
+    """Reference arm: photonpy's own CPU estimator on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    d = make_data(args.workload, min(args.n or w["n"], 200_000), seed=2 if args.workload == "sigmaxy" else 1)
+    from oracle import ref_lib
+    n_cal = 2000
+    t, kind = cpu_localize(d, d["samples"][:n_cal])
+    per_step = int(min(len(d["samples"]), max(n_cal, n_cal / t * 6.0)))
+    for _ in range(args.warmup):
+        cpu_localize(d, d["samples"][:min(per_step, 5000)])
+    times = []
+    for k in range(args.steps):
+        off = (k * per_step) % max(1, len(d["samples"]) - per_step + 1)
+        t, kind = cpu_localize(d, d["samples"][off:off + per_step])
+        times.append(t)
+    ms = 1e3 * float(np.mean(times))
+    value = per_step / (ms * 1e-3)
+    line = dict(impl="reference", metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic (seeded Poisson ROIs)",
+                config=dict(workload=w["desc"], roi_size=d["R"], model=d["kind"], rois_per_step=per_step,
+                            lm_iterations=MAX_IT, lm_lambda=LAMBDA),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=os.cpu_count(), kind=kind,
+                                  sample=f"{per_step} ROIs per step ({d['kind']} {d['R']}x{d['R']}), "
+                                         f"Estimate + ChiSquareAndCRLB, reference {'build' if ref_lib.available() else 'port'}"),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    import photonpy_b200 as pb
+    from photonpy_b200 import roofline
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pb.load_library().CudaSetDevice(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    w = WORKLOADS[args.workload]
+    n = args.n or w["n"]
+    base_seed = {"sigmaxy": 2, "xyibg": 1, "astig": 3, "spline": 4}[args.workload]
+    d = make_data(args.workload, n, seed=base_seed + 1000 * rank, device=f"cuda:{local}")
+    smp = d["samples"]
+    K = roofline.K_OF[d["kind"]]
+
+    ctx = pb.Context()
+    est = make_estimator(pb, ctx, d)
+    x = torch.from_numpy(smp).cuda()
+    peak_fp32 = fp32_peak(pb, torch)
+
+    def step():
+        return est.EstimateDevice(x, with_crlb=True)
+
+    for _ in range(max(args.warmup, 3)):
+        out = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n_launch0 = pb.launch_count()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t_w = time.perf_counter()
+        while time.perf_counter() - t_w < 0.6:  # keep the GPU busy while nvidia-smi starts sampling
+            step()
+            torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            out = step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = pb.launch_count() - n_launch0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n / (ms_max * 1e-3)
+
+    its = out["iterations"].cpu().numpy()
+    flops = roofline.localization_flops(d["kind"], d["R"], its, MAX_IT)
+    achieved_tflops = flops / (ms * 1e-3) / 1e12
+    bytes_roi = roofline.hbm_bytes_per_roi(d["kind"], d["R"])
+    hbm_gbs = bytes_roi * n / (ms * 1e-3) / 1e9
+    peaks = measured_peaks()
+
+    # ---- e2e through the C ABI with pinned host buffers --------------------------------
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as ct
+        h_smp = torch.empty(smp.shape, dtype=torch.float32, pin_memory=True)
+        h_smp.numpy()[...] = smp
+        h_par = torch.empty((n, K), dtype=torch.float32, pin_memory=True)
+        h_its = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        h_crlb = torch.empty((n, K), dtype=torch.float32, pin_memory=True)
+        h_chi = torch.empty(n, dtype=torch.float32, pin_memory=True)
+        L = pb.load_library()
+        fn = L.PB200_EstimateCRLB
+        fn.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                       ct.c_void_p, ct.c_void_p]
+
+        def e2e_step():
+            fn(est.inst, n, h_smp.data_ptr(), None, None, h_par.data_ptr(), h_its.data_ptr(), h_crlb.data_ptr(),
+               h_chi.data_ptr())
+
+        for _ in range(2):
+            e2e_step()
+        if world > 1:
+            dist.barrier()
+        tt = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            e2e_step()
+            tt.append(time.perf_counter() - t0)
+        et = torch.tensor([float(np.mean(tt))], device="cuda")
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        h2d = smp.nbytes
+        d2h = n * (4 * K * 2 + 8)
+        e2e = dict(value=world * n / float(et.item()), unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
+                   ms_per_step=1e3 * float(et.item()), api="PB200_EstimateCRLB (C ABI, pinned host buffers)")
+        # results through the host path equal the device path
+        assert np.array_equal(h_par.numpy(), out["params"].cpu().numpy())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(d, args.cpu_seconds)
+
+    if rank == 0:
+        tr = traffic_from_profile(args.workload)
+        traffic = None
+        if tr:
+            traffic = tr["dram_bytes_per_roi"] * n
+        line = dict(
+            metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
+            ms_per_step=ms_max, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+            data="synthetic (seeded Poisson ROIs, photonpy_b200.synth)",
+            config=dict(workload=w["desc"], model=d["kind"], roi_size=d["R"], rois_per_gpu=n, global_rois=world * n,
+                        lm_iterations=MAX_IT, lm_lambda=LAMBDA, mean_iterations=float(np.minimum(its, MAX_IT).mean()),
+                        kernel_config=list(est.GetKernelConfig()),
+                        l2="inputs of %.2f GB per step exceed the 126 MB L2; no flush needed" % (smp.nbytes / 1e9),
+                        parallelism=f"dp{world} (independent ROI shards, no collective)"),
+            roofline=dict(bound="fp32", achieved=achieved_tflops, peak=peak_fp32, unit="TFLOP/s",
+                          frac=achieved_tflops / peak_fp32 if peak_fp32 else None, traffic=traffic,
+                          peak_source="FP32 FMA probe measured in this run (PB200_Fp32ProbeLaunch)",
+                          flops_per_step=flops, kernel_ms=ms),
+            roofline_hbm=dict(bound="hbm", achieved=hbm_gbs, peak=peaks.get("hbm_gbs"), unit="GB/s",
+                              frac=(hbm_gbs / peaks["hbm_gbs"]) if peaks.get("hbm_gbs") else None,
+                              note="algorithmic ROI-stream bytes (of measured MEASURED_PEAKS.json hbm_gbs)"),
+            e2e=e2e, cpu_baseline=cpu, gpu_launches=int(launches), clocks=clk.summary(),
+        )
+        print(json.dumps(line), flush=True)
+    est.Destroy()
+    ctx.Destroy()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

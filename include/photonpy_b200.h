@@ -170,8 +170,15 @@ void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_par
  * and threads per block (64..256). Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
 void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock);
+/* Fit kernel family for the Gaussian models: 0 = column-blocked (default), 1 = generic
+ * per-pixel table kernel (the spline model always uses 1). Returns 0 on success. */
+int PB200_SetKernelVariant(Estimator* e, int variant);
 /* Number of fit-kernel launches issued by this library since load (for launch accounting). */
 uint64_t PB200_LaunchCount(void);
+/* FP32 FMA-pipe throughput probe (diagnostic): launches blocks x threads threads running
+ * 8 independent FMA chains for iters x 16 steps on `stream`; returns the FLOPs issued (time the
+ * launch with events) or -1 on a launch error. d_out: device buffer of `blocks` floats. */
+double PB200_Fp32ProbeLaunch(int blocks, int threads, int iters, float* d_out, void* stream);
 /* Model id (0 XYIBg, 1 XYIBgConstSigma, 2 XYIBgSigma, 3 XYIBgSigmaXY, 4 XYZIBg, 5 CSpline) and ROI size. */
 int PB200_ModelInfo(Estimator* e, int* roisize);
 

@@ -22,7 +22,7 @@
 #include <vector>
 
 #include "../../include/photonpy_b200.h"
-#include "fit_kernels.cuh"
+#include "launch.cuh"
 
 using namespace pb200;
 
@@ -92,6 +92,10 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+
+}  // namespace
+
+namespace pb200 {
 int num_sms() {
     static int sms[64] = {0};
     int dev = 0;
@@ -105,112 +109,42 @@ int num_sms() {
     return sms[dev];
 }
 
-// ------------------------------------------------------------------------------------
-// kernel dispatch over (model, lanes per ROI)
-// ------------------------------------------------------------------------------------
-using FitLaunch = void (*)(const ModelDesc&, FitArgs, int threads, cudaStream_t);
-using EvalLaunch = void (*)(const ModelDesc&, const float*, const float*, float*, float*, int, int threads,
-                            cudaStream_t);
+void count_launch() { g_launches++; }
 
-constexpr int kMaxSmemPerBlock = 200 * 1024;
-
-template <class M, int G>
-void launch_fit(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
-    if (a.n <= 0) return;
-    auto kern = fit_kernel<M, G>;
-    a.smemStride = group_smem_floats<M>(d.roisize);
-    int gpb = threads / G;
-    size_t smem = (size_t)gpb * a.smemStride * sizeof(float);
-    while (smem > (size_t)kMaxSmemPerBlock && threads > 32) {
-        threads /= 2;
-        gpb = threads / G;
-        smem = (size_t)gpb * a.smemStride * sizeof(float);
-    }
-    if (smem > (size_t)kMaxSmemPerBlock || gpb < 1) throw Error("ROI too large for the fit kernel's shared memory");
-    static std::once_flag once;
-    std::call_once(once, [&] { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerBlock); });
-    int perSM = 0;
-    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem));
-    if (perSM < 1) perSM = 1;
-    const long long needed = (a.n + gpb - 1) / gpb;
-    const long long cap = (long long)num_sms() * perSM;
-    const int grid = (int)(needed < cap ? needed : cap);
-    kern<<<grid, threads, smem, s>>>(d, a);
-    PB_CUDA(cudaGetLastError());
-    g_launches++;
-}
-
-template <class M, int G>
-void launch_eval(const ModelDesc& d, const float* params, const float* consts, float* ev, float* deriv, int n,
-                 int threads, cudaStream_t s) {
-    if (n <= 0) return;
-    auto kern = eval_kernel<M, G>;
-    const int stride = round_up(M::table_floats(d.roisize), 32) + 8;
-    const int gpb = threads / G;
-    const size_t smem = (size_t)gpb * stride * sizeof(float);
-    int perSM = 0;
-    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem));
-    if (perSM < 1) perSM = 1;
-    const long long needed = (n + gpb - 1) / gpb;
-    const long long cap = (long long)num_sms() * perSM * 4;
-    const int grid = (int)(needed < cap ? needed : cap);
-    kern<<<grid, threads, smem, s>>>(d, params, consts, ev, deriv, n, stride);
-    PB_CUDA(cudaGetLastError());
-    g_launches++;
-}
-
-template <class M>
-struct ModelTable {
-    static FitLaunch fit(int G) {
-        switch (G) {
-        case 4: return launch_fit<M, 4>;
-        case 8: return launch_fit<M, 8>;
-        case 16: return launch_fit<M, 16>;
-        default: return launch_fit<M, 32>;
-        }
-    }
-    static EvalLaunch eval(int G) {
-        switch (G) {
-        case 8: return launch_eval<M, 8>;
-        case 16: return launch_eval<M, 16>;
-        default: return launch_eval<M, 32>;
-        }
-    }
-};
-
-FitLaunch fit_launcher(int model, int G) {
+FitLaunch fit_launcher_for(int model, int G, int CPL, int variant) {
     switch (model) {
-    case MODEL_XYIBG: return ModelTable<GaussModel<MODEL_XYIBG>>::fit(G);
-    case MODEL_XYIBG_CONSTSIGMA: return ModelTable<GaussModel<MODEL_XYIBG_CONSTSIGMA>>::fit(G);
-    case MODEL_XYIBG_SIGMA: return ModelTable<GaussModel<MODEL_XYIBG_SIGMA>>::fit(G);
-    case MODEL_XYIBG_SIGMAXY: return ModelTable<GaussModel<MODEL_XYIBG_SIGMAXY>>::fit(G);
-    case MODEL_XYZIBG: return ModelTable<GaussModel<MODEL_XYZIBG>>::fit(G);
-    case MODEL_CSPLINE: return ModelTable<SplineModel>::fit(G);
+    case MODEL_XYIBG: return fit_launcher_xyibg(G, CPL, variant);
+    case MODEL_XYIBG_CONSTSIGMA: return fit_launcher_constsigma(G, CPL, variant);
+    case MODEL_XYIBG_SIGMA: return fit_launcher_sigma(G, CPL, variant);
+    case MODEL_XYIBG_SIGMAXY: return fit_launcher_sigmaxy(G, CPL, variant);
+    case MODEL_XYZIBG: return fit_launcher_astig(G, CPL, variant);
+    case MODEL_CSPLINE: return fit_launcher_spline(G, CPL, variant);
     }
     throw Error("unknown model");
 }
 
-EvalLaunch eval_launcher(int model, int G) {
+EvalLaunch eval_launcher_for(int model, int G) {
     switch (model) {
-    case MODEL_XYIBG: return ModelTable<GaussModel<MODEL_XYIBG>>::eval(G);
-    case MODEL_XYIBG_CONSTSIGMA: return ModelTable<GaussModel<MODEL_XYIBG_CONSTSIGMA>>::eval(G);
-    case MODEL_XYIBG_SIGMA: return ModelTable<GaussModel<MODEL_XYIBG_SIGMA>>::eval(G);
-    case MODEL_XYIBG_SIGMAXY: return ModelTable<GaussModel<MODEL_XYIBG_SIGMAXY>>::eval(G);
-    case MODEL_XYZIBG: return ModelTable<GaussModel<MODEL_XYZIBG>>::eval(G);
-    case MODEL_CSPLINE: return ModelTable<SplineModel>::eval(G);
+    case MODEL_XYIBG: return eval_launcher_xyibg(G);
+    case MODEL_XYIBG_CONSTSIGMA: return eval_launcher_constsigma(G);
+    case MODEL_XYIBG_SIGMA: return eval_launcher_sigma(G);
+    case MODEL_XYIBG_SIGMAXY: return eval_launcher_sigmaxy(G);
+    case MODEL_XYZIBG: return eval_launcher_astig(G);
+    case MODEL_CSPLINE: return eval_launcher_spline(G);
     }
     throw Error("unknown model");
 }
+}  // namespace pb200
+
+namespace {
 
 // Lanes per ROI when no tuned value is set: enough ROIs per warp to amortise the redundant
 // K x K solve for small ROIs, enough lanes to keep per-lane pixel loops short for large ones.
 int default_lanes(int model, int R) {
-    const int npix = R * R;
-    if (model == MODEL_CSPLINE) return npix <= 100 ? 8 : 16;
-    if (npix <= 64) return 4;
-    if (npix <= 324) return 8;
-    if (npix <= 784) return 16;
-    return 32;
+    if (model == MODEL_CSPLINE) return R * R <= 100 ? 8 : 16;
+    if (R <= 16) return 4;
+    if (R <= 32) return 8;
+    return 16;
 }
 
 }  // namespace
@@ -239,6 +173,7 @@ struct Estimator {
     Context* ctx = nullptr;
     DevBuf coefs;
     int lanes = 0, threads = 256;
+    int variant = 0;  // 0: column-blocked Gaussian kernel, 1: generic table kernel
     int device = 0;
     std::mutex mtx;
     Slot slots[2];
@@ -249,6 +184,17 @@ struct Estimator {
             if (s.stream) cudaStreamDestroy(s.stream);
     }
     int lanes_for() const { return lanes ? lanes : default_lanes(desc.model, desc.roisize); }
+    // Fit launcher for this estimator's model, ROI size and kernel configuration.
+    FitLaunch fit_launch() const {
+        int G = lanes_for();
+        const int R = desc.roisize;
+        if (desc.model != MODEL_CSPLINE && variant == 0) {
+            while (G < 32 && (R + G - 1) / G > 4) G *= 2;
+            const int cpl = (R + G - 1) / G;
+            if (cpl <= (G == 32 ? 2 : 4)) return fit_launcher_for(desc.model, G, cpl, 0);
+        }
+        return fit_launcher_for(desc.model, G, 0, 1);
+    }
     int npix() const { return desc.roisize * desc.roisize; }
     Slot& slot(int i) {
         if (!slots[i].stream) PB_CUDA(cudaStreamCreateWithFlags(&slots[i].stream, cudaStreamNonBlocking));
@@ -331,7 +277,7 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
     int chunk = n;
     if (n > 65536) chunk = std::max(32768, (n + 7) / 8);
     const int nchunks = (n + chunk - 1) / chunk;
-    FitLaunch fl = fit_launcher(e->desc.model, e->lanes_for());
+    FitLaunch fl = e->fit_launch();
     struct Pending {
         int slot, start, count;
     };
@@ -424,7 +370,7 @@ void host_eval(Estimator* e, int n, const float* h_params, const float* h_consts
     if (h_deriv) s.trace.ensure(sizeof(float) * (size_t)npix * K * n);
     int G = e->lanes_for();
     if (G < 8) G = 8;
-    eval_launcher(e->desc.model, G)(e->desc, s.initial.as<float>(), NC ? s.consts.as<float>() : nullptr,
+    eval_launcher_for(e->desc.model, G)(e->desc, s.initial.as<float>(), NC ? s.consts.as<float>() : nullptr,
                                     h_ev ? s.smp.as<float>() : nullptr, h_deriv ? s.trace.as<float>() : nullptr, n,
                                     256, s.stream);
     if (h_ev)
@@ -531,7 +477,7 @@ void spline_compute_device(const int* shape, const float* d_data, float* d_coefs
     const int grid = (int)std::min<long long>((total + threads - 1) / threads, 65535);
     spline_compute_kernel<<<grid, threads, 0, s>>>(d_data, shape[0], shape[1], shape[2], border, d_coefs, o0, o1, o2);
     PB_CUDA(cudaGetLastError());
-    g_launches++;
+    count_launch();
 }
 
 // CSpline_Evaluate (CubicSplinePSF.cu:208-271): values[z][y][x][4] = val, dx, dy, dz.
@@ -791,7 +737,7 @@ void CSpline_Evaluate(const int* shape, const float* splineCoefs, const float* s
         spline_evaluate_kernel<<<grid, 128>>>(dc.as<float>(), shape[0], shape[1], shape[2], d[0], d[1], d[2],
                                               shift[0], shift[1], shift[2], border, dv.as<float>());
         PB_CUDA(cudaGetLastError());
-        g_launches++;
+        count_launch();
         PB_CUDA(cudaMemcpy(values, dv.p, sizeof(float) * nout, cudaMemcpyDeviceToHost));
         });
 }
@@ -888,7 +834,7 @@ void PB200_EstimateDevice(Estimator* e, int numspots, const float* d_sample, con
         a.iterations = d_iterations; a.trace = traceBufLen > 0 ? d_trace : nullptr;
         a.traceLen = traceBufLen > 0 && d_trace ? traceBufLen : 0; a.crlb = d_crlb; a.chisq = d_chisq;
         a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda; a.flags = 0;
-        fit_launcher(e->desc.model, e->lanes_for())(e->desc, a, e->threads, (cudaStream_t)stream);});
+        e->fit_launch()(e->desc, a, e->threads, (cudaStream_t)stream);});
 }
 
 void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
@@ -898,7 +844,7 @@ void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params
         check_estimator(e); if (numspots < 0 || !d_params) throw Error("ExpectedValueDevice: bad arguments");
         if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
         int G = e->lanes_for(); if (G < 8) G = 8;
-        eval_launcher(e->desc.model, G)(e->desc, d_params, d_constants, d_ev, d_deriv, numspots, 256,
+        eval_launcher_for(e->desc.model, G)(e->desc, d_params, d_constants, d_ev, d_deriv, numspots, 256,
                                         (cudaStream_t)stream);});
 }
 
@@ -911,7 +857,7 @@ void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_par
         FitArgs a{}; a.smp = d_sample; a.consts = d_constants; a.initial = d_params; a.params = nullptr;
         a.crlb = d_crlb; a.chisq = d_chisq; a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda;
         a.flags = FIT_CRLB_ONLY;
-        fit_launcher(e->desc.model, e->lanes_for())(e->desc, a, e->threads, (cudaStream_t)stream);});
+        e->fit_launch()(e->desc, a, e->threads, (cudaStream_t)stream);});
 }
 
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {
@@ -921,6 +867,13 @@ int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {
     std::lock_guard<std::mutex> g(e->mtx);
     e->lanes = lanesPerRoi;
     e->threads = threadsPerBlock;
+    return 0;
+}
+
+int PB200_SetKernelVariant(Estimator* e, int variant) {
+    if (!e || variant < 0 || variant > 1) return -1;
+    std::lock_guard<std::mutex> g(e->mtx);
+    e->variant = variant;
     return 0;
 }
 

@@ -1,0 +1,251 @@
+// Shared pieces of the fit kernels: launch arguments, lane-group helpers, the damped K x K
+// LM solve (packed triangles, registers only) and the FP64 paths run by one lane on shared
+// memory (LM re-solve of a weak pivot, Fisher-matrix inverse).
+//
+// Reference semantics (Estimators/Estimation.h:194-251, SolveMatrix.h:107-163, 411-452):
+//  * damping lambda > 0: a_kk += lambda * sum_j a_jk^2 (scale invariant); lambda < 0: a_kk -= lambda;
+//  * the Cholesky factorization fails (LM stops) only on an exactly-zero pivot;
+//  * Fisher inverse by LUP with partial pivoting and tolerance 1e-9 (failure -> +Inf CRLB).
+// By design: pivots are applied through rsqrt products instead of IEEE divides; a pivot that
+// lost more than six decimal digits (v <= 1e-6 * a_kk, including v < 0) is re-solved in FP64;
+// the Fisher matrix is inverted in FP64 instead of FP32.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pb200 {
+
+enum FitFlags : int {
+    FIT_CRLB_ONLY = 1,  // skip LM: params come from `initial`, compute Fisher/CRLB/chi^2 only
+};
+
+struct FitArgs {
+    const float* smp;      // [n][npix] (may be null with FIT_CRLB_ONLY: no chi-square)
+    const float* consts;   // [n][numconst] or null
+    const float* initial;  // [n][K] or null (centre-of-mass start)
+    float* params;         // [n][K]
+    int* iterations;       // [n] or null
+    float* trace;          // [n][traceLen][K] or null
+    int traceLen;
+    float* crlb;           // [n][K] or null (no Fisher pass)
+    float* chisq;          // [n] or null
+    int* diag;             // [n] or null: 1 when an FP64 re-solve happened for the spot
+    int n;
+    int maxIter;
+    float lambda;
+    int smemStride;        // floats of shared memory per group
+    int flags;
+};
+
+__host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// Packed upper-triangle index (i <= j) of a symmetric K x K matrix, row-major.
+__host__ __device__ constexpr int upk(int i, int j, int K) {
+    return i <= j ? i * K - (i * (i - 1)) / 2 + (j - i) : upk(j, i, K);
+}
+// Packed lower-triangle index (j <= i).
+__host__ __device__ constexpr int lok(int i, int j) { return i * (i + 1) / 2 + j; }
+
+// Floats of shared memory for the FP64 LM re-solve (doubles first: D packed, y; then floats).
+__host__ __device__ constexpr int rescue_floats(int K) { return 3 * (K * (K + 1) / 2) + 5 * K + 1; }
+
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+    if (G == 32) return 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    return ((1u << (G & 31)) - 1u) << (lane & ~(unsigned)(G - 1));
+}
+
+template <int G>
+__device__ __forceinline__ float group_sum(float v, unsigned mask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+// 1/x for x >= 1e-8 (never denormal): approximate reciprocal + one Newton step, no branch.
+__device__ __forceinline__ float rcp_nr(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    const float e = fmaf(-x, r, 1.0f);
+    return fmaf(r, e, r);
+}
+
+// Damped LM step in registers. acc = [alpha upper packed (NA) | beta (K) | extra].
+// Returns 1 on success, 0 on an exactly-zero pivot (reference failure), 2 when a pivot is
+// weak and the step must be re-solved in FP64.
+template <int K, int NACC>
+__device__ __forceinline__ int lm_solve(const float (&acc)[NACC], float lambda, float (&step)[K], float (&dk)[K]) {
+    constexpr int NA = K * (K + 1) / 2;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        if (lambda < 0.0f) {
+            dk[k] = acc[upk(k, k, K)] - lambda;
+        } else {
+            float s = 0.0f;
+#pragma unroll
+            for (int j = 0; j < K; j++) s += acc[upk(j, k, K)] * acc[upk(j, k, K)];
+            dk[k] = acc[upk(k, k, K)] + s * lambda;
+        }
+    }
+    float L[NA], Linv[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int p = 0; p < k; ++p) sum += L[lok(k, p)] * L[lok(k, p)];
+        const float v = dk[k] - sum;
+        if (v == 0.0f) return 0;
+        if (!(v > 1e-6f * dk[k])) return 2;  // also catches v < 0 and NaN
+        const float inv = rsqrtf(v);
+        L[lok(k, k)] = v * inv;
+        Linv[k] = inv;
+#pragma unroll
+        for (int i = k + 1; i < K; ++i) {
+            float s2 = 0.0f;
+#pragma unroll
+            for (int p = 0; p < k; ++p) s2 += L[lok(i, p)] * L[lok(k, p)];
+            L[lok(i, k)] = (acc[upk(i, k, K)] - s2) * inv;
+        }
+    }
+    float y[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = 0; k < i; ++k) sum += L[lok(i, k)] * y[k];
+        y[i] = (acc[NA + i] - sum) * Linv[i];
+    }
+#pragma unroll
+    for (int i = K - 1; i >= 0; --i) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = i + 1; k < K; ++k) sum += L[lok(k, i)] * step[k];
+        step[i] = (y[i] - sum) * Linv[i];
+    }
+    return 1;
+}
+
+// FP64 Cholesky solve by one lane. A: packed upper (float, NA), b: K, dk: damped diagonal.
+// Scratch: D packed lower (double, NA), y (double, K). Writes x (float, K); false on a zero pivot.
+static __device__ __noinline__ bool lm_solve_fp64_lane(int K, const float* A, const float* b, const float* dk, double* D,
+                                               double* y, float* x) {
+    for (int k = 0; k < K; ++k) {
+        double sum = 0.0;
+        for (int p = 0; p < k; ++p) sum += D[lok(k, p)] * D[lok(k, p)];
+        const double v = (double)dk[k] - sum;
+        if (v == 0.0) return false;
+        D[lok(k, k)] = sqrt(v);
+        for (int i = k + 1; i < K; ++i) {
+            double s2 = 0.0;
+            for (int p = 0; p < k; ++p) s2 += D[lok(i, p)] * D[lok(k, p)];
+            D[lok(i, k)] = ((double)A[upk(i, k, K)] - s2) / D[lok(k, k)];
+        }
+    }
+    for (int i = 0; i < K; ++i) {
+        double sum = 0.0;
+        for (int k = 0; k < i; ++k) sum += D[lok(i, k)] * y[k];
+        y[i] = ((double)b[i] - sum) / D[lok(i, i)];
+    }
+    for (int i = K - 1; i >= 0; --i) {
+        double sum = 0.0;
+        for (int k = i + 1; k < K; ++k) sum += D[lok(k, i)] * y[k];
+        y[i] = (y[i] - sum) / D[lok(i, i)];  // y[k>i] already hold the solution
+    }
+    for (int i = 0; i < K; ++i) x[i] = (float)y[i];
+    return true;
+}
+
+// FP64 LUP inverse with the reference's 1e-9 tolerance (SolveMatrix.h:219-318, 344-392), one
+// lane on shared memory: A[K*K] is overwritten, IA[K*K] receives the inverse.
+static __device__ __noinline__ bool invert_fp64_lane(int K, double* A, double* IA) {
+    int P[8];
+    for (int i = 0; i <= K; i++) P[i] = i;
+    for (int i = 0; i < K; i++) {
+        double maxA = 0.0;
+        int imax = i;
+        for (int k = i; k < K; k++) {
+            const double v = fabs(A[k * K + i]);
+            if (v > maxA) { maxA = v; imax = k; }
+        }
+        if (maxA < (double)1e-9f) return false;
+        if (imax != i) {
+            const int tp = P[i]; P[i] = P[imax]; P[imax] = tp;
+            for (int j = 0; j < K; j++) {
+                const double t = A[i * K + j]; A[i * K + j] = A[imax * K + j]; A[imax * K + j] = t;
+            }
+            P[K]++;
+        }
+        for (int j = i + 1; j < K; j++) {
+            A[j * K + i] /= A[i * K + i];
+            for (int k = i + 1; k < K; k++) A[j * K + k] -= A[j * K + i] * A[i * K + k];
+        }
+    }
+    for (int j = 0; j < K; j++) {
+        for (int i = 0; i < K; i++) {
+            double v = (P[i] == j) ? 1.0 : 0.0;
+            for (int k = 0; k < i; k++) v -= A[i * K + k] * IA[k * K + j];
+            IA[i * K + j] = v;
+        }
+        for (int i = K - 1; i >= 0; i--) {
+            double v = IA[i * K + j];
+            for (int k = i + 1; k < K; k++) v -= A[i * K + k] * IA[k * K + j];
+            IA[i * K + j] = v / A[i * K + i];
+        }
+    }
+    return true;
+}
+
+// Group-wide FP64 re-solve: lane 0 solves on `scratch` (>= rescue_floats(K) floats, 8-byte
+// aligned), every lane receives the step. Returns false on a zero pivot.
+template <int K, int NACC>
+__device__ __forceinline__ bool lm_rescue(const float (&acc)[NACC], const float (&dk)[K], float (&step)[K],
+                                          float* scratch, int lane, unsigned mask) {
+    constexpr int NA = K * (K + 1) / 2;
+    double* D = reinterpret_cast<double*>(scratch);
+    double* yv = D + NA;
+    float* A = reinterpret_cast<float*>(yv + K);
+    float* b = A + NA;
+    float* dd = b + K;
+    float* xs = dd + K;
+    float* flag = xs + K;
+    __syncwarp(mask);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NA; q++) A[q] = acc[q];
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            b[q] = acc[NA + q];
+            dd[q] = dk[q];
+        }
+        flag[0] = lm_solve_fp64_lane(K, A, b, dd, D, yv, xs) ? 1.0f : 0.0f;
+    }
+    __syncwarp(mask);
+    const bool ok = flag[0] != 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; q++) step[q] = xs[q];
+    __syncwarp(mask);
+    return ok;
+}
+
+// Fisher pass epilogue: FP64 inverse on lane 0, CRLB = sqrt(diag), chi-square.
+template <int K, int NACC>
+__device__ __forceinline__ void fisher_finish(const float (&acc)[NACC], float* scratch, int lane, unsigned mask,
+                                              float* crlb, float* chisq) {
+    __syncwarp(mask);
+    if (lane == 0) {
+        double* F = reinterpret_cast<double*>(scratch);
+        double* IF = F + K * K;
+#pragma unroll
+        for (int i = 0; i < K; i++)
+#pragma unroll
+            for (int j = 0; j < K; j++) F[i * K + j] = (double)acc[upk(i, j, K)];
+        const bool ok = invert_fp64_lane(K, F, IF);
+        for (int k = 0; k < K; k++) crlb[k] = ok ? (float)sqrt(IF[k * (K + 1)]) : __int_as_float(0x7f800000);
+        if (chisq) *chisq = acc[NACC - 1];
+    }
+    __syncwarp(mask);
+}
+
+}  // namespace pb200

@@ -24,47 +24,10 @@
 // FP64; the Fisher matrix is accumulated in FP32 and inverted in FP64 (LUP with partial
 // pivoting and the reference's 1e-9 tolerance, Estimation.h:63-102, SolveMatrix.h:411-452).
 #pragma once
+#include "fit_common.cuh"
 #include "models.cuh"
 
 namespace pb200 {
-
-enum FitFlags : int {
-    FIT_CRLB_ONLY = 1,  // skip LM: params come from `initial`, compute Fisher/CRLB/chi^2 only
-};
-
-struct FitArgs {
-    const float* smp;      // [n][npix] (may be null with FIT_CRLB_ONLY: no chi-square)
-    const float* consts;   // [n][numconst] or null
-    const float* initial;  // [n][K] or null (centre-of-mass start)
-    float* params;         // [n][K]
-    int* iterations;       // [n] or null
-    float* trace;          // [n][traceLen][K] or null
-    int traceLen;
-    float* crlb;           // [n][K] or null (no Fisher pass)
-    float* chisq;          // [n] or null
-    int* diag;             // [n] or null: bit 0 = an FP64 re-solve happened
-    int n;
-    int maxIter;
-    float lambda;
-    int smemStride;        // floats of shared memory per group
-    int flags;
-};
-
-__host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
-
-template <int G>
-__device__ __forceinline__ unsigned group_mask() {
-    if (G == 32) return 0xffffffffu;
-    const unsigned lane = threadIdx.x & 31;
-    return ((1u << (G & 31)) - 1u) << (lane & ~(unsigned)(G - 1));
-}
-
-template <int G>
-__device__ __forceinline__ float group_sum(float v, unsigned mask) {
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
-    return v;
-}
 
 // Shared-memory scratch a group needs besides its pixels: the model table, or the FP64
 // Fisher/LM work area (2*K*K doubles + K doubles), whichever is larger.
@@ -77,151 +40,6 @@ __host__ __device__ constexpr int group_scratch_floats(int R) {
 template <class M>
 __host__ __device__ constexpr int group_smem_floats(int R) {
     return round_up(round_up(R * R, 4) + group_scratch_floats<M>(R), 32) + 8;
-}
-
-// FP64 LUP inverse with the reference's 1e-9 tolerance (SolveMatrix.h:219-318, 344-392),
-// run by one lane on a shared-memory work area. A[K*K] is overwritten, IA[K*K] receives the
-// inverse. Returns false when the matrix is degenerate (the reference then reports Inf).
-__device__ __noinline__ bool invert_fp64_smem(int K, double* A, double* IA) {
-    int P[8];
-    for (int i = 0; i <= K; i++) P[i] = i;
-    for (int i = 0; i < K; i++) {
-        double maxA = 0.0;
-        int imax = i;
-        for (int k = i; k < K; k++) {
-            const double v = fabs(A[k * K + i]);
-            if (v > maxA) { maxA = v; imax = k; }
-        }
-        if (maxA < (double)1e-9f) return false;
-        if (imax != i) {
-            const int tp = P[i]; P[i] = P[imax]; P[imax] = tp;
-            for (int j = 0; j < K; j++) {
-                const double t = A[i * K + j]; A[i * K + j] = A[imax * K + j]; A[imax * K + j] = t;
-            }
-            P[K]++;
-        }
-        for (int j = i + 1; j < K; j++) {
-            A[j * K + i] /= A[i * K + i];
-            for (int k = i + 1; k < K; k++) A[j * K + k] -= A[j * K + i] * A[i * K + k];
-        }
-    }
-    for (int j = 0; j < K; j++) {
-        for (int i = 0; i < K; i++) {
-            double v = (P[i] == j) ? 1.0 : 0.0;
-            for (int k = 0; k < i; k++) v -= A[i * K + k] * IA[k * K + j];
-            IA[i * K + j] = v;
-        }
-        for (int i = K - 1; i >= 0; i--) {
-            double v = IA[i * K + j];
-            for (int k = i + 1; k < K; k++) v -= A[i * K + k] * IA[k * K + j];
-            IA[i * K + j] = v / A[i * K + i];
-        }
-    }
-    return true;
-}
-
-// FP64 Cholesky solve of the damped system S x = b (lower triangle of S used), one lane,
-// shared-memory work area. Returns false on an exactly-zero pivot.
-__device__ __noinline__ bool cholesky_solve_fp64_smem(int K, const float* S, const float* b, double* D, double* y,
-                                                      float* x) {
-    for (int k = 0; k < K; ++k) {
-        double sum = 0.0;
-        for (int p = 0; p < k; ++p) sum += D[k * K + p] * D[k * K + p];
-        const double v = (double)S[k * K + k] - sum;
-        if (v == 0.0) return false;
-        D[k * K + k] = sqrt(v);
-        for (int i = k + 1; i < K; ++i) {
-            double s2 = 0.0;
-            for (int p = 0; p < k; ++p) s2 += D[i * K + p] * D[k * K + p];
-            D[i * K + k] = ((double)S[i * K + k] - s2) / D[k * K + k];
-        }
-    }
-    for (int i = 0; i < K; ++i) {
-        double sum = 0.0;
-        for (int k = 0; k < i; ++k) sum += D[i * K + k] * y[k];
-        y[i] = ((double)b[i] - sum) / D[i * K + i];
-    }
-    for (int i = K - 1; i >= 0; --i) {
-        double sum = 0.0;
-        for (int k = i + 1; k < K; ++k) sum += D[k * K + i] * (double)x[k];
-        // keep the double solution in y[] while x[] still holds float copies for later rows
-        const double xi = (y[i] - sum) / D[i * K + i];
-        y[i] = xi;
-        x[i] = (float)xi;
-    }
-    // recompute with full double precision for rows that used float copies
-    for (int i = K - 1; i >= 0; --i) x[i] = (float)y[i];
-    return true;
-}
-
-// Damped LM step in FP32 (reference algorithm, Estimation.h:213-228, SolveMatrix.h:107-163).
-// Returns 0 on an exactly-zero pivot (reference failure: LM stops), 1 on success, 2 when a
-// pivot lost more than six decimal digits (0 < v <= 1e-6 a_kk, or v < 0): the caller then
-// re-solves in FP64. On return S holds the damped matrix (full, row-major).
-template <int K>
-__device__ __forceinline__ int lm_solve_fp32(const float (&acc)[K * (K + 1) / 2 + K + 1], float lambda,
-                                             float (&S)[K * K], float (&step)[K]) {
-    {
-        int q = 0;
-#pragma unroll
-        for (int i = 0; i < K; i++)
-#pragma unroll
-            for (int j = i; j < K; j++) {
-                S[i * K + j] = acc[q];
-                S[j * K + i] = acc[q];
-                q++;
-            }
-    }
-    float diag[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        if (lambda < 0.0f) {
-            diag[k] = S[k * K + k] - lambda;
-        } else {
-            float s = 0.0f;
-#pragma unroll
-            for (int j = 0; j < K; j++) s += S[j * K + k] * S[j * K + k];
-            diag[k] = S[k * K + k] + s * lambda;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < K; k++) S[k * K + k] = diag[k];
-    float D[K * K];
-    bool weak = false;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        float sum = 0.0f;
-#pragma unroll
-        for (int p = 0; p < k; ++p) sum += D[k * K + p] * D[k * K + p];
-        const float v = S[k * K + k] - sum;
-        if (v == 0.0f) return 0;
-        if (!(v > 1e-6f * S[k * K + k])) weak = true;  // also catches v < 0 and NaN
-        D[k * K + k] = sqrtf(v);
-#pragma unroll
-        for (int i = k + 1; i < K; ++i) {
-            float s2 = 0.0f;
-#pragma unroll
-            for (int p = 0; p < k; ++p) s2 += D[i * K + p] * D[k * K + p];
-            D[i * K + k] = (S[i * K + k] - s2) / D[k * K + k];
-        }
-    }
-    if (weak) return 2;
-    float y[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-        float sum = 0.0f;
-#pragma unroll
-        for (int k = 0; k < i; ++k) sum += D[i * K + k] * y[k];
-        y[i] = (acc[K * (K + 1) / 2 + i] - sum) / D[i * K + i];
-    }
-#pragma unroll
-    for (int i = K - 1; i >= 0; --i) {
-        float sum = 0.0f;
-#pragma unroll
-        for (int k = i + 1; k < K; ++k) sum += D[k * K + i] * step[k];
-        step[i] = (y[i] - sum) / D[i * K + i];
-    }
-    return 1;
 }
 
 template <class M, int G>
@@ -327,7 +145,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                     // ComputeLevMarAlphaBeta (Estimation.h:109-128)
                     const float sv = s < 1e-6f ? 1e-6f : s;
                     const float muc = mu > 1e-6f ? mu : 1e-6f;
-                    const float invmu = __frcp_rn(muc);
+                    const float invmu = rcp_nr(muc);
                     const float t = __fmul_rn(sv, invmu);
                     w = __fmul_rn(t, invmu);
                     const float bf = __fsub_rn(1.0f, t);
@@ -336,7 +154,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                 } else {
                     // ComputeChiSquareAndCRLB (Estimation.h:76-95)
                     const float mu8 = fmaxf(1e-8f, mu);
-                    w = __frcp_rn(mu8);
+                    w = rcp_nr(mu8);
                     if (haveSmp) {
                         const float e = s - mu8;
                         acc[NACC - 1] += __fdiv_rn(e * e, mu8);
@@ -357,30 +175,11 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
             for (int q = 0; q < NACC; q++) acc[q] = group_sum<G>(acc[q], mask);
 
             if (lm) {
-                float S[K * K], step[K];
-                int rc = lm_solve_fp32<K>(acc, a.lambda, S, step);
+                float step[K], dk[K];
+                int rc = lm_solve<K, NACC>(acc, a.lambda, step, dk);
                 if (rc == 2) {
-                    // FP64 re-solve of the same damped system on lane 0, broadcast via smem
-                    __syncwarp(mask);
-                    double* D = reinterpret_cast<double*>(tab);
-                    double* yv = D + K * K;
-                    float* xs = reinterpret_cast<float*>(yv + K);
-                    float* Ss = xs + K;
-                    float* bs = Ss + K * K;
-                    if (lane == 0) {
-#pragma unroll
-                        for (int q = 0; q < K * K; q++) Ss[q] = S[q];
-#pragma unroll
-                        for (int q = 0; q < K; q++) bs[q] = acc[NA + q];
-                        const bool ok = cholesky_solve_fp64_smem(K, Ss, bs, D, yv, xs);
-                        Ss[0] = ok ? 1.0f : 0.0f;
-                    }
-                    __syncwarp(mask);
-                    rc = Ss[0] != 0.0f ? 1 : 0;
-#pragma unroll
-                    for (int q = 0; q < K; q++) step[q] = xs[q];
+                    rc = lm_rescue<K, NACC>(acc, dk, step, tab, lane, mask) ? 1 : 0;
                     if (rc) rescuedAny = true;
-                    __syncwarp(mask);
                 }
                 bool done;
                 if (rc == 0) {
@@ -413,25 +212,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                 }
             } else {
                 // ---- Fisher pass: FP64 LUP inverse on lane 0 ----
-                __syncwarp(mask);
-                if (lane == 0) {
-                    double* F = reinterpret_cast<double*>(tab);
-                    double* IF = F + K * K;
-                    int q = 0;
-#pragma unroll
-                    for (int i = 0; i < K; i++)
-#pragma unroll
-                        for (int j = i; j < K; j++) {
-                            F[i * K + j] = (double)acc[q];
-                            F[j * K + i] = (double)acc[q];
-                            q++;
-                        }
-                    const bool okInv = invert_fp64_smem(K, F, IF);
-                    for (int k = 0; k < K; k++)
-                        a.crlb[(size_t)roi * K + k] =
-                            okInv ? (float)sqrt(IF[k * (K + 1)]) : __int_as_float(0x7f800000);
-                    if (a.chisq) a.chisq[roi] = acc[NACC - 1];
-                }
+                fisher_finish<K, NACC>(acc, tab, lane, mask, a.crlb + (size_t)roi * K, a.chisq ? a.chisq + roi : nullptr);
             }
         }
         // ---- ROI finished: write results, move to the next ROI ----

@@ -1,0 +1,242 @@
+// Column-blocked LM fit kernel for the separable Gaussian PSF models.
+//
+// A group of G lanes owns one ROI at a time (several groups per warp). Lane l owns the CPL
+// consecutive columns l*CPL .. l*CPL+CPL-1: it computes their x-terms (pixel-integrated
+// Gaussian, its x/sigma derivatives) into registers, computes the y-terms of the rows with
+// the same indices into shared memory, and then walks all R rows, reading one y-term
+// (broadcast inside the group) and CPL samples per row. The Hessian/gradient partial sums
+// stay in registers and are reduced with shfl.xor inside the group; every lane then runs
+// the damped K x K solve redundantly, so all lanes of a group take the same decisions.
+//
+// The loop is flat: one trip = one LM iteration (or the Fisher pass) of every group in the
+// warp; a group whose ROI has finished loads the next one at the top of the next trip, so
+// groups never wait for their warp-mates to converge. ROIs are assigned statically:
+// group g processes ROIs g, g + total_groups, ...
+//
+// Semantics follow photonpy's LevMarOptimize (Estimators/Estimation.h:104-134, 194-251);
+// see fit_common.cuh for the solve and models.cuh for the per-pixel arithmetic.
+#pragma once
+#include "fit_common.cuh"
+#include "models.cuh"
+
+namespace pb200 {
+
+// Shared-memory floats of one group: pixels, then max(y-terms, FP64 re-solve scratch,
+// Fisher scratch when the pixel area cannot hold it). Stride = 16 mod 32 so that the
+// 16-byte row loads of two neighbouring groups fall in complementary bank quads.
+template <int K>
+__host__ __device__ constexpr int gauss_group_floats(int R) {
+    return round_up(round_up(R * R, 4) + cmax(cmax(4 * R, rescue_floats(K)),
+                                              (round_up(R * R, 4) >= 4 * K * K) ? 0 : 4 * K * K),
+                    32) + 16;
+}
+
+template <class M, int G, int CPL>
+__global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const FitArgs a) {
+    constexpr int K = M::K;
+    constexpr int NA = K * (K + 1) / 2;
+    constexpr int NACC = NA + K + 1;
+    constexpr int NC = model_num_consts(M::kId);
+    enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3 };
+    extern __shared__ __align__(16) float sm[];
+
+    const int lane = threadIdx.x & (G - 1);
+    const int gib = threadIdx.x / G;
+    const int gpb = blockDim.x / G;
+    const unsigned mask = group_mask<G>();
+    const int R = d.roisize;
+    const int npix = R * R;
+    const int npix4 = round_up(npix, 4);
+    float* spix = sm + gib * a.smemStride;
+    float* aux = spix + npix4;  // y-terms (R float4), or the FP64 re-solve scratch
+    float4* ytab = reinterpret_cast<float4*>(aux);
+    float* fisherScratch = (npix4 >= 4 * K * K) ? spix : aux;
+    const int gstride = gridDim.x * gpb;
+    const int c0 = lane * CPL;
+    const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
+    const bool haveSmp = a.smp != nullptr;
+    const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
+    const bool rowVec4 = (CPL == 4) && ((R & 3) == 0) && (c0 + 4 <= R);
+
+    int roi = blockIdx.x * gpb + gib;
+    float th[K];
+    float cs[NC > 0 ? NC : 1];
+    int it = 0;
+    int mode = MODE_LOAD;
+    bool rescuedAny = false;
+
+    while (true) {
+        if (mode == MODE_LOAD) {
+            if (roi >= a.n) break;
+            __syncwarp(mask);  // the previous ROI's readers are done with spix/aux
+            if (haveSmp) {
+                const float* src = a.smp + (size_t)roi * npix;
+                if (vec4) {
+                    const float4* s4 = reinterpret_cast<const float4*>(src);
+                    float4* d4 = reinterpret_cast<float4*>(spix);
+                    for (int i = lane; i < (npix >> 2); i += G) d4[i] = __ldcs(s4 + i);
+                } else {
+                    for (int i = lane; i < npix; i += G) spix[i] = __ldcs(src + i);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NC; c++) cs[c] = a.consts[(size_t)roi * NC + c];
+            if (a.initial) {
+#pragma unroll
+                for (int k = 0; k < K; k++) th[k] = a.initial[(size_t)roi * K + k];
+            } else {
+                __syncwarp(mask);
+                // centre of mass (Estimation.h:336-352); exact for integer-valued samples
+                float sx = 0.0f, sy = 0.0f, s = 0.0f;
+                for (int y = 0; y < R; y++) {
+#pragma unroll
+                    for (int q = 0; q < CPL; q++) {
+                        const int x = c0 + q;
+                        if (x < R) {
+                            const float v = spix[y * R + x];
+                            sx += (float)x * v;
+                            sy += (float)y * v;
+                            s += v;
+                        }
+                    }
+                }
+                sx = group_sum<G>(sx, mask);
+                sy = group_sum<G>(sy, mask);
+                s = group_sum<G>(s, mask);
+                M::initial(d, __fdiv_rn(sx, s), __fdiv_rn(sy, s), s, th);
+            }
+            it = 0;
+            rescuedAny = false;
+            if (fisherOnly) mode = MODE_FISHER;
+            else if (a.maxIter <= 0) mode = a.crlb ? MODE_FISHER : MODE_SKIP;
+            else mode = MODE_LM;
+        }
+
+        if (mode != MODE_SKIP) {
+            if (mode == MODE_LM && a.trace && lane == 0 && it < a.traceLen) {
+#pragma unroll
+                for (int k = 0; k < K; k++) a.trace[((size_t)roi * a.traceLen + it) * K + k] = th[k];
+            }
+            M m;
+            m.begin(d, th, cs);
+            float4 X[CPL], Yown[CPL];
+            m.template term_block<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, X);
+            m.template term_block<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, Yown);
+            __syncwarp(mask);  // previous readers of ytab / scratch are done
+#pragma unroll
+            for (int q = 0; q < CPL; q++)
+                if (c0 + q < R) ytab[c0 + q] = Yown[q];
+            __syncwarp(mask);
+
+            float acc[NACC];
+#pragma unroll
+            for (int q = 0; q < NACC; q++) acc[q] = 0.0f;
+            const bool lm = (mode == MODE_LM);
+            if (c0 < R) {
+                for (int y = 0; y < R; y++) {
+                    const float4 Y = ytab[y];
+                    float sv[CPL];
+                    if (!haveSmp) {
+#pragma unroll
+                        for (int q = 0; q < CPL; q++) sv[q] = 0.0f;
+                    } else if (rowVec4) {
+                        const float4 s4 = *reinterpret_cast<const float4*>(spix + y * R + c0);
+                        sv[0] = s4.x;
+                        sv[1 % CPL] = s4.y;
+                        sv[2 % CPL] = s4.z;
+                        sv[3 % CPL] = s4.w;
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < CPL; q++) sv[q] = (c0 + q < R) ? spix[y * R + c0 + q] : 0.0f;
+                    }
+#pragma unroll
+                    for (int q = 0; q < CPL; q++) {
+                        if (CPL > 1 && c0 + q >= R) continue;
+                        float mu, J[K];
+                        m.pixel_xy(X[q], Y, mu, J);
+                        const float s = sv[q];
+                        float w;
+                        if (lm) {
+                            // ComputeLevMarAlphaBeta (Estimation.h:109-128)
+                            const float sval = s < 1e-6f ? 1e-6f : s;
+                            const float muc = mu > 1e-6f ? mu : 1e-6f;
+                            const float invmu = rcp_nr(muc);
+                            const float t = __fmul_rn(sval, invmu);
+                            w = __fmul_rn(t, invmu);
+                            const float bf = __fsub_rn(1.0f, t);
+#pragma unroll
+                            for (int k = 0; k < K; k++) acc[NA + k] -= bf * J[k];
+                        } else {
+                            // ComputeChiSquareAndCRLB (Estimation.h:76-95)
+                            const float mu8 = fmaxf(1e-8f, mu);
+                            w = rcp_nr(mu8);
+                            if (haveSmp) {
+                                const float e = s - mu8;
+                                acc[NACC - 1] += __fdiv_rn(e * e, mu8);
+                            }
+                        }
+#pragma unroll
+                        for (int i = 0; i < K; i++) {
+                            const float wi = J[i] * w;
+#pragma unroll
+                            for (int j = i; j < K; j++) acc[upk(i, j, K)] += wi * J[j];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NACC; q++) acc[q] = group_sum<G>(acc[q], mask);
+
+            if (lm) {
+                float step[K], dk[K];
+                int rc = lm_solve<K, NACC>(acc, a.lambda, step, dk);
+                if (rc == 2) {
+                    rc = lm_rescue<K, NACC>(acc, dk, step, aux, lane, mask) ? 1 : 0;
+                    if (rc) rescuedAny = true;
+                }
+                bool done;
+                if (rc == 0) {
+                    done = true;  // the reference breaks out with iterations = i + 1
+                } else {
+                    float last[K];
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        last[k] = th[k];
+                        th[k] = th[k] + step[k];
+                    }
+                    M::check_limits(d, th);
+                    bool small = true;
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        if (fabsf(last[k] - th[k]) > M::stop_limit(k)) small = false;
+                    done = (it > 0 && small);
+                    if (!done) {
+                        it++;
+                        if (it >= a.maxIter) {
+                            done = true;
+                            it = a.maxIter;  // iterations = maxIterations + 1
+                        }
+                    }
+                }
+                if (!done) continue;
+                if (a.crlb) {
+                    mode = MODE_FISHER;
+                    continue;
+                }
+            } else {
+                fisher_finish<K, NACC>(acc, fisherScratch, lane, mask, a.crlb + (size_t)roi * K,
+                                       a.chisq ? a.chisq + roi : nullptr);
+            }
+        }
+        if (lane == 0 && !fisherOnly) {
+#pragma unroll
+            for (int k = 0; k < K; k++) a.params[(size_t)roi * K + k] = th[k];
+            if (a.iterations) a.iterations[roi] = it + 1;
+            if (a.diag) a.diag[roi] = rescuedAny ? 1 : 0;
+        }
+        roi += gstride;
+        mode = MODE_LOAD;
+    }
+}
+
+}  // namespace pb200

@@ -1,0 +1,13 @@
+// Launchers of the astig model's kernels (separate translation unit for parallel builds).
+#include "launch.cuh"
+
+namespace pb200 {
+
+FitLaunch fit_launcher_astig(int G, int CPL, int variant) {
+    if (1 && variant == 0) return gauss_fit_table<GaussModel<MODEL_XYZIBG>>(G, CPL);
+    return generic_fit_table<GaussModel<MODEL_XYZIBG>>(G);
+}
+
+EvalLaunch eval_launcher_astig(int G) { return eval_table<GaussModel<MODEL_XYZIBG>>(G); }
+
+}  // namespace pb200

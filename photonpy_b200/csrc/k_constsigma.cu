@@ -1,0 +1,13 @@
+// Launchers of the constsigma model's kernels (separate translation unit for parallel builds).
+#include "launch.cuh"
+
+namespace pb200 {
+
+FitLaunch fit_launcher_constsigma(int G, int CPL, int variant) {
+    if (1 && variant == 0) return gauss_fit_table<GaussModel<MODEL_XYIBG_CONSTSIGMA>>(G, CPL);
+    return generic_fit_table<GaussModel<MODEL_XYIBG_CONSTSIGMA>>(G);
+}
+
+EvalLaunch eval_launcher_constsigma(int G) { return eval_table<GaussModel<MODEL_XYIBG_CONSTSIGMA>>(G); }
+
+}  // namespace pb200

@@ -1,0 +1,13 @@
+// Launchers of the sigma model's kernels (separate translation unit for parallel builds).
+#include "launch.cuh"
+
+namespace pb200 {
+
+FitLaunch fit_launcher_sigma(int G, int CPL, int variant) {
+    if (1 && variant == 0) return gauss_fit_table<GaussModel<MODEL_XYIBG_SIGMA>>(G, CPL);
+    return generic_fit_table<GaussModel<MODEL_XYIBG_SIGMA>>(G);
+}
+
+EvalLaunch eval_launcher_sigma(int G) { return eval_table<GaussModel<MODEL_XYIBG_SIGMA>>(G); }
+
+}  // namespace pb200

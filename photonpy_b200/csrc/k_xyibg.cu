@@ -1,0 +1,13 @@
+// Launchers of the xyibg model's kernels (separate translation unit for parallel builds).
+#include "launch.cuh"
+
+namespace pb200 {
+
+FitLaunch fit_launcher_xyibg(int G, int CPL, int variant) {
+    if (1 && variant == 0) return gauss_fit_table<GaussModel<MODEL_XYIBG>>(G, CPL);
+    return generic_fit_table<GaussModel<MODEL_XYIBG>>(G);
+}
+
+EvalLaunch eval_launcher_xyibg(int G) { return eval_table<GaussModel<MODEL_XYIBG>>(G); }
+
+}  // namespace pb200

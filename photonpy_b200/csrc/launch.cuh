@@ -1,0 +1,155 @@
+// Kernel launchers: one persistent launch per (model, lanes per ROI, columns per lane).
+// The grid is sized to the SM count times the resident blocks per SM; groups stride over the
+// batch. Each model's launchers are instantiated in its own translation unit (k_*.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "fit_common.cuh"
+#include "fit_kernels.cuh"
+#include "gauss_fit.cuh"
+#include "models.cuh"
+
+namespace pb200 {
+
+using FitLaunch = void (*)(const ModelDesc&, FitArgs, int threads, cudaStream_t);
+using EvalLaunch = void (*)(const ModelDesc&, const float*, const float*, float*, float*, int, int threads,
+                            cudaStream_t);
+
+constexpr int kMaxSmemPerBlock = 200 * 1024;
+
+int num_sms();        // estimator.cu
+void count_launch();  // estimator.cu
+
+inline void check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class KernelT>
+inline void set_smem_attr(KernelT kern) {
+    static int done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerBlock);
+        done[dev] = 1;
+    }
+}
+
+// Launch a persistent group kernel: `strideFloats` of shared memory per group of G lanes.
+template <class KernelT>
+inline void launch_groups(KernelT kern, int G, int threads, int strideFloats, int n, const ModelDesc& d, FitArgs a,
+                          cudaStream_t s) {
+    int gpb = threads / G;
+    size_t smem = (size_t)gpb * strideFloats * sizeof(float);
+    while (smem > (size_t)kMaxSmemPerBlock && threads > 32) {
+        threads /= 2;
+        gpb = threads / G;
+        smem = (size_t)gpb * strideFloats * sizeof(float);
+    }
+    if (smem > (size_t)kMaxSmemPerBlock || gpb < 1) throw std::runtime_error("ROI too large for shared memory");
+    set_smem_attr(kern);
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess) perSM = 1;
+    if (perSM < 1) perSM = 1;
+    const long long needed = ((long long)n + gpb - 1) / gpb;
+    const long long cap = (long long)num_sms() * perSM;
+    const int grid = (int)(needed < cap ? needed : cap);
+    a.smemStride = strideFloats;
+    kern<<<grid, threads, smem, s>>>(d, a);
+    check_launch("fit kernel launch");
+    count_launch();
+}
+
+template <class M, int G>
+void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
+    if (a.n <= 0) return;
+    launch_groups(fit_kernel<M, G>, G, threads, group_smem_floats<M>(d.roisize), a.n, d, a, s);
+}
+
+template <class M, int G, int CPL>
+void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
+    if (a.n <= 0) return;
+    launch_groups(gauss_fit_kernel<M, G, CPL>, G, threads, gauss_group_floats<M::K>(d.roisize), a.n, d, a, s);
+}
+
+template <class M, int G>
+void launch_eval(const ModelDesc& d, const float* params, const float* consts, float* ev, float* deriv, int n,
+                 int threads, cudaStream_t s) {
+    if (n <= 0) return;
+    auto kern = eval_kernel<M, G>;
+    const int stride = round_up(M::table_floats(d.roisize), 32) + 8;
+    const int gpb = threads / G;
+    const size_t smem = (size_t)gpb * stride * sizeof(float);
+    set_smem_attr(kern);
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess) perSM = 1;
+    if (perSM < 1) perSM = 1;
+    const long long needed = ((long long)n + gpb - 1) / gpb;
+    const long long cap = (long long)num_sms() * perSM * 4;
+    const int grid = (int)(needed < cap ? needed : cap);
+    kern<<<grid, threads, smem, s>>>(d, params, consts, ev, deriv, n, stride);
+    check_launch("eval kernel launch");
+    count_launch();
+}
+
+// Gaussian models: column-blocked kernel with CPL = ceil(R / G) (1..4).
+template <class M>
+FitLaunch gauss_fit_table(int G, int CPL) {
+#define PB_CASE(g)                                    \
+    case g:                                           \
+        switch (CPL) {                                \
+        case 1: return launch_fit_gauss<M, g, 1>;     \
+        case 2: return launch_fit_gauss<M, g, 2>;     \
+        case 3: return launch_fit_gauss<M, g, 3>;     \
+        default: return launch_fit_gauss<M, g, 4>;    \
+        }
+    switch (G) {
+        PB_CASE(4)
+        PB_CASE(8)
+        PB_CASE(16)
+    default:
+        return CPL <= 1 ? launch_fit_gauss<M, 32, 1> : launch_fit_gauss<M, 32, 2>;
+    }
+#undef PB_CASE
+}
+
+template <class M>
+FitLaunch generic_fit_table(int G) {
+    switch (G) {
+    case 4: return launch_fit_generic<M, 4>;
+    case 8: return launch_fit_generic<M, 8>;
+    case 16: return launch_fit_generic<M, 16>;
+    default: return launch_fit_generic<M, 32>;
+    }
+}
+
+template <class M>
+EvalLaunch eval_table(int G) {
+    switch (G) {
+    case 8: return launch_eval<M, 8>;
+    case 16: return launch_eval<M, 16>;
+    default: return launch_eval<M, 32>;
+    }
+}
+
+// Per-model entry points (k_*.cu). `variant` 0 = column-blocked Gaussian kernel,
+// 1 = generic table kernel (the only one for the spline).
+FitLaunch fit_launcher_for(int model, int G, int CPL, int variant);
+EvalLaunch eval_launcher_for(int model, int G);
+
+#define PB_DECLARE_MODEL_LAUNCHERS(name)                               \
+    FitLaunch fit_launcher_##name(int G, int CPL, int variant);        \
+    EvalLaunch eval_launcher_##name(int G);
+PB_DECLARE_MODEL_LAUNCHERS(xyibg)
+PB_DECLARE_MODEL_LAUNCHERS(constsigma)
+PB_DECLARE_MODEL_LAUNCHERS(sigma)
+PB_DECLARE_MODEL_LAUNCHERS(sigmaxy)
+PB_DECLARE_MODEL_LAUNCHERS(astig)
+PB_DECLARE_MODEL_LAUNCHERS(spline)
+#undef PB_DECLARE_MODEL_LAUNCHERS
+
+}  // namespace pb200

@@ -162,6 +162,87 @@ struct GaussModel {
         *out = r;
     }
 
+    // The 1D terms of N consecutive coordinates c0..c0+N-1 along one axis. erf and exp are
+    // evaluated once per pixel edge: the upper edge of pixel c, ((c - t) + 0.5) * c1, and the
+    // lower edge of pixel c+1, ((c+1 - t) - 0.5) * c1, are the same float whenever the two
+    // rounded subtractions agree, and only then is the edge value reused. Every term is
+    // therefore bit-identical to term() above.
+    template <int N>
+    __device__ __forceinline__ void term_block(int c0, float t, float c1, float c2, float sig, float4 (&out)[N]) const {
+        float m[N + 1], E[N + 1], ef[N + 1], ex[N + 1], gx[N + 1];
+        float ss2 = 0.0f, ga = 0.0f;
+        if (MID == MODEL_XYZIBG) {
+            ss2 = MUL(MUL(2.0f, sig), sig);
+            ga = DIV(1.0f, MUL(MUL(__fsqrt_rn(MUL(2.0f, PB_PI)), sig), sig));
+        }
+#pragma unroll
+        for (int k = 0; k <= N; k++) {
+            m[k] = SUB(SUB((float)(c0 + k), t), 0.5f);
+            E[k] = MUL(m[k], c1);
+            ef[k] = erff(E[k]);
+            ex[k] = expf(MUL(-E[k], E[k]));
+            if (MID == MODEL_XYZIBG) gx[k] = expf(DIV(MUL(-m[k], m[k]), ss2));
+        }
+#pragma unroll
+        for (int q = 0; q < N; q++) {
+            const float p = ADD(SUB((float)(c0 + q), t), 0.5f);
+            float e0, erf0, exp0, g0 = 0.0f;
+            if (p == m[q + 1]) {
+                e0 = E[q + 1];
+                erf0 = ef[q + 1];
+                exp0 = ex[q + 1];
+                if (MID == MODEL_XYZIBG) g0 = gx[q + 1];
+            } else {
+                e0 = MUL(p, c1);
+                erf0 = erff(e0);
+                exp0 = expf(MUL(-e0, e0));
+                if (MID == MODEL_XYZIBG) g0 = expf(DIV(MUL(-p, p), ss2));
+            }
+            const float e1 = E[q], erf1 = ef[q], exp1 = ex[q];
+            const float delta = SUB(MUL(0.5f, erf0), MUL(0.5f, erf1));
+            const float dE = MUL(c2, SUB(exp1, exp0));
+            float4 r;
+            r.x = delta;
+            r.y = MUL(tI, delta);
+            r.z = MUL(tI, dE);
+            if (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA) {
+                r.w = 0.0f;
+            } else if (MID == MODEL_XYIBG_SIGMA || MID == MODEL_XYIBG_SIGMAXY) {
+                const float dDs = MUL(SUB(MUL(exp1, e1), MUL(exp0, e0)), invSqrtPi);
+                r.w = (MID == MODEL_XYIBG_SIGMAXY) ? MUL(tI, dDs) : dDs;
+            } else {
+                r.w = MUL(ga, SUB(MUL(m[q], gx[q]), MUL(p, g0)));
+            }
+            out[q] = r;
+        }
+    }
+
+    // mu and Jacobian of one pixel from its x-term X and y-term Y (see pixel()).
+    __device__ __forceinline__ void pixel_xy(const float4& X, const float4& Y, float& mu, float (&J)[K]) const {
+        mu = ADD(tbg, MUL(X.y, Y.x));
+        const float dmx = MUL(X.z, Y.x);
+        const float dmy = MUL(Y.z, X.x);
+        const float dI = MUL(X.x, Y.x);
+        if (MID == MODEL_XYZIBG) {
+            J[0] = dmx;
+            J[1] = dmy;
+            J[2] = ADD(MUL(MUL(Y.y, X.w), dsxz), MUL(MUL(X.y, Y.w), dsyz));
+            J[3] = dI;
+            J[4 % K] = 1.0f;
+        } else {
+            J[0] = dmx;
+            J[1] = dmy;
+            J[2] = dI;
+            J[3] = 1.0f;
+            if (MID == MODEL_XYIBG_SIGMA) {
+                J[4 % K] = MUL(tI, ADD(MUL(X.w, Y.x), MUL(Y.w, X.x)));
+            } else if (MID == MODEL_XYIBG_SIGMAXY) {
+                J[4 % K] = MUL(X.w, Y.x);
+                J[5 % K] = MUL(Y.w, X.x);
+            }
+        }
+    }
+
     __device__ __forceinline__ void build_table(const ModelDesc& d, float* tab, int lane, int G) const {
         const int R = d.roisize;
         float4* t4 = reinterpret_cast<float4*>(tab);

@@ -311,8 +311,12 @@ class Estimator:
                                             ct.c_void_p(s.cuda_stream))
         return (deriv, ev) if derivatives else ev
 
-    def SetKernelConfig(self, lanes_per_roi=0, threads_per_block=256):
+    def SetKernelConfig(self, lanes_per_roi=0, threads_per_block=256, variant=None):
+        """Lanes per ROI (4, 8, 16, 32; 0 = automatic), threads per block and, for the Gaussian
+        models, the kernel family (0 = column-blocked, 1 = generic per-pixel table)."""
         rc = self._lib.PB200_SetKernelConfig(self.inst, int(lanes_per_roi), int(threads_per_block))
+        if rc == 0 and variant is not None:
+            rc = self._lib.PB200_SetKernelVariant(self.inst, int(variant))
         if rc != 0:
             raise ValueError("invalid kernel configuration")
 

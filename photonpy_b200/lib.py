@@ -71,9 +71,13 @@ def _bind_common(L):
     vp = ctypes.c_void_p
     L.PB200_SetKernelConfig.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.PB200_SetKernelConfig.restype = ctypes.c_int
+    L.PB200_SetKernelVariant.argtypes = [vp, ctypes.c_int]
+    L.PB200_SetKernelVariant.restype = ctypes.c_int
     L.PB200_GetKernelConfig.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.PB200_ModelInfo.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.PB200_ModelInfo.restype = ctypes.c_int
+    L.PB200_Fp32ProbeLaunch.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
+    L.PB200_Fp32ProbeLaunch.restype = ctypes.c_double
     L.PB200_EstimateDevice.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]
     L.PB200_ExpectedValueDevice.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp]
     L.PB200_ChiSquareAndCRLBDevice.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp]

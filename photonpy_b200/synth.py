@@ -61,6 +61,43 @@ def astig_calib_nm(A=0.1, B=0.0, s0=1.3, c=150.0, d=400.0, zrange=(-600.0, 600.0
     return x, y, tuple(zrange)
 
 
+_TORCH = {"device": None, "gen": None}
+
+
+def use_torch(device, seed):
+    """Route Poisson draws and expected values of the generators below through torch on
+    `device` (much faster for million-ROI batches); None restores numpy. Ground truth is
+    still drawn with numpy's seeded generator; the Poisson stream comes from a torch
+    generator seeded with `seed`."""
+    if device is None:
+        _TORCH["device"] = None
+        _TORCH["gen"] = None
+        return
+    import torch
+    _TORCH["device"] = torch.device(device)
+    g = torch.Generator(device=_TORCH["device"])
+    g.manual_seed(int(seed))
+    _TORCH["gen"] = g
+
+
+def _gauss2d_poisson_torch(R, x, y, I, bg, sx, sy):
+    import torch
+    dev = _TORCH["device"]
+    f64 = dict(device=dev, dtype=torch.float64)
+    pix = torch.arange(R, **f64)
+
+    def delta(c, s):
+        c = torch.tensor(np.array(c, np.float64), **f64)[:, None]
+        s = torch.tensor(np.array(s, np.float64), **f64)[:, None] * SQRT2
+        return 0.5 * torch.special.erf((pix[None] - c + 0.5) / s) - 0.5 * torch.special.erf((pix[None] - c - 0.5) / s)
+
+    dx = delta(x, sx)
+    dy = delta(y, sy)
+    ev = torch.tensor(np.array(bg, np.float64), **f64)[:, None, None] + \
+        torch.tensor(np.array(I, np.float64), **f64)[:, None, None] * dy[:, :, None] * dx[:, None, :]
+    return torch.poisson(ev, generator=_TORCH["gen"]).to(torch.float32).cpu().numpy()
+
+
 def _poisson(rng, ev, chunk=1 << 22):
     out = np.empty(ev.shape, np.float32)
     flat_in = ev.reshape(-1)
@@ -68,6 +105,18 @@ def _poisson(rng, ev, chunk=1 << 22):
     for s in range(0, flat_in.size, chunk):
         flat_out[s:s + chunk] = rng.poisson(flat_in[s:s + chunk])
     return out
+
+
+def _gauss_samples(rng, R, x, y, I, bg, sx, sy, chunk):
+    """Poisson ROIs for the given truth arrays, generated chunk by chunk."""
+    sx = np.broadcast_to(np.asarray(sx, np.float64), np.shape(x))
+    sy = np.broadcast_to(np.asarray(sy, np.float64), np.shape(x))
+    if _TORCH["device"] is not None:
+        ch = 1 << 18
+        return _gen_chunks(len(x), ch, lambda a, b: _gauss2d_poisson_torch(R, x[a:b], y[a:b], I[a:b], bg[a:b],
+                                                                          sx[a:b], sy[a:b]))
+    return _gen_chunks(len(x), chunk, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
+                                                                          sx[a:b], sy[a:b])))
 
 
 def _gen_chunks(n, chunk, fn):
@@ -82,9 +131,7 @@ def xyibg(n, seed=1, R=10, sigma=1.5, xy=(4.0, 6.0)):
     I = rng.uniform(500, 5000, n)
     bg = rng.uniform(2, 10, n)
     truth = np.stack([x, y, I, bg], 1).astype(np.float32)
-    s = np.full(n, sigma)
-    smp = _gen_chunks(n, 65536, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
-                                                                     s[a:b], s[a:b])))
+    smp = _gauss_samples(rng, R, x, y, I, bg, sigma, sigma, 65536)
     return dict(kind="XYIBg", R=R, sigma=(sigma, sigma), samples=smp, truth=truth)
 
 
@@ -123,8 +170,7 @@ def sigmaxy(n, seed=2, R=16, init_sigma=1.7, xy=(6.5, 8.5)):
     I = np.exp(rng.uniform(math.log(200), math.log(20000), n))
     bg = rng.uniform(1, 20, n)
     truth = np.stack([x, y, I, bg, sx, sy], 1).astype(np.float32)
-    smp = _gen_chunks(n, 32768, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
-                                                                     sx[a:b], sy[a:b])))
+    smp = _gauss_samples(rng, R, x, y, I, bg, sx, sy, 32768)
     return dict(kind="XYIBgSigmaXY", R=R, sigma=(init_sigma, init_sigma), samples=smp, truth=truth)
 
 
@@ -140,8 +186,7 @@ def astig(n, seed=3, R=12, A=0.1, B=0.0, zr=(-400.0, 400.0), xy=None, zrange=(-6
     sx = astig_sigma(z, *cx)
     sy = astig_sigma(z, *cy)
     truth = np.stack([x, y, z, I, bg], 1).astype(np.float32)
-    smp = _gen_chunks(n, 65536, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
-                                                                     sx[a:b], sy[a:b])))
+    smp = _gauss_samples(rng, R, x, y, I, bg, sx, sy, 65536)
     return dict(kind="XYZIBg", R=R, astig=(cx, cy), zrange=zrange, samples=smp, truth=truth)
 
 
@@ -181,8 +226,7 @@ def spline(n, seed=4, R=13, zr=(-0.38, 0.38), A=0.1, B=0.0):
     sx = astig_sigma(z, *cx)
     sy = astig_sigma(z, *cy)
     truth = np.stack([x, y, z, I, bg], 1).astype(np.float32)
-    smp = _gen_chunks(n, 65536, lambda a, b: _poisson(rng, gauss2d_ev(R, x[a:b], y[a:b], I[a:b], bg[a:b],
-                                                                     sx[a:b], sy[a:b])))
+    smp = _gauss_samples(rng, R, x, y, I, bg, sx, sy, 65536)
     return dict(kind="CSpline", R=R, samples=smp, truth=truth)
 
 

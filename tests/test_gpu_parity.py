@@ -68,9 +68,12 @@ def test_expected_value_and_derivatives(name, ctx):
     n = len(g["ev"])
     c = g.get("constants")
     deriv, ev = est.Derivatives(g["truth"][:n], constants=None if c is None else c[:n])
-    assert np.allclose(ev, g["ev"], rtol=2e-5, atol=1e-5)
+    # DeltaX = 0.5 erf(a) - 0.5 erf(b) cancels in the tails, so a last-ulp difference between
+    # CUDA's and glibc's erff shows up as an absolute error of about I * ulp(1) per pixel.
+    I = g["truth"][:n, 3 if name.startswith(("astig", "spline")) else 2]
+    atol = 4 * 1.2e-7 * I[:, None, None] + 1e-5
+    assert np.all(np.abs(ev - g["ev"]) <= 2e-5 * np.abs(g["ev"]) + atol)
     scale = np.abs(g["deriv"]).max(axis=(2, 3), keepdims=True) + 1e-20
-    assert np.abs(deriv - g["deriv"]).max() / 1 <= np.inf
     assert (np.abs(deriv - g["deriv"]) / scale).max() < 1e-4
     ev2 = est.ExpectedValue(g["truth"][:n], constants=None if c is None else c[:n])
     assert np.array_equal(ev2, ev)
@@ -102,4 +105,23 @@ def test_fused_estimate_crlb_equals_separate_calls(name, ctx):
     crlb2, chisq2 = est.CRLBAndChiSquare(p, g["samples"], constants=c)
     assert np.array_equal(crlb, crlb2)
     assert np.array_equal(chisq, chisq2)
+    est.Destroy()
+
+
+@pytest.mark.parametrize("name", ["xyibg_r10", "sigmaxy_r16", "astig_r12", "constsigma_r9"])
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_kernel_variants_agree(name, lanes, ctx):
+    """The column-blocked kernel and the generic per-pixel table kernel, at every lanes-per-ROI
+    setting, give the same fits (same arithmetic, different summation order)."""
+    g = load_golden(name)
+    est = cuda_estimator(name, g, ctx)
+    c = g.get("constants")
+    est.SetKernelConfig(lanes, 256, variant=0)
+    p0, _, _, it0 = est.Estimate(g["samples"], constants=c, return_iterations=True)
+    est.SetKernelConfig(lanes, 256, variant=1)
+    p1, _, _, it1 = est.Estimate(g["samples"], constants=c, return_iterations=True)
+    conv = (it0 <= 50) & (it1 <= 50)
+    st = parity_stats(name, p0, it0, p1, it1)
+    assert st["pos_ok_converged"] >= 0.97, st
+    assert np.mean(it0 == it1) >= 0.4, st
     est.Destroy()
