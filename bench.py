@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0, help="lanes per ROI (0 = library default)")
+    ap.add_argument("--threads", type=int, default=256, help="threads per block")
+    ap.add_argument("--variant", type=int, default=None, help="Gaussian kernel family (0 column-blocked, 1 generic)")
     return ap.parse_args()
 
 
@@ -323,6 +326,7 @@ def main():
 
     ctx = pb.Context()
     est = make_estimator(pb, ctx, d)
+    est.SetKernelConfig(args.lanes, args.threads, variant=args.variant)
     x = torch.from_numpy(smp).cuda()
     peak_fp32 = fp32_peak(pb, torch)
 
@@ -335,7 +339,6 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    n_launch0 = pb.launch_count()
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -343,6 +346,7 @@ def main():
         while time.perf_counter() - t_w < 0.6:  # keep the GPU busy while nvidia-smi starts sampling
             step()
             torch.cuda.synchronize()
+        n_launch0 = pb.launch_count()
         ev0.record(stream)
         for _ in range(args.steps):
             out = step()
@@ -382,6 +386,8 @@ def main():
         def e2e_step():
             fn(est.inst, n, h_smp.data_ptr(), None, None, h_par.data_ptr(), h_its.data_ptr(), h_crlb.data_ptr(),
                h_chi.data_ptr())
+        from photonpy_b200.lib import check_error
+        check_error("PB200_EstimateCRLB")
 
         for _ in range(2):
             e2e_step()

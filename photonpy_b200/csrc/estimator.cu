@@ -161,7 +161,7 @@ struct Context {
 
 struct Slot {
     cudaStream_t stream = nullptr;
-    DevBuf smp, consts, initial, params, iters, trace, crlb, chisq;
+    DevBuf smp, consts, initial, params, iters, trace, crlb, chisq, fisher;
 };
 
 struct Estimator {
@@ -326,7 +326,10 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
             s.trace.ensure(sizeof(float) * (size_t)traceLen * K * count);
             PB_CUDA(cudaMemsetAsync(s.trace.p, 0, sizeof(float) * (size_t)traceLen * K * count, s.stream));
         }
-        if (h_crlb) s.crlb.ensure(sizeof(float) * K * count);
+        if (h_crlb) {
+            s.crlb.ensure(sizeof(float) * K * count);
+            s.fisher.ensure(sizeof(float) * fisher_row_floats(K) * count);
+        }
         if (h_chisq || h_crlb) s.chisq.ensure(sizeof(float) * count);
         FitArgs a{};
         a.smp = h_smp ? s.smp.as<float>() : nullptr;
@@ -342,7 +345,9 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         a.maxIter = e->lm.iterations;
         a.lambda = e->lm.lambda;
         a.flags = flags;
+        a.fisher = h_crlb ? s.fisher.as<float>() : nullptr;
         fl(e->desc, a, e->threads, s.stream);
+        if (h_crlb) launch_crlb(K, a.fisher, a.crlb, a.chisq, count, s.stream);
         pend.push_back({c & 1, start, count});
         if (pend.size() == 2) {
             d2h(pend.front());
@@ -570,6 +575,43 @@ Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const floa
     }
     attach(e, ctx);
     return e;
+}
+
+// Device-pointer fit on a caller stream. With a CRLB request the packed Fisher rows go to a
+// stream-ordered scratch allocation (cudaMallocAsync), which is freed on the same stream after
+// crlb_kernel has consumed it; concurrent calls on different streams therefore never share it.
+// Keep freed stream-ordered allocations in the device's default pool instead of returning them
+// to the driver at every synchronisation (repeated calls would otherwise remap memory each time).
+void keep_pool_memory() {
+    static bool done[64] = {false};
+    int dev = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    cudaMemPool_t pool;
+    PB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t threshold = UINT64_MAX;
+    PB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    done[dev] = true;
+}
+
+void run_fit_device(Estimator* e, FitArgs a, cudaStream_t s) {
+    if (a.crlb) {
+        keep_pool_memory();
+        void* scratch = nullptr;
+        const size_t bytes = sizeof(float) * fisher_row_floats(e->K) * (size_t)a.n;
+        PB_CUDA(cudaMallocAsync(&scratch, bytes, s));
+        a.fisher = static_cast<float*>(scratch);
+        try {
+            e->fit_launch()(e->desc, a, e->threads, s);
+            launch_crlb(e->K, a.fisher, a.crlb, a.chisq, a.n, s);
+        } catch (...) {
+            cudaFreeAsync(scratch, s);
+            throw;
+        }
+        PB_CUDA(cudaFreeAsync(scratch, s));
+    } else {
+        e->fit_launch()(e->desc, a, e->threads, s);
+    }
 }
 
 void check_estimator(Estimator* e) {
@@ -834,7 +876,7 @@ void PB200_EstimateDevice(Estimator* e, int numspots, const float* d_sample, con
         a.iterations = d_iterations; a.trace = traceBufLen > 0 ? d_trace : nullptr;
         a.traceLen = traceBufLen > 0 && d_trace ? traceBufLen : 0; a.crlb = d_crlb; a.chisq = d_chisq;
         a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda; a.flags = 0;
-        e->fit_launch()(e->desc, a, e->threads, (cudaStream_t)stream);});
+        run_fit_device(e, a, (cudaStream_t)stream);});
 }
 
 void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
@@ -857,7 +899,7 @@ void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_par
         FitArgs a{}; a.smp = d_sample; a.consts = d_constants; a.initial = d_params; a.params = nullptr;
         a.crlb = d_crlb; a.chisq = d_chisq; a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda;
         a.flags = FIT_CRLB_ONLY;
-        e->fit_launch()(e->desc, a, e->threads, (cudaStream_t)stream);});
+        run_fit_device(e, a, (cudaStream_t)stream);});
 }
 
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {

@@ -30,6 +30,8 @@ struct FitArgs {
     float* crlb;           // [n][K] or null (no Fisher pass)
     float* chisq;          // [n] or null
     int* diag;             // [n] or null: 1 when an FP64 re-solve happened for the spot
+    float* fisher;         // [n][K(K+1)/2 + 1] scratch: packed FP32 Fisher matrix + chi-square, inverted
+                           // afterwards by crlb_kernel; null = invert in the fit kernel (lane 0)
     int n;
     int maxIter;
     float lambda;
@@ -41,11 +43,13 @@ __host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // Packed upper-triangle index (i <= j) of a symmetric K x K matrix, row-major.
-__host__ __device__ constexpr int upk(int i, int j, int K) {
-    return i <= j ? i * K - (i * (i - 1)) / 2 + (j - i) : upk(j, i, K);
+// Written without recursion so that, inside fully unrolled loops, it folds to a constant and
+// the packed arrays it indexes stay in registers.
+__host__ __device__ __forceinline__ constexpr int upk(int i, int j, int K) {
+    return (i <= j) ? (i * K - (i * (i - 1)) / 2 + (j - i)) : (j * K - (j * (j - 1)) / 2 + (i - j));
 }
 // Packed lower-triangle index (j <= i).
-__host__ __device__ constexpr int lok(int i, int j) { return i * (i + 1) / 2 + j; }
+__host__ __device__ __forceinline__ constexpr int lok(int i, int j) { return i * (i + 1) / 2 + j; }
 
 // Floats of shared memory for the FP64 LM re-solve (doubles first: D packed, y; then floats).
 __host__ __device__ constexpr int rescue_floats(int K) { return 3 * (K * (K + 1) / 2) + 5 * K + 1; }
@@ -74,39 +78,49 @@ __device__ __forceinline__ float rcp_nr(float x) {
 
 // Damped LM step in registers. acc = [alpha upper packed (NA) | beta (K) | extra].
 // Returns 1 on success, 0 on an exactly-zero pivot (reference failure), 2 when a pivot is
-// weak and the step must be re-solved in FP64.
+// weak and the step must be re-solved in FP64. (Two-dimensional arrays and running packed
+// indices keep every access compile-time after unrolling, so nothing lands in local memory.)
 template <int K, int NACC>
 __device__ __forceinline__ int lm_solve(const float (&acc)[NACC], float lambda, float (&step)[K], float (&dk)[K]) {
     constexpr int NA = K * (K + 1) / 2;
+    float A[K][K];
+    {
+        int q = 0;
+#pragma unroll
+        for (int i = 0; i < K; i++)
+#pragma unroll
+            for (int j = i; j < K; j++) {
+                A[i][j] = acc[q];
+                A[j][i] = acc[q];
+                q++;
+            }
+    }
 #pragma unroll
     for (int k = 0; k < K; k++) {
-        if (lambda < 0.0f) {
-            dk[k] = acc[upk(k, k, K)] - lambda;
-        } else {
-            float s = 0.0f;
+        float s = 0.0f;
 #pragma unroll
-            for (int j = 0; j < K; j++) s += acc[upk(j, k, K)] * acc[upk(j, k, K)];
-            dk[k] = acc[upk(k, k, K)] + s * lambda;
-        }
+        for (int j = 0; j < K; j++) s += A[j][k] * A[j][k];
+        dk[k] = (lambda < 0.0f) ? A[k][k] - lambda : A[k][k] + s * lambda;
     }
-    float L[NA], Linv[K];
+    float L[K][K], Linv[K];
+    int status = 1;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         float sum = 0.0f;
 #pragma unroll
-        for (int p = 0; p < k; ++p) sum += L[lok(k, p)] * L[lok(k, p)];
+        for (int p = 0; p < k; ++p) sum += L[k][p] * L[k][p];
         const float v = dk[k] - sum;
-        if (v == 0.0f) return 0;
-        if (!(v > 1e-6f * dk[k])) return 2;  // also catches v < 0 and NaN
+        if (v == 0.0f) status = 0;
+        else if (!(v > 1e-6f * dk[k]) && status == 1) status = 2;  // also catches v < 0 and NaN
         const float inv = rsqrtf(v);
-        L[lok(k, k)] = v * inv;
+        L[k][k] = v * inv;
         Linv[k] = inv;
 #pragma unroll
         for (int i = k + 1; i < K; ++i) {
             float s2 = 0.0f;
 #pragma unroll
-            for (int p = 0; p < k; ++p) s2 += L[lok(i, p)] * L[lok(k, p)];
-            L[lok(i, k)] = (acc[upk(i, k, K)] - s2) * inv;
+            for (int p = 0; p < k; ++p) s2 += L[i][p] * L[k][p];
+            L[i][k] = (A[i][k] - s2) * inv;
         }
     }
     float y[K];
@@ -114,17 +128,17 @@ __device__ __forceinline__ int lm_solve(const float (&acc)[NACC], float lambda, 
     for (int i = 0; i < K; ++i) {
         float sum = 0.0f;
 #pragma unroll
-        for (int k = 0; k < i; ++k) sum += L[lok(i, k)] * y[k];
+        for (int k = 0; k < i; ++k) sum += L[i][k] * y[k];
         y[i] = (acc[NA + i] - sum) * Linv[i];
     }
 #pragma unroll
     for (int i = K - 1; i >= 0; --i) {
         float sum = 0.0f;
 #pragma unroll
-        for (int k = i + 1; k < K; ++k) sum += L[lok(k, i)] * step[k];
+        for (int k = i + 1; k < K; ++k) sum += L[k][i] * step[k];
         step[i] = (y[i] - sum) * Linv[i];
     }
-    return 1;
+    return status;
 }
 
 // FP64 Cholesky solve by one lane. A: packed upper (float, NA), b: K, dk: damped diagonal.
@@ -229,7 +243,96 @@ __device__ __forceinline__ bool lm_rescue(const float (&acc)[NACC], const float 
     return ok;
 }
 
-// Fisher pass epilogue: FP64 inverse on lane 0, CRLB = sqrt(diag), chi-square.
+// Fisher pass epilogue, deferred form: the group's lanes store the packed FP32 Fisher matrix
+// and the chi-square of ROI `roi` into the scratch row; crlb_kernel inverts it later.
+template <int K, int NACC, int G>
+__device__ __forceinline__ void fisher_store(const float (&acc)[NACC], float* row, int lane) {
+    constexpr int NA = K * (K + 1) / 2;
+#pragma unroll
+    for (int q = 0; q < NA; q++)
+        if ((q % G) == lane) row[q] = acc[q];
+    if (lane == ((NA) % G)) row[NA] = acc[NACC - 1];
+}
+
+// One thread per ROI: FP64 LUP inverse of the packed Fisher matrix (reference algorithm and
+// 1e-9 tolerance, SolveMatrix.h:219-318, 344-392), CRLB = sqrt(diag) (+Inf when singular, as
+// Estimation.h:101 via InvertMatrix), chi-square copied out.
+template <int K>
+__global__ void __launch_bounds__(128) crlb_kernel(const float* __restrict__ fisher, float* __restrict__ crlb,
+                                                   float* __restrict__ chisq, int n) {
+    constexpr int NA = K * (K + 1) / 2;
+    for (int roi = blockIdx.x * blockDim.x + threadIdx.x; roi < n; roi += gridDim.x * blockDim.x) {
+        const float* row = fisher + (size_t)roi * (NA + 1);
+        double A[K][K];
+        {
+            int q = 0;
+#pragma unroll
+            for (int i = 0; i < K; i++)
+#pragma unroll
+                for (int j = i; j < K; j++) {
+                    const double v = (double)row[q++];
+                    A[i][j] = v;
+                    A[j][i] = v;
+                }
+        }
+        int P[K];
+#pragma unroll
+        for (int i = 0; i < K; i++) P[i] = i;
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            double maxA = 0.0;
+            int imax = i;
+#pragma unroll
+            for (int k = i; k < K; k++) {
+                const double v = fabs(A[k][i]);
+                if (v > maxA) { maxA = v; imax = k; }
+            }
+            if (maxA < (double)1e-9f) ok = false;
+            // row swap i <-> imax with compile-time indices only
+#pragma unroll
+            for (int r = i + 1; r < K; r++) {
+                if (r == imax) {
+                    const int tp = P[i]; P[i] = P[r]; P[r] = tp;
+#pragma unroll
+                    for (int j = 0; j < K; j++) {
+                        const double t = A[i][j]; A[i][j] = A[r][j]; A[r][j] = t;
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = i + 1; j < K; j++) {
+                A[j][i] /= A[i][i];
+#pragma unroll
+                for (int k = i + 1; k < K; k++) A[j][k] -= A[j][i] * A[i][k];
+            }
+        }
+        // column j of the inverse: forward (unit lower) then backward substitution; keep the diagonal
+        float* out = crlb + (size_t)roi * K;
+#pragma unroll
+        for (int j = 0; j < K; j++) {
+            double x[K];
+#pragma unroll
+            for (int i = 0; i < K; i++) {
+                double v = (P[i] == j) ? 1.0 : 0.0;
+#pragma unroll
+                for (int k = 0; k < i; k++) v -= A[i][k] * x[k];
+                x[i] = v;
+            }
+#pragma unroll
+            for (int i = K - 1; i >= 0; i--) {
+                double v = x[i];
+#pragma unroll
+                for (int k = i + 1; k < K; k++) v -= A[i][k] * x[k];
+                x[i] = v / A[i][i];
+            }
+            out[j] = ok ? (float)sqrt(x[j]) : __int_as_float(0x7f800000);
+        }
+        if (chisq) chisq[roi] = row[NA];
+    }
+}
+
+// Fisher pass epilogue, in-kernel form: FP64 inverse on lane 0, CRLB = sqrt(diag), chi-square.
 template <int K, int NACC>
 __device__ __forceinline__ void fisher_finish(const float (&acc)[NACC], float* scratch, int lane, unsigned mask,
                                               float* crlb, float* chisq) {
@@ -237,10 +340,15 @@ __device__ __forceinline__ void fisher_finish(const float (&acc)[NACC], float* s
     if (lane == 0) {
         double* F = reinterpret_cast<double*>(scratch);
         double* IF = F + K * K;
+        int q = 0;
 #pragma unroll
         for (int i = 0; i < K; i++)
 #pragma unroll
-            for (int j = 0; j < K; j++) F[i * K + j] = (double)acc[upk(i, j, K)];
+            for (int j = i; j < K; j++) {
+                F[i * K + j] = (double)acc[q];
+                F[j * K + i] = (double)acc[q];
+                q++;
+            }
         const bool ok = invert_fp64_lane(K, F, IF);
         for (int k = 0; k < K; k++) crlb[k] = ok ? (float)sqrt(IF[k * (K + 1)]) : __int_as_float(0x7f800000);
         if (chisq) *chisq = acc[NACC - 1];

@@ -211,8 +211,10 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                     continue;
                 }
             } else {
-                // ---- Fisher pass: FP64 LUP inverse on lane 0 ----
-                fisher_finish<K, NACC>(acc, tab, lane, mask, a.crlb + (size_t)roi * K, a.chisq ? a.chisq + roi : nullptr);
+                // ---- Fisher pass: deferred FP64 inverse (crlb_kernel), or on lane 0 ----
+                if (a.fisher) fisher_store<K, NACC, G>(acc, a.fisher + (size_t)roi * (NA + 1), lane);
+                else fisher_finish<K, NACC>(acc, tab, lane, mask, a.crlb + (size_t)roi * K,
+                                            a.chisq ? a.chisq + roi : nullptr);
             }
         }
         // ---- ROI finished: write results, move to the next ROI ----

@@ -175,11 +175,12 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
                                 acc[NACC - 1] += __fdiv_rn(e * e, mu8);
                             }
                         }
+                        int qa = 0;
 #pragma unroll
                         for (int i = 0; i < K; i++) {
                             const float wi = J[i] * w;
 #pragma unroll
-                            for (int j = i; j < K; j++) acc[upk(i, j, K)] += wi * J[j];
+                            for (int j = i; j < K; j++) acc[qa++] += wi * J[j];
                         }
                     }
                 }
@@ -223,6 +224,8 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
                     mode = MODE_FISHER;
                     continue;
                 }
+            } else if (a.fisher) {
+                fisher_store<K, NACC, G>(acc, a.fisher + (size_t)roi * (NA + 1), lane);
             } else {
                 fisher_finish<K, NACC>(acc, fisherScratch, lane, mask, a.crlb + (size_t)roi * K,
                                        a.chisq ? a.chisq + roi : nullptr);

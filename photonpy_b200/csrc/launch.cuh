@@ -28,14 +28,13 @@ inline void check_launch(const char* what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Opt the kernel in to more than 48 KB of dynamic shared memory. Set on every launch: the
+// attribute is per kernel and per device, and the call costs about a microsecond.
 template <class KernelT>
-inline void set_smem_attr(KernelT kern) {
-    static int done[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerBlock);
-        done[dev] = 1;
+inline void set_smem_attr(KernelT kern, size_t smem) {
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
 }
 
@@ -51,10 +50,10 @@ inline void launch_groups(KernelT kern, int G, int threads, int strideFloats, in
         smem = (size_t)gpb * strideFloats * sizeof(float);
     }
     if (smem > (size_t)kMaxSmemPerBlock || gpb < 1) throw std::runtime_error("ROI too large for shared memory");
-    set_smem_attr(kern);
+    set_smem_attr(kern, smem);
     int perSM = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess) perSM = 1;
-    if (perSM < 1) perSM = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess || perSM < 1)
+        throw std::runtime_error("fit kernel: occupancy query failed");
     const long long needed = ((long long)n + gpb - 1) / gpb;
     const long long cap = (long long)num_sms() * perSM;
     const int grid = (int)(needed < cap ? needed : cap);
@@ -84,10 +83,10 @@ void launch_eval(const ModelDesc& d, const float* params, const float* consts, f
     const int stride = round_up(M::table_floats(d.roisize), 32) + 8;
     const int gpb = threads / G;
     const size_t smem = (size_t)gpb * stride * sizeof(float);
-    set_smem_attr(kern);
+    set_smem_attr(kern, smem);
     int perSM = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess) perSM = 1;
-    if (perSM < 1) perSM = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess || perSM < 1)
+        throw std::runtime_error("eval kernel: occupancy query failed");
     const long long needed = ((long long)n + gpb - 1) / gpb;
     const long long cap = (long long)num_sms() * perSM * 4;
     const int grid = (int)(needed < cap ? needed : cap);
@@ -135,6 +134,23 @@ EvalLaunch eval_table(int G) {
     default: return launch_eval<M, 32>;
     }
 }
+
+// FP64 CRLB from the packed Fisher scratch rows (one thread per ROI).
+inline void launch_crlb(int K, const float* fisher, float* crlb, float* chisq, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    const int threads = 128;
+    const int grid = (n + threads - 1) / threads < 65535 * 4 ? (n + threads - 1) / threads : 65535 * 4;
+    switch (K) {
+    case 4: crlb_kernel<4><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
+    case 5: crlb_kernel<5><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
+    case 6: crlb_kernel<6><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
+    default: throw std::runtime_error("crlb: unsupported number of parameters");
+    }
+    check_launch("crlb kernel launch");
+    count_launch();
+}
+
+inline int fisher_row_floats(int K) { return K * (K + 1) / 2 + 1; }
 
 // Per-model entry points (k_*.cu). `variant` 0 = column-blocked Gaussian kernel,
 // 1 = generic table kernel (the only one for the spline).

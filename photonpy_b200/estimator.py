@@ -15,7 +15,7 @@ import numpy as np
 import numpy.ctypeslib as ctl
 
 from .context import Context
-from .lib import NullableFloatArrayType, NullableIntArrayType
+from .lib import NullableFloatArrayType, NullableIntArrayType, check_error
 
 
 class EstimatorProperties(ct.Structure):
@@ -276,6 +276,7 @@ class Estimator:
         if n > 0:
             self._EstimateCRLB(self.inst, n, imgs, constants if self.numconst else None, initial, params, its, crlb,
                                chisq)
+            check_error("EstimateWithCRLB")
         return params, its, crlb, chisq
 
     def EstimateDevice(self, imgs, constants=None, initial=None, with_crlb=True, trace_len=0, stream=None):
@@ -296,6 +297,7 @@ class Estimator:
         self._lib.PB200_EstimateDevice(self.inst, n, _ptr(imgs), _ptr(constants), _ptr(initial), _ptr(out["params"]),
                                        _ptr(out["iterations"]), _ptr(out.get("trace")), int(trace_len),
                                        _ptr(out.get("crlb")), _ptr(out.get("chisq")), ct.c_void_p(s.cuda_stream))
+        check_error("EstimateDevice")
         return out
 
     def ExpectedValueDevice(self, params, constants=None, derivatives=False, stream=None):
@@ -309,6 +311,7 @@ class Estimator:
         s = stream if stream is not None else torch.cuda.current_stream(params.device)
         self._lib.PB200_ExpectedValueDevice(self.inst, n, _ptr(params), _ptr(constants), _ptr(ev), _ptr(deriv),
                                             ct.c_void_p(s.cuda_stream))
+        check_error("ExpectedValueDevice")
         return (deriv, ev) if derivatives else ev
 
     def SetKernelConfig(self, lanes_per_roi=0, threads_per_block=256, variant=None):

@@ -36,3 +36,18 @@ def ctx():
     c = pb.Context()
     yield c
     c.Destroy()
+
+
+@pytest.fixture(autouse=True)
+def no_native_error(request):
+    """GPU tests fail if any C-ABI call reported an error (the reference-compatible API only
+    prints errors and leaves outputs zero)."""
+    if request.node.get_closest_marker("gpu") is None:
+        yield
+        return
+    import photonpy_b200 as pb
+    from photonpy_b200 import lib
+    lib.clear_error()
+    yield
+    msg = pb.last_error()
+    assert msg == "", f"native error: {msg}"
