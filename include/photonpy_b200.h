@@ -166,6 +166,20 @@ void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params
                                float* d_ev, float* d_deriv, void* stream);
 void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_params, const float* d_sample,
                                   const float* d_constants, float* d_crlb, float* d_chisq, void* stream);
+/* No counterpart in the reference. Fused fit + CRLB + chi-square like PB200_EstimateDevice,
+ * for callers that must not allocate device memory during a fit (real-time acquisition loops
+ * with all device memory reserved in advance, hosts whose memory must come from their own
+ * pools): it calls no cudaMalloc/cudaFree or other allocating routine. Its only scratch, the
+ * packed Fisher rows, lives in a fixed device array of 32768 spots x 22 floats (2.75 MiB per
+ * GPU that loads the library, kept until exit), so numspots above 32768 is rejected with an
+ * error (split the batch). All pointers are device memory; d_crlb is required, d_iterations and
+ * d_chisq may be NULL. The first call on a device looks up the array's device address; make
+ * that first call before any stream capture. Every call shares the array and overwrites the
+ * rows it uses, so calls whose kernels overlap on the GPU (other streams, other threads) race:
+ * serialise them. Returns 0 on success, -1 on error (message in PB200_GetLastError). */
+int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                              const float* d_initial, float* d_params, int* d_iterations, float* d_crlb,
+                              float* d_chisq, void* stream);
 /* Kernel configuration used for this estimator: lanes per ROI (4, 8, 16, 32; 0 = automatic)
  * and threads per block (64..256). Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);

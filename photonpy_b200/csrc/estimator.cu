@@ -931,6 +931,81 @@ int PB200_ModelInfo(Estimator* e, int* roisize) {
     return e->desc.model;
 }
 
+// ---- allocation-free fused fit + CRLB ----
+// Some callers must not allocate device memory while they fit: acquisition software that
+// fits frames from a real-time loop with all of its device memory reserved up front (a
+// cudaMalloc or cudaFree there can stall until other streams finish, or fail half-way through
+// a run), and host frameworks whose memory may only come from their own pools. For them the
+// fused path keeps its one piece of scratch, the packed Fisher rows, in the fixed array below.
+}  // extern "C"
+
+namespace {
+// Largest batch one PB200_EstimateCRLBNoAlloc call accepts.
+constexpr int kNoAllocMaxSpots = 32768;
+// Packed Fisher matrix of up to K = 6 parameters (21 floats) plus the chi-square.
+constexpr int kNoAllocRowFloats = 22;
+// 32768 x 22 floats = 2.75 MiB, reserved on every GPU that loads this library until exit.
+static __device__ __align__(256) float g_noallocFisher[kNoAllocMaxSpots * kNoAllocRowFloats];
+
+// Device address of g_noallocFisher on the current device. In host code the array's name is
+// only a host-side stand-in, so the real address is looked up once per device, with that
+// device current, and cached.
+float* noalloc_scratch() {
+    static std::mutex mtx;
+    static float* addr[64] = {nullptr};
+    int dev = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error("PB200_EstimateCRLBNoAlloc: device index out of range");
+    std::lock_guard<std::mutex> g(mtx);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&p, g_noallocFisher);
+        if (rc != cudaSuccess)
+            throw Error(std::string("PB200_EstimateCRLBNoAlloc: cudaGetSymbolAddress failed: ") +
+                        cudaGetErrorString(rc));
+        addr[dev] = static_cast<float*>(p);
+    }
+    return addr[dev];
+}
+}  // namespace
+
+extern "C" {
+
+int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                              const float* d_initial, float* d_params, int* d_iterations, float* d_crlb,
+                              float* d_chisq, void* stream) {
+    if (numspots == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            check_estimator(e);
+            if (numspots < 0 || numspots > kNoAllocMaxSpots)
+                throw Error("PB200_EstimateCRLBNoAlloc: numspots must be in [0, " + std::to_string(kNoAllocMaxSpots) +
+                            "], got " + std::to_string(numspots) + "; split the batch");
+            if (!d_sample || !d_params || !d_crlb) throw Error("PB200_EstimateCRLBNoAlloc: null sample/params/crlb");
+            if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+            if (fisher_row_floats(e->K) > kNoAllocRowFloats) throw Error("PB200_EstimateCRLBNoAlloc: too many parameters");
+            float* scratch = noalloc_scratch();
+            FitArgs a{};
+            a.smp = d_sample;
+            a.consts = d_constants;
+            a.initial = d_initial;
+            a.params = d_params;
+            a.iterations = d_iterations;
+            a.crlb = d_crlb;
+            a.chisq = d_chisq;
+            a.fisher = scratch;
+            a.n = numspots;
+            a.maxIter = e->lm.iterations;
+            a.lambda = e->lm.lambda;
+            a.flags = 0;
+            const cudaStream_t s = (cudaStream_t)stream;
+            e->fit_launch()(e->desc, a, e->threads, s);
+            launch_crlb(e->K, scratch, d_crlb, d_chisq, numspots, s);
+            return 0;
+        },
+        -1);
+}
+
 // ---- loader-time exports ----
 int CudaGetNumDevices(void) {
     int n = 0;
