@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sigmaxy", choices=["sigmaxy", "xyibg", "astig", "spline"])
+    ap.add_argument("--workload", default="sigmaxy", choices=["sigmaxy", "xyibg", "astig", "spline", "mixed"])
+    ap.add_argument("--tile", type=int, default=8, help="mixed workload: ROIs per tile")
     ap.add_argument("--n", type=int, default=None, help="ROIs per GPU (default: the workload's size)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -68,6 +69,8 @@ WORKLOADS = {
     "xyibg": dict(n=1_000_000, desc="XYIBg 10x10 fixed-sigma 2D Gaussian MLE + CRLB"),
     "astig": dict(n=1_000_000, desc="XYZIBg 12x12 astigmatic 3D Gaussian MLE + CRLB (reference 4-term form)"),
     "spline": dict(n=500_000, desc="CSpline XYZIBg 13x13 cubic-spline 3D MLE + CRLB"),
+    "mixed": dict(n=4_000_000, desc="mixed batch: ROI sizes {7,9,11,16} p={.2,.3,.3,.2}, 50% XYIBg / 30% "
+                                    "XYIBgSigmaXY / 20% astig XYZIBg, LM + CRLB"),
 }
 
 
@@ -297,10 +300,118 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def mixed_estimator(pb, ctx, g):
+    G = pb.GaussianPSFMethods(ctx)
+    if g["kind"] == "XYIBg":
+        return G.CreatePSF_XYIBg(g["R"], g["sigma"], True)
+    if g["kind"] == "XYIBgSigmaXY":
+        return G.CreatePSF_XYIBgSigmaXY(g["R"], g["sigma"], True)
+    cx, cy = g["astig"]
+    return G.CreatePSF_XYZIBg(g["R"], pb.Gauss3D_Calibration(cx[:4], cy[:4], g["zrange"]), True)
+
+
+def run_mixed(args):
+    """Mixed workload: one persistent graph-replayed launch (fused) vs one launch per
+    (model, ROI size) bucket (plain), device-resident inputs; CPU and reference-GPU baselines."""
+    import torch
+    import photonpy_b200 as pb
+    from photonpy_b200 import roofline, synth
+    from photonpy_b200.mixed import MixedBatch
+    w = WORKLOADS["mixed"]
+    n = args.n or w["n"]
+    synth.use_torch("cuda", 5)
+    groups = synth.mixed(n, seed=5)
+    ctx = pb.Context()
+    ests = [mixed_estimator(pb, ctx, g) for g in groups]
+    xs = [torch.from_numpy(g["samples"]).cuda() for g in groups]
+    mb = MixedBatch(list(zip(ests, xs)), tile_rois=args.tile, threads=args.threads)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        mb.run(s)
+        s.synchronize()
+        mb.capture(s)
+
+    def timed(fn, k):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        s.synchronize()
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record(s)
+        for _ in range(k):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    with torch.cuda.stream(s):
+        with ClockSampler(0) as clk:
+            n0 = pb.launch_count()
+            ms_fused = timed(lambda: mb.run(s), args.steps)
+            launches = pb.launch_count() - n0
+        ms_plain = timed(lambda: mb.run_plain(s), args.steps)
+    flops = 0.0
+    for g, r in zip(groups, mb.results()):
+        flops += roofline.localization_flops(g["kind"], g["R"], r["iterations"].cpu().numpy(), MAX_IT)
+    peak = fp32_peak(pb, torch)
+    # baselines on a bounded proportional sample: reference CPU estimator and the reference's own
+    # one-thread-per-ROI GPU kernels (through its host API, copies included)
+    cpu = ref_gpu = None
+    from oracle import ref_lib
+    if ref_lib.available() and not args.no_cpu_baseline:
+        frac = min(1.0, 60000 / n)
+        tot, t_cpu, t_gpu = 0, 0.0, 0.0
+        for g in groups:
+            m = max(1, int(len(g["samples"]) * frac))
+            sub = dict(g, samples=g["samples"][:m])
+            dt, kind = cpu_localize(sub, sub["samples"])
+            t_cpu += dt
+            est = ref_gpu_estimator(g)
+            t0 = time.perf_counter()
+            p, _, _ = est.estimate(sub["samples"], trace_len=0)
+            est.crlb_chisq(p, sub["samples"])
+            t_gpu += time.perf_counter() - t0
+            est.close()
+            tot += m
+        cpu = dict(value=tot / t_cpu, unit=UNIT, cores=os.cpu_count(), kind="reference",
+                   sample=f"{tot} ROIs ({frac:.3%} of every bucket), Estimate + ChiSquareAndCRLB")
+        ref_gpu = dict(value=tot / t_gpu, unit=UNIT,
+                       what="photonpy's own one-thread-per-ROI CUDA kernels built for sm_100a, one call per "
+                            "bucket through its host API (host copies included)", sample=f"{tot} ROIs")
+    line = dict(
+        metric=METRIC, value=n / (ms_fused * 1e-3), unit=UNIT, n_gpus=1, steps=args.steps, warmup=max(args.warmup, 3),
+        ms_per_step=ms_fused, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+        data="synthetic (seeded Poisson ROIs, photonpy_b200.synth)",
+        config=dict(workload=w["desc"], rois=n, buckets=len(groups), tile_rois=args.tile, lanes_per_roi=4,
+                    graph_replay=True, lm_iterations=MAX_IT, lm_lambda=LAMBDA,
+                    l2="inputs of %.2f GB per step exceed the 126 MB L2" % (sum(x.numel() for x in xs) * 4 / 1e9)),
+        plain_gpu=dict(value=n / (ms_plain * 1e-3), ms_per_step=ms_plain, launches_per_step=2 * len(groups),
+                       what="one fit launch + one CRLB launch per (model, ROI size) bucket, same kernels"),
+        fused_over_plain=ms_plain / ms_fused,
+        roofline=dict(bound="fp32", achieved=flops / (ms_fused * 1e-3) / 1e12, peak=peak, unit="TFLOP/s",
+                      frac=flops / (ms_fused * 1e-3) / 1e12 / peak if peak else None, traffic=None,
+                      peak_source="FP32 FMA probe measured in this run"),
+        cpu_baseline=cpu, reference_gpu_plain=ref_gpu, gpu_launches=int(launches), clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+    mb.close()
+    ctx.Destroy()
+
+
+def ref_gpu_estimator(d):
+    from oracle import ref_lib
+    k = d["kind"]
+    if k in ("XYIBg", "XYIBgSigmaXY"):
+        return ref_lib.RefEstimator(k, d["R"], cuda=True, sigma=d["sigma"])
+    cx, cy = d["astig"]
+    return ref_lib.RefEstimator(k, d["R"], cuda=True, astig=(cx[:4], cy[:4]), zrange=d["zrange"])
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "mixed":
+        run_mixed(args)
         return
     import torch
     import torch.distributed as dist

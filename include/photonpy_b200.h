@@ -25,6 +25,7 @@ extern "C" {
 
 typedef struct Estimator Estimator; /* opaque */
 typedef struct Context Context;     /* opaque */
+typedef struct MixedPlan MixedPlan; /* opaque */
 
 /* LMParams, Estimators/Estimator.h:18-26. `factor` is accepted and unused, as in the reference. */
 typedef struct LMParams {
@@ -128,6 +129,39 @@ void Estimator_ComputeDerivatives(Estimator* e, int numspots, const float* param
 void Estimator_ChiSquareAndCRLB(Estimator* e, const float* params, const float* sample, const float* constants,
                                 const int* spotpos, int numspots, float* crlb, float* chisq);
 
+/* ---- Estimation queue, Estimators/EstimationQueue.h:21-25, 112-126 --------------------
+ * Streams ROIs from host memory through the fused fit + CRLB + chi-square kernels: spots are
+ * packed into pinned batches of batchSize; a worker thread launches waiting batches on
+ * numStreams CUDA streams (numStreams < 0: 3), several full batches per launch when they
+ * are waiting; results are collected per batch. GetResults returns only whole batches,
+ * removes them from the queue, and does not keep batch order (sort by id). Differences from
+ * the reference, none of which changes a result: maxQueueLen counts SPOTS (waiting or in
+ * flight) and EstimQueue_Schedule blocks on entry while that count is at least
+ * max(maxQueueLen, batchSize); a batch never mixes spots scheduled with and without initial
+ * values (a change flushes the batch); roipos is returned as scheduled; diag is ignored
+ * (numDiag is 0). */
+typedef struct EstimQueue EstimQueue;  /* opaque; the reference's EstimationQueue */
+typedef struct EstimatorResult {       /* Estimators/EstimationQueue.h:21-25 */
+    int id;
+    float chisq;
+    int iterations;
+} EstimatorResult;
+EstimQueue* EstimQueue_Create(Estimator* psf, int batchSize, int maxQueueLen, bool keepSamples, int numStreams,
+                              Context* ctx);                                   /* EstimationQueue.cpp:317 */
+void EstimQueue_Delete(EstimQueue* q);                                         /* EstimationQueue.cpp:336 */
+/* ids[n], samples[n][H][W], initial[n][K] (nullable), constants[n][numConst] (nullable when
+ * numConst is 0), roipos[n][2]; copied before the call returns. EstimationQueue.cpp:346 */
+void EstimQueue_Schedule(EstimQueue* q, int numspots, const int* ids, const float* h_samples, const float* h_initial,
+                         const float* h_constants, const int* h_roipos);
+void EstimQueue_Flush(EstimQueue* q);                                          /* EstimationQueue.cpp:357 */
+bool EstimQueue_IsIdle(EstimQueue* q);                                         /* EstimationQueue.cpp:367 */
+int EstimQueue_GetResultCount(EstimQueue* q);                                  /* EstimationQueue.cpp:378 */
+int EstimQueue_GetQueueLength(EstimQueue* q);                                  /* EstimationQueue.cpp:389 */
+/* Copies whole finished batches while they fit in maxresults; every output nullable (samples
+ * only when the queue keeps them). Returns the number of spots copied. EstimationQueue.cpp:402 */
+int EstimQueue_GetResults(EstimQueue* q, int maxresults, float* estim, float* diag, float* crlb, int* roipos,
+                          float* samples, EstimatorResult* results);
+
 /* ---- Loader-time exports bound eagerly by photonpy/cpp/lib.py ------------------------ */
 int CudaGetNumDevices(void);                                                        /* CudaUtils.cu:12 */
 bool CudaSetDevice(int index);                                                      /* CudaUtils.cu:19 */
@@ -166,6 +200,33 @@ void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params
                                float* d_ev, float* d_deriv, void* stream);
 void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_params, const float* d_sample,
                                   const float* d_constants, float* d_crlb, float* d_chisq, void* stream);
+/* Adjoint of the summed Poisson NLL (no reference counterpart). For each spot n:
+ * nll[n] = sum_p mu_p - x_p log(max(mu_p, 1e-6)); dparams[n][k] = g_n dNLL_n/dtheta_k (true
+ * derivatives, also for sigma); d_dcalib is ACCUMULATED into (zero it first): sum_n g_n dNLL_n/dcal
+ * for XYIBg (sigma_x, sigma_y: 2 floats), XYZIBg (s0, gamma, d, A, B for x then y: 10 floats) and
+ * CSpline (one value per coefficient, the coefficient array's shape). g_n = d_gradOut[n] or 1.
+ * `calib` (host, nullable) overrides the estimator's sigma pair (XYIBg) or astig coefficients
+ * (XYZIBg, 10 floats); d_coefs (device, nullable) overrides the spline coefficients. Device
+ * pointers, caller stream; d_nll/d_dparams/d_dcalib nullable. Returns 0 or -1 (error). */
+int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, const float* d_params,
+                            const float* d_constants, const float* calib, const float* d_coefs, const float* d_gradOut,
+                            float* d_nll, float* d_dparams, float* d_dcalib, void* stream);
+/* Mixed batches (no reference counterpart; photonpy runs one estimator, i.e. one model and
+ * ROI size, per call). A plan binds nbuckets (estimator, count, device buffers) groups; one
+ * run fits all of them in a single persistent launch in which warps claim tiles of tileRois
+ * ROIs of one bucket from a counter, followed by the FP64 CRLB kernels. Buckets must be
+ * Gaussian models with ROI size <= 16. d_constants/d_iterations/d_crlb/d_chisq arrays (and
+ * their entries) may be NULL. The plan owns its scratch (task table, tile counter, Fisher
+ * rows). threadsPerBlock selects the kernel's register budget: 128 (3 blocks per SM),
+ * 256 (2 blocks per SM), 129 (128 threads, 4 blocks per SM). PB200_MixedPlanCapture records one run into a CUDA graph on `stream` (non-default);
+ * later PB200_MixedPlanRun calls replay it. Runs of one plan must not overlap. */
+MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int* counts, const float* const* d_samples,
+                                 const float* const* d_constants, float* const* d_params, int* const* d_iterations,
+                                 float* const* d_crlb, float* const* d_chisq, int tileRois, int threadsPerBlock);
+int PB200_MixedPlanRun(MixedPlan* plan, void* stream);
+int PB200_MixedPlanCapture(MixedPlan* plan, void* stream);
+int PB200_MixedPlanInfo(MixedPlan* plan, int* ntasks, int* totalTiles, int* strideFloats);
+void PB200_MixedPlanDestroy(MixedPlan* plan);
 /* No counterpart in the reference. Fused fit + CRLB + chi-square like PB200_EstimateDevice,
  * for callers that must not allocate device memory during a fit (real-time acquisition loops
  * with all device memory reserved in advance, hosts whose memory must come from their own

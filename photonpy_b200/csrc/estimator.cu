@@ -18,11 +18,14 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
 #include "../../include/photonpy_b200.h"
+#include "host_internal.h"
 #include "launch.cuh"
+#include "mixed.cuh"
 
 using namespace pb200;
 
@@ -123,6 +126,18 @@ FitLaunch fit_launcher_for(int model, int G, int CPL, int variant) {
     throw Error("unknown model");
 }
 
+AdjointLaunch adjoint_launcher_for(int model) {
+    switch (model) {
+    case MODEL_XYIBG: return adjoint_launcher_xyibg();
+    case MODEL_XYIBG_CONSTSIGMA: return adjoint_launcher_constsigma();
+    case MODEL_XYIBG_SIGMA: return adjoint_launcher_sigma();
+    case MODEL_XYIBG_SIGMAXY: return adjoint_launcher_sigmaxy();
+    case MODEL_XYZIBG: return adjoint_launcher_astig();
+    case MODEL_CSPLINE: return adjoint_launcher_spline();
+    }
+    throw Error("unknown model");
+}
+
 EvalLaunch eval_launcher_for(int model, int G) {
     switch (model) {
     case MODEL_XYIBG: return eval_launcher_xyibg(G);
@@ -157,7 +172,27 @@ struct Estimator;
 struct Context {
     std::mutex mtx;
     std::unordered_set<Estimator*> objects;
+    std::unordered_map<void*, void (*)(void*)> owned;  // queues and other non-estimator objects
 };
+
+namespace pb200 {
+void context_attach(Context* ctx, void* obj, void (*destroy)(void*)) {
+    if (!ctx) return;
+    std::lock_guard<std::mutex> g(ctx->mtx);
+    ctx->owned[obj] = destroy;
+}
+
+void context_detach(Context* ctx, void* obj) {
+    if (!ctx) return;
+    std::lock_guard<std::mutex> g(ctx->mtx);
+    ctx->owned.erase(obj);
+}
+
+void set_last_error(const std::string& msg) {
+    t_lastError = msg;
+    debug_printf("%s\n", msg.c_str());
+}
+}  // namespace pb200
 
 struct Slot {
     cudaStream_t stream = nullptr;
@@ -653,11 +688,15 @@ Context* Context_Create(void) { return new Context(); }
 void Context_Destroy(Context* ctx) {
     if (!ctx) return;
     std::vector<Estimator*> objs;
+    std::vector<std::pair<void*, void (*)(void*)>> owned;
     {
         std::lock_guard<std::mutex> g(ctx->mtx);
         objs.assign(ctx->objects.begin(), ctx->objects.end());
         ctx->objects.clear();
+        owned.assign(ctx->owned.begin(), ctx->owned.end());
+        ctx->owned.clear();
     }
+    for (auto& o : owned) o.second(o.first);  // queues first: they use the estimators
     for (auto* e : objs) {
         e->ctx = nullptr;
         delete e;
@@ -930,6 +969,210 @@ int PB200_ModelInfo(Estimator* e, int* roisize) {
     if (roisize) *roisize = e->desc.roisize;
     return e->desc.model;
 }
+
+int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, const float* d_params,
+                            const float* d_constants, const float* calib, const float* d_coefs, const float* d_gradOut,
+                            float* d_nll, float* d_dparams, float* d_dcalib, void* stream) {
+    if (numspots == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            check_estimator(e);
+            if (numspots < 0 || !d_sample || !d_params) throw Error("PoissonNLLAdjoint: bad arguments");
+            if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+            ModelDesc d = e->desc;
+            if (calib) {
+                if (d.model == MODEL_XYIBG) {
+                    d.sigma[0] = calib[0];
+                    d.sigma[1] = calib[1];
+                } else if (d.model == MODEL_XYZIBG) {
+                    for (int i = 0; i < 5; i++) {
+                        d.astig_x[i] = calib[i];
+                        d.astig_y[i] = calib[5 + i];
+                    }
+                }
+            }
+            if (d_coefs && d.model == MODEL_CSPLINE) d.coefs = d_coefs;
+            AdjointArgs a{};
+            a.smp = d_sample;
+            a.params = d_params;
+            a.consts = d_constants;
+            a.gradOut = d_gradOut;
+            a.nll = d_nll;
+            a.dparams = d_dparams;
+            a.dcalib = d_dcalib;
+            a.n = numspots;
+            adjoint_launcher_for(d.model)(d, a, (cudaStream_t)stream);
+            return 0;
+        },
+        -1);
+}
+
+// ---- mixed-model, mixed-size batches in one persistent launch ----
+}  // extern "C"
+
+struct MixedPlan {
+    int device = 0;
+    int ntasks = 0, totalTiles = 0, tileRois = 32, variant = 0, strideFloats = 0;
+    std::vector<MixedTask> tasks;
+    std::vector<int> K;
+    DevBuf dTasks, dCounter, dFisher;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+    ~MixedPlan() {
+        if (graphExec) cudaGraphExecDestroy(graphExec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+void mixed_enqueue(MixedPlan* p, cudaStream_t s) {
+    PB_CUDA(cudaMemsetAsync(p->dCounter.p, 0, sizeof(int), s));
+    launch_mixed(p->dTasks.as<MixedTask>(), p->ntasks, p->totalTiles, p->tileRois, p->dCounter.as<int>(),
+                 p->strideFloats, p->variant, s);
+    for (int b = 0; b < p->ntasks; b++) {
+        const FitArgs& a = p->tasks[b].a;
+        if (a.crlb) launch_crlb(p->K[b], a.fisher, a.crlb, a.chisq, a.n, s);
+    }
+}
+}  // namespace
+
+extern "C" {
+
+MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int* counts, const float* const* d_samples,
+                                 const float* const* d_constants, float* const* d_params, int* const* d_iterations,
+                                 float* const* d_crlb, float* const* d_chisq, int tileRois, int threadsPerBlock) {
+    return guarded(
+        [&]() -> MixedPlan* {
+            if (nbuckets <= 0 || !ests || !counts || !d_samples || !d_params)
+                throw Error("MixedPlanCreate: bad arguments");
+            if (tileRois < 1) tileRois = 32;
+            auto* p = new MixedPlan();
+            try {
+                PB_CUDA(cudaGetDevice(&p->device));
+                p->tileRois = tileRois;
+                // threadsPerBlock picks the kernel variant: 128 (3 blocks/SM, inlined handlers),
+                // 256 (2 blocks/SM, separate handlers), 129 (128 threads, 4 blocks/SM, separate handlers)
+                p->variant = threadsPerBlock == 256 ? 1 : (threadsPerBlock == 129 ? 2 : 0);
+                const int G = mixed_lanes();
+                size_t fisherFloats = 0;
+                for (int b = 0; b < nbuckets; b++) {
+                    Estimator* e = ests[b];
+                    check_estimator(e);
+                    const int R = e->desc.roisize;
+                    const int cpl = (R + G - 1) / G;
+                    if (e->desc.model == MODEL_CSPLINE || cpl > 4)
+                        throw Error("MixedPlanCreate: buckets must be Gaussian models with ROI size <= 16");
+                    if (counts[b] < 0) throw Error("MixedPlanCreate: negative count");
+                    if (e->numconst && counts[b] > 0 && (!d_constants || !d_constants[b]))
+                        throw Error("MixedPlanCreate: a bucket needs per-spot constants");
+                    if (d_crlb && d_crlb[b]) fisherFloats += (size_t)fisher_row_floats(e->K) * counts[b];
+                }
+                p->dFisher.ensure(sizeof(float) * (fisherFloats ? fisherFloats : 1));
+                size_t off = 0;
+                for (int b = 0; b < nbuckets; b++) {
+                    Estimator* e = ests[b];
+                    if (counts[b] == 0) continue;
+                    MixedTask t{};
+                    t.d = e->desc;
+                    FitArgs& a = t.a;
+                    a.smp = d_samples[b];
+                    a.consts = d_constants ? d_constants[b] : nullptr;
+                    a.params = d_params[b];
+                    a.iterations = d_iterations ? d_iterations[b] : nullptr;
+                    a.crlb = d_crlb ? d_crlb[b] : nullptr;
+                    a.chisq = d_chisq ? d_chisq[b] : nullptr;
+                    a.n = counts[b];
+                    a.maxIter = e->lm.iterations;
+                    a.lambda = e->lm.lambda;
+                    if (a.crlb) {
+                        a.fisher = p->dFisher.as<float>() + off;
+                        off += (size_t)fisher_row_floats(e->K) * counts[b];
+                    }
+                    t.tileBegin = p->totalTiles;
+                    const int cpl = (e->desc.roisize + G - 1) / G;
+                    t.handler = e->desc.model * 4 + cpl - 1;
+                    p->totalTiles += (counts[b] + tileRois - 1) / tileRois;
+                    switch (e->K) {
+                    case 4: p->strideFloats = std::max(p->strideFloats, gauss_group_floats<4>(e->desc.roisize)); break;
+                    case 5: p->strideFloats = std::max(p->strideFloats, gauss_group_floats<5>(e->desc.roisize)); break;
+                    default: p->strideFloats = std::max(p->strideFloats, gauss_group_floats<6>(e->desc.roisize)); break;
+                    }
+                    p->tasks.push_back(t);
+                    p->K.push_back(e->K);
+                }
+                p->ntasks = (int)p->tasks.size();
+                p->dTasks.ensure(sizeof(MixedTask) * std::max(1, p->ntasks));
+                if (p->ntasks)
+                    PB_CUDA(cudaMemcpy(p->dTasks.p, p->tasks.data(), sizeof(MixedTask) * p->ntasks,
+                                       cudaMemcpyHostToDevice));
+                p->dCounter.ensure(sizeof(int));
+            } catch (...) {
+                delete p;
+                throw;
+            }
+            return p;
+        },
+        (MixedPlan*)nullptr);
+}
+
+int PB200_MixedPlanRun(MixedPlan* p, void* stream) {
+    return guarded(
+        [&]() -> int {
+            if (!p) throw Error("MixedPlanRun: null plan");
+            if (p->ntasks == 0) return 0;
+            const cudaStream_t s = (cudaStream_t)stream;
+            if (p->graphExec) {
+                PB_CUDA(cudaGraphLaunch(p->graphExec, s));
+                for (int b = 0; b <= p->ntasks; b++)  // the graph holds the fit kernel and one CRLB kernel per bucket
+                    if (b == p->ntasks || p->tasks[b].a.crlb) count_launch();
+            } else {
+                mixed_enqueue(p, s);
+            }
+            return 0;
+        },
+        -1);
+}
+
+int PB200_MixedPlanCapture(MixedPlan* p, void* stream) {
+    return guarded(
+        [&]() -> int {
+            if (!p) throw Error("MixedPlanCapture: null plan");
+            if (p->ntasks == 0) return 0;
+            const cudaStream_t s = (cudaStream_t)stream;
+            if (!s) throw Error("MixedPlanCapture: needs a non-default stream");
+            if (p->graphExec) {
+                cudaGraphExecDestroy(p->graphExec);
+                p->graphExec = nullptr;
+            }
+            if (p->graph) {
+                cudaGraphDestroy(p->graph);
+                p->graph = nullptr;
+            }
+            PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+            try {
+                mixed_enqueue(p, s);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            PB_CUDA(cudaStreamEndCapture(s, &p->graph));
+            PB_CUDA(cudaGraphInstantiate(&p->graphExec, p->graph, 0));
+            return 0;
+        },
+        -1);
+}
+
+int PB200_MixedPlanInfo(MixedPlan* p, int* ntasks, int* totalTiles, int* strideFloats) {
+    if (!p) return -1;
+    if (ntasks) *ntasks = p->ntasks;
+    if (totalTiles) *totalTiles = p->totalTiles;
+    if (strideFloats) *strideFloats = p->strideFloats;
+    return 0;
+}
+
+void PB200_MixedPlanDestroy(MixedPlan* p) { delete p; }
 
 // ---- allocation-free fused fit + CRLB ----
 // Some callers must not allocate device memory while they fit: acquisition software that

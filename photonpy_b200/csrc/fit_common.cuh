@@ -76,6 +76,13 @@ __device__ __forceinline__ float rcp_nr(float x) {
     return fmaf(r, e, r);
 }
 
+// 1/x with the approximate reciprocal alone (within 1 ulp), for the per-pixel LM weights.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Damped LM step in registers. acc = [alpha upper packed (NA) | beta (K) | extra].
 // Returns 1 on success, 0 on an exactly-zero pivot (reference failure), 2 when a pivot is
 // weak and the step must be re-solved in FP64. (Two-dimensional arrays and running packed

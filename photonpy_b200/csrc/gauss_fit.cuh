@@ -24,41 +24,35 @@ namespace pb200 {
 // Shared-memory floats of one group: pixels, then max(y-terms, FP64 re-solve scratch,
 // Fisher scratch when the pixel area cannot hold it). Stride = 16 mod 32 so that the
 // 16-byte row loads of two neighbouring groups fall in complementary bank quads.
-template <int K>
+template <int K, int NE = 3>
 __host__ __device__ constexpr int gauss_group_floats(int R) {
-    return round_up(round_up(R * R, 4) + cmax(cmax(4 * R, rescue_floats(K)),
+    return round_up(round_up(R * R, 4) + cmax(cmax(cmax(4 * R, 2 * (R + 1) * NE), rescue_floats(K)),
                                               (round_up(R * R, 4) >= 4 * K * K) ? 0 : 4 * K * K),
                     32) + 16;
 }
 
+// Fit the ROIs roi, roi + roiStep, ... < roiEnd of one (model, ROI size) with one group of G
+// lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_floats floats).
 template <class M, int G, int CPL>
-__global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const FitArgs a) {
+__device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArgs& a, int roi, const int roiEnd,
+                                                const int roiStep, float* spix, const int lane, const unsigned mask) {
     constexpr int K = M::K;
     constexpr int NA = K * (K + 1) / 2;
     constexpr int NACC = NA + K + 1;
     constexpr int NC = model_num_consts(M::kId);
     enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3 };
-    extern __shared__ __align__(16) float sm[];
-
-    const int lane = threadIdx.x & (G - 1);
-    const int gib = threadIdx.x / G;
-    const int gpb = blockDim.x / G;
-    const unsigned mask = group_mask<G>();
     const int R = d.roisize;
     const int npix = R * R;
     const int npix4 = round_up(npix, 4);
-    float* spix = sm + gib * a.smemStride;
     float* aux = spix + npix4;  // y-terms (R float4), or the FP64 re-solve scratch
     float4* ytab = reinterpret_cast<float4*>(aux);
     float* fisherScratch = (npix4 >= 4 * K * K) ? spix : aux;
-    const int gstride = gridDim.x * gpb;
     const int c0 = lane * CPL;
     const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
     const bool haveSmp = a.smp != nullptr;
     const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
     const bool rowVec4 = (CPL == 4) && ((R & 3) == 0) && (c0 + 4 <= R);
 
-    int roi = blockIdx.x * gpb + gib;
     float th[K];
     float cs[NC > 0 ? NC : 1];
     int it = 0;
@@ -67,7 +61,7 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
 
     while (true) {
         if (mode == MODE_LOAD) {
-            if (roi >= a.n) break;
+            if (roi >= roiEnd) break;
             __syncwarp(mask);  // the previous ROI's readers are done with spix/aux
             if (haveSmp) {
                 const float* src = a.smp + (size_t)roi * npix;
@@ -119,10 +113,22 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
             }
             M m;
             m.begin(d, th, cs);
-            float4 X[CPL], Yown[CPL];
-            m.template term_block<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, X);
-            m.template term_block<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, Yown);
+            // erf/exp at the 2(R+1) pixel edges, lane-strided so that neighbouring lanes (and the
+            // same lane of every group in the warp) evaluate neighbouring edges: erff's branches
+            // stay coherent across the warp
+            constexpr int NE = M::kEdgeFloats;
+            float* ex = aux;
+            float* ey = aux + (R + 1) * NE;
             __syncwarp(mask);  // previous readers of ytab / scratch are done
+            for (int e = lane; e < 2 * (R + 1); e += G) {
+                if (e <= R) m.edge(e, m.tx, m.cx1, m.sigx, ex + e * NE);
+                else m.edge(e - (R + 1), m.ty, m.cy1, m.sigy, ey + (e - (R + 1)) * NE);
+            }
+            __syncwarp(mask);
+            float4 X[CPL], Yown[CPL];
+            m.template terms_from_edges<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, ex, R, X);
+            m.template terms_from_edges<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, ey, R, Yown);
+            __syncwarp(mask);  // every lane has read its edges before ytab overwrites them
 #pragma unroll
             for (int q = 0; q < CPL; q++)
                 if (c0 + q < R) ytab[c0 + q] = Yown[q];
@@ -157,10 +163,10 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
                         const float s = sv[q];
                         float w;
                         if (lm) {
-                            // ComputeLevMarAlphaBeta (Estimation.h:109-128)
-                            const float sval = s < 1e-6f ? 1e-6f : s;
-                            const float muc = mu > 1e-6f ? mu : 1e-6f;
-                            const float invmu = rcp_nr(muc);
+                            // ComputeLevMarAlphaBeta (Estimation.h:109-128); a NaN sample counts as 1e-6
+                            const float sval = fmaxf(s, 1e-6f);
+                            const float muc = fmaxf(mu, 1e-6f);
+                            const float invmu = rcp_fast(muc);
                             const float t = __fmul_rn(sval, invmu);
                             w = __fmul_rn(t, invmu);
                             const float bf = __fsub_rn(1.0f, t);
@@ -237,9 +243,21 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
             if (a.iterations) a.iterations[roi] = it + 1;
             if (a.diag) a.diag[roi] = rescuedAny ? 1 : 0;
         }
-        roi += gstride;
+        roi += roiStep;
         mode = MODE_LOAD;
     }
+}
+
+
+// Standalone launch: every group of the grid strides over the whole batch.
+template <class M, int G, int CPL>
+__global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const FitArgs a) {
+    extern __shared__ __align__(16) float sm[];
+    const int lane = threadIdx.x & (G - 1);
+    const int gib = threadIdx.x / G;
+    const int gpb = blockDim.x / G;
+    gauss_fit_range<M, G, CPL>(d, a, blockIdx.x * gpb + gib, a.n, gridDim.x * gpb, sm + gib * a.smemStride, lane,
+                               group_mask<G>());
 }
 
 }  // namespace pb200

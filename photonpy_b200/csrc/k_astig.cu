@@ -10,4 +10,6 @@ FitLaunch fit_launcher_astig(int G, int CPL, int variant) {
 
 EvalLaunch eval_launcher_astig(int G) { return eval_table<GaussModel<MODEL_XYZIBG>>(G); }
 
+AdjointLaunch adjoint_launcher_astig() { return launch_adjoint<GaussModel<MODEL_XYZIBG>, 8>; }
+
 }  // namespace pb200

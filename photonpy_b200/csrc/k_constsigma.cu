@@ -10,4 +10,6 @@ FitLaunch fit_launcher_constsigma(int G, int CPL, int variant) {
 
 EvalLaunch eval_launcher_constsigma(int G) { return eval_table<GaussModel<MODEL_XYIBG_CONSTSIGMA>>(G); }
 
+AdjointLaunch adjoint_launcher_constsigma() { return launch_adjoint<GaussModel<MODEL_XYIBG_CONSTSIGMA>, 8>; }
+
 }  // namespace pb200

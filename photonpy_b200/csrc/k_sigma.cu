@@ -10,4 +10,6 @@ FitLaunch fit_launcher_sigma(int G, int CPL, int variant) {
 
 EvalLaunch eval_launcher_sigma(int G) { return eval_table<GaussModel<MODEL_XYIBG_SIGMA>>(G); }
 
+AdjointLaunch adjoint_launcher_sigma() { return launch_adjoint<GaussModel<MODEL_XYIBG_SIGMA>, 8>; }
+
 }  // namespace pb200

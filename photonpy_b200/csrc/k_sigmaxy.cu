@@ -10,4 +10,6 @@ FitLaunch fit_launcher_sigmaxy(int G, int CPL, int variant) {
 
 EvalLaunch eval_launcher_sigmaxy(int G) { return eval_table<GaussModel<MODEL_XYIBG_SIGMAXY>>(G); }
 
+AdjointLaunch adjoint_launcher_sigmaxy() { return launch_adjoint<GaussModel<MODEL_XYIBG_SIGMAXY>, 8>; }
+
 }  // namespace pb200

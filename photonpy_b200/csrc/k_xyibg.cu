@@ -10,4 +10,6 @@ FitLaunch fit_launcher_xyibg(int G, int CPL, int variant) {
 
 EvalLaunch eval_launcher_xyibg(int G) { return eval_table<GaussModel<MODEL_XYIBG>>(G); }
 
+AdjointLaunch adjoint_launcher_xyibg() { return launch_adjoint<GaussModel<MODEL_XYIBG>, 8>; }
+
 }  // namespace pb200

@@ -9,12 +9,14 @@
 
 #include "fit_common.cuh"
 #include "fit_kernels.cuh"
+#include "adjoint.cuh"
 #include "gauss_fit.cuh"
 #include "models.cuh"
 
 namespace pb200 {
 
 using FitLaunch = void (*)(const ModelDesc&, FitArgs, int threads, cudaStream_t);
+using AdjointLaunch = void (*)(const ModelDesc&, AdjointArgs, cudaStream_t);
 using EvalLaunch = void (*)(const ModelDesc&, const float*, const float*, float*, float*, int, int threads,
                             cudaStream_t);
 
@@ -72,7 +74,8 @@ void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t
 template <class M, int G, int CPL>
 void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
     if (a.n <= 0) return;
-    launch_groups(gauss_fit_kernel<M, G, CPL>, G, threads, gauss_group_floats<M::K>(d.roisize), a.n, d, a, s);
+    launch_groups(gauss_fit_kernel<M, G, CPL>, G, threads, gauss_group_floats<M::K, M::kEdgeFloats>(d.roisize), a.n,
+                  d, a, s);
 }
 
 template <class M, int G>
@@ -92,6 +95,26 @@ void launch_eval(const ModelDesc& d, const float* params, const float* consts, f
     const int grid = (int)(needed < cap ? needed : cap);
     kern<<<grid, threads, smem, s>>>(d, params, consts, ev, deriv, n, stride);
     check_launch("eval kernel launch");
+    count_launch();
+}
+
+template <class M, int G>
+void launch_adjoint(const ModelDesc& d, AdjointArgs a, cudaStream_t s) {
+    if (a.n <= 0) return;
+    auto kern = adjoint_kernel<M, G>;
+    const int threads = 256;
+    a.smemStride = adjoint_group_floats<M>(d.roisize);
+    const int gpb = threads / G;
+    const size_t smem = (size_t)gpb * a.smemStride * sizeof(float);
+    set_smem_attr(kern, smem);
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, smem) != cudaSuccess || perSM < 1)
+        throw std::runtime_error("adjoint kernel: occupancy query failed");
+    const long long needed = ((long long)a.n + gpb - 1) / gpb;
+    const long long cap = (long long)num_sms() * perSM;
+    const int grid = (int)(needed < cap ? needed : cap);
+    kern<<<grid, threads, smem, s>>>(d, a);
+    check_launch("adjoint kernel launch");
     count_launch();
 }
 
@@ -152,6 +175,12 @@ inline void launch_crlb(int K, const float* fisher, float* crlb, float* chisq, i
 
 inline int fisher_row_floats(int K) { return K * (K + 1) / 2 + 1; }
 
+// Mixed-model persistent kernel (k_mixed.cu).
+struct MixedTask;
+int mixed_lanes();
+void launch_mixed(const MixedTask* d_tasks, int ntasks, int totalTiles, int tileRois, int* d_counter,
+                  int strideFloats, int variant, cudaStream_t s);
+
 // Per-model entry points (k_*.cu). `variant` 0 = column-blocked Gaussian kernel,
 // 1 = generic table kernel (the only one for the spline).
 FitLaunch fit_launcher_for(int model, int G, int CPL, int variant);
@@ -159,7 +188,8 @@ EvalLaunch eval_launcher_for(int model, int G);
 
 #define PB_DECLARE_MODEL_LAUNCHERS(name)                               \
     FitLaunch fit_launcher_##name(int G, int CPL, int variant);        \
-    EvalLaunch eval_launcher_##name(int G);
+    EvalLaunch eval_launcher_##name(int G);                            \
+    AdjointLaunch adjoint_launcher_##name();
 PB_DECLARE_MODEL_LAUNCHERS(xyibg)
 PB_DECLARE_MODEL_LAUNCHERS(constsigma)
 PB_DECLARE_MODEL_LAUNCHERS(sigma)

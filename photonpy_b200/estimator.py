@@ -279,20 +279,23 @@ class Estimator:
             check_error("EstimateWithCRLB")
         return params, its, crlb, chisq
 
-    def EstimateDevice(self, imgs, constants=None, initial=None, with_crlb=True, trace_len=0, stream=None):
-        """Fit torch CUDA tensors in place on the device (no host copies, no synchronisation).
-        Returns dict(params, iterations, crlb, chisq[, trace]) of torch tensors."""
+    def EstimateDevice(self, imgs, constants=None, initial=None, with_crlb=True, trace_len=0, stream=None,
+                       out=None):
+        """Fit torch CUDA tensors on the device (no host copies, no synchronisation).
+        Returns dict(params, iterations, crlb, chisq[, trace]) of torch tensors; `out` may
+        supply preallocated tensors for any of them."""
         import torch
         n = imgs.shape[0]
         dev = imgs.device
         assert imgs.is_cuda and imgs.dtype == torch.float32 and imgs.is_contiguous()
-        out = dict(params=torch.empty((n, self.numparams), device=dev, dtype=torch.float32),
-                   iterations=torch.empty(n, device=dev, dtype=torch.int32))
+        out = dict(out or {})
+        out.setdefault("params", torch.empty((n, self.numparams), device=dev, dtype=torch.float32))
+        out.setdefault("iterations", torch.empty(n, device=dev, dtype=torch.int32))
         if with_crlb:
-            out["crlb"] = torch.empty((n, self.numparams), device=dev, dtype=torch.float32)
-            out["chisq"] = torch.empty(n, device=dev, dtype=torch.float32)
+            out.setdefault("crlb", torch.empty((n, self.numparams), device=dev, dtype=torch.float32))
+            out.setdefault("chisq", torch.empty(n, device=dev, dtype=torch.float32))
         if trace_len > 0:
-            out["trace"] = torch.zeros((n, trace_len, self.numparams), device=dev, dtype=torch.float32)
+            out.setdefault("trace", torch.zeros((n, trace_len, self.numparams), device=dev, dtype=torch.float32))
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         self._lib.PB200_EstimateDevice(self.inst, n, _ptr(imgs), _ptr(constants), _ptr(initial), _ptr(out["params"]),
                                        _ptr(out["iterations"]), _ptr(out.get("trace")), int(trace_len),

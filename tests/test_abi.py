@@ -23,7 +23,9 @@ def test_header_declares_reference_abi():
     for must in ["Estimator_Estimate", "Estimator_ChiSquareAndCRLB", "Estimator_ComputeDerivatives",
                  "Estimator_ComputeExpectedValue", "Gauss2D_CreatePSF_XYIBg", "Gauss2D_CreatePSF_XYIBgSigmaXY",
                  "Gauss2D_CreatePSF_XYZIBg", "CSpline_CreatePSF", "CSpline_Compute", "Context_Create",
-                 "Context_Destroy", "Estimator_GetParamLimits", "Estimator_SetLMParams"]:
+                 "Context_Destroy", "Estimator_GetParamLimits", "Estimator_SetLMParams", "EstimQueue_Create",
+                 "EstimQueue_Delete", "EstimQueue_Schedule", "EstimQueue_Flush", "EstimQueue_IsIdle",
+                 "EstimQueue_GetResultCount", "EstimQueue_GetQueueLength", "EstimQueue_GetResults"]:
         assert must in names
 
 
