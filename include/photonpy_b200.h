@@ -129,6 +129,18 @@ void Estimator_ComputeDerivatives(Estimator* e, int numspots, const float* param
 void Estimator_ChiSquareAndCRLB(Estimator* e, const float* params, const float* sample, const float* constants,
                                 const int* spotpos, int numspots, float* crlb, float* chisq);
 
+/* ---- Likelihood-ratio test, Estimators/GLRT_PSF.cu:58-170 ---------------------------
+ * GLRT_CreatePSF returns an estimator with the model's parameters, limits and fit whose
+ * Estimate also writes 3 diagnostics per spot (numDiag = 3): ll_on = sum d log(mu) - mu at
+ * the fitted parameters, ll_off = sum d log(mean) - mean for the background-only model, and
+ * mean; d = max(sample, 1e-8), mu clamped at 1e-8 (GLRT_PSF.cu:104-131). The reference takes
+ * `mean` from the FIRST ROI of the call for every spot (its inner loop variable shadows the
+ * spot index, GLRT_PSF.cu:107-108); here each spot uses its own mean unless
+ * PB200_SetGLRTReferenceMean(e, 1) selects the reference's behaviour (extension, returns 0 or
+ * -1). The GLRT estimator is a copy of `model` (deleting the model does not affect it). */
+Estimator* GLRT_CreatePSF(Estimator* model, Context* ctx);                     /* GLRT_PSF.cu:156 */
+int PB200_SetGLRTReferenceMean(Estimator* e, int on);
+
 /* ---- Estimation queue, Estimators/EstimationQueue.h:21-25, 112-126 --------------------
  * Streams ROIs from host memory through the fused fit + CRLB + chi-square kernels: spots are
  * packed into pinned batches of batchSize; a worker thread launches waiting batches on
@@ -138,8 +150,9 @@ void Estimator_ChiSquareAndCRLB(Estimator* e, const float* params, const float* 
  * the reference, none of which changes a result: maxQueueLen counts SPOTS (waiting or in
  * flight) and EstimQueue_Schedule blocks on entry while that count is at least
  * max(maxQueueLen, batchSize); a batch never mixes spots scheduled with and without initial
- * values (a change flushes the batch); roipos is returned as scheduled; diag is ignored
- * (numDiag is 0). */
+ * values (a change flushes the batch); roipos is returned as scheduled; diag receives
+ * numDiag floats per spot (the GLRT values for GLRT estimators, none otherwise). Inputs are
+ * staged in a bounded pool of pinned buffers: Schedule also waits while all are in use. */
 typedef struct EstimQueue EstimQueue;  /* opaque; the reference's EstimationQueue */
 typedef struct EstimatorResult {       /* Estimators/EstimationQueue.h:21-25 */
     int id;
@@ -198,6 +211,11 @@ void PB200_EstimateDevice(Estimator* e, int numspots, const float* d_sample, con
                           float* d_crlb, float* d_chisq, void* stream);
 void PB200_ExpectedValueDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
                                float* d_ev, float* d_deriv, void* stream);
+/* PB200_EstimateDevice with the per-spot diagnostics of the estimator (numDiag floats per spot:
+ * 3 for GLRT estimators, none otherwise; d_diag nullable) and without the trace. */
+void PB200_EstimateDeviceDiag(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                              const float* d_initial, float* d_params, float* d_diag, int* d_iterations,
+                              float* d_crlb, float* d_chisq, void* stream);
 void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_params, const float* d_sample,
                                   const float* d_constants, float* d_crlb, float* d_chisq, void* stream);
 /* Adjoint of the summed Poisson NLL (no reference counterpart). For each spot n:

@@ -75,7 +75,8 @@ NVCC=${NVCC:-nvcc}
 FLAGS=(-x cu -std=c++17 -O3 -Xcompiler -fPIC,-fpermissive,-w,-O3 --expt-extended-lambda --expt-relaxed-constexpr
        -gencode arch=compute_100a,code=sm_100a -I. -IEstimators -include msvc_compat.h -DNDEBUG)
 SRCS=(Estimators/Estimator.cpp StringUtils.cpp Context.cpp DebugImageCallback.cpp Rendering.cpp CudaUtils.cu
-      Estimators/EstimatorImpl.cu Estimators/Gaussian/GaussianPSF.cu Estimators/CSpline/CubicSplinePSF.cu)
+      Estimators/EstimatorImpl.cu Estimators/Gaussian/GaussianPSF.cu Estimators/CSpline/CubicSplinePSF.cu
+      Estimators/EstimationQueue.cpp Estimators/GLRT_PSF.cu)
 OBJS=()
 pids=()
 for s in "${SRCS[@]}"; do

@@ -80,6 +80,7 @@ def lib():
                 f = getattr(L, "pso_crlb" + sfx)
                 f.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, fp, fp, dp]
             L.pso_spline_compute.argtypes = [ip, fp, fp, ct.c_int]
+            L.pso_glrt_f32.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, fp, fp]
             L.pso_sizeof_model.restype = ct.c_int
             assert L.pso_sizeof_model() == ct.sizeof(PsoModel), "oracle struct layout mismatch"
             _lib = L
@@ -170,6 +171,18 @@ class Model:
         if return_fisher:
             return crlb, chisq, fisher
         return crlb, chisq
+
+
+    def glrt(self, params, samples, constants=None, mean_roi=None):
+        """GLRT diagnostics {ll_on, ll_off, mean} per spot at `params` (GLRT_PSF.cu:96-131);
+        mean_roi (npix samples) replaces each spot's own mean source, as the reference's loop does."""
+        params = _f32(params)
+        samples = _f32(samples)
+        n = params.shape[0]
+        out = np.zeros((n, 3), np.float32)
+        lib().pso_glrt_f32(ct.byref(self.s), n, _fptr(params), _fptr(samples), _fptr(_f32(constants)),
+                           _fptr(_f32(mean_roi)), _fptr(out))
+        return out
 
 
 def spline_compute(data, border=0):

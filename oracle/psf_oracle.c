@@ -150,3 +150,37 @@ int pso_spline_compute(const int* shape, const float* data, float* coefs, int bo
             }
     return 0;
 }
+
+/* Likelihood-ratio test of GLRT_PSF::Estimate (GLRT_PSF.cu:96-131), after the fit: per spot
+ * out[3] = {ll_on, ll_off, mean}, with mu = the model's expected value at params[spot]
+ * clamped at 1e-8, d = max(sample, 1e-8), mean = (sequential float sum of the mean source)
+ * / npix, ll_on = sum d log(mu) - mu, ll_off = sum d log(mean) - mean, both summed pixel by
+ * pixel in row-major order as the reference does. mean_roi == NULL: each spot's own samples
+ * are the mean source; otherwise every spot uses mean_roi (npix floats), which is what the
+ * reference computes (its mean loop reads the first ROI of the call, GLRT_PSF.cu:107-108). */
+int pso_glrt_f32(const pso_model_t* m, int n, const float* params, const float* samples, const float* constants,
+                 const float* mean_roi, float* out)
+{
+    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_num_constants(m->model);
+    float* ev = (float*)malloc(sizeof(float) * npix);
+    for (int s = 0; s < n; s++) {
+        const float* smp = samples + (size_t)s * npix;
+        pso_derivatives_f32(m, 1, params + (size_t)s * K, nc ? constants + (size_t)s * nc : NULL, NULL, ev);
+        const float* src = mean_roi ? mean_roi : smp;
+        float mean = 0.0f;
+        for (int p = 0; p < npix; p++) mean += src[p];
+        mean /= (float)npix;
+        float ll_on = 0.0f, ll_off = 0.0f;
+        for (int p = 0; p < npix; p++) {
+            const float mu = fmaxf(ev[p], 1e-8f);
+            const float d = fmaxf(smp[p], 1e-8f);
+            ll_on += d * logf(mu) - mu;
+            ll_off += d * logf(mean) - mean;
+        }
+        out[(size_t)s * 3 + 0] = ll_on;
+        out[(size_t)s * 3 + 1] = ll_off;
+        out[(size_t)s * 3 + 2] = mean;
+    }
+    free(ev);
+    return 0;
+}

@@ -68,6 +68,21 @@ def lib():
         L.Estimator_ComputeDerivatives.argtypes = [vp, ct.c_int, vp, vp, vp, vp, vp]
         L.Estimator_ComputeExpectedValue.argtypes = [vp, ct.c_int, vp, vp, vp, vp]
         L.CSpline_Compute.argtypes = [vp, vp, vp, ct.c_int]
+        if hasattr(L, "GLRT_CreatePSF"):
+            L.GLRT_CreatePSF.argtypes = [vp, vp]
+            L.GLRT_CreatePSF.restype = vp
+        if hasattr(L, "EstimQueue_Create"):
+            L.EstimQueue_Create.argtypes = [vp, ct.c_int, ct.c_int, ct.c_bool, ct.c_int, vp]
+            L.EstimQueue_Create.restype = vp
+            L.EstimQueue_Delete.argtypes = [vp]
+            L.EstimQueue_Schedule.argtypes = [vp, ct.c_int, vp, vp, vp, vp, vp]
+            L.EstimQueue_Flush.argtypes = [vp]
+            L.EstimQueue_IsIdle.argtypes = [vp]
+            L.EstimQueue_IsIdle.restype = ct.c_bool
+            L.EstimQueue_GetResultCount.argtypes = [vp]
+            L.EstimQueue_GetResultCount.restype = ct.c_int
+            L.EstimQueue_GetResults.argtypes = [vp, ct.c_int, vp, vp, vp, vp, vp, vp]
+            L.EstimQueue_GetResults.restype = ct.c_int
         _lib = L
     return _lib
 
@@ -179,6 +194,79 @@ class RefEstimator:
             self.close()
         except Exception:
             pass
+
+
+class RefGLRT:
+    """The reference's GLRT estimator (GLRT_CreatePSF, GLRT_PSF.cu:156) wrapping a CUDA RefEstimator."""
+
+    def __init__(self, model: RefEstimator):
+        self.model = model
+        self.inst = lib().GLRT_CreatePSF(model.inst, model.ctx)
+        if not self.inst:
+            raise RuntimeError("reference GLRT_CreatePSF failed")
+        self.K = model.K
+        lmp = LMParams()
+        lmp.iterations, lmp.lambda_, lmp.factor = model.iterations, 1e-18, 0
+        lib().Estimator_SetLMParams(self.inst, ct.byref(lmp))
+
+    def estimate(self, samples):
+        """-> params [n][K], diag [n][3] = (ll_on, ll_off, mean)."""
+        L = lib()
+        samples = np.ascontiguousarray(samples, dtype=np.float32)
+        n = samples.shape[0]
+        params = np.zeros((n, self.K), np.float32)
+        diag = np.zeros((n, 3), np.float32)
+        its = np.zeros(n, np.int32)
+        const = np.zeros((n, max(self.model.numconst, 1)), np.float32)
+        roipos = np.zeros((n, 2), np.int32)
+        trace = np.zeros((n, 1, self.K), np.float32)
+        L.Estimator_Estimate(self.inst, n, _p(samples), _p(const), _p(roipos), None, _p(params), _p(diag), _p(its),
+                             _p(trace), 1)
+        return params, diag
+
+
+EstimResultDType = np.dtype([("id", "<i4"), ("chisq", "<f4"), ("iterations", "<i4")])
+
+
+class RefQueue:
+    """The reference's EstimationQueue (EstimationQueue.cpp:317-420) over a CUDA RefEstimator."""
+
+    def __init__(self, model: RefEstimator, batchSize=1024, maxQueueLen=5, numStreams=-1):
+        self.model = model
+        self.inst = lib().EstimQueue_Create(model.inst, batchSize, maxQueueLen, False, numStreams, None)
+        if not self.inst:
+            raise RuntimeError("reference EstimQueue_Create failed")
+
+    def schedule(self, samples, ids):
+        samples = np.ascontiguousarray(samples, dtype=np.float32)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        n = samples.shape[0]
+        const = np.zeros((n, max(self.model.numconst, 1)), np.float32)
+        roipos = np.zeros((n, 2), np.int32)
+        lib().EstimQueue_Schedule(self.inst, n, _p(ids), _p(samples), None, _p(const), _p(roipos))
+
+    def wait(self, sleep=0.001):
+        import time
+        lib().EstimQueue_Flush(self.inst)
+        while not lib().EstimQueue_IsIdle(self.inst):
+            time.sleep(sleep)
+
+    def results(self):
+        """-> (estim [n][K], crlb [n][K], ids, chisq, iterations), whole batches in the queue's order."""
+        L = lib()
+        n = L.EstimQueue_GetResultCount(self.inst)
+        K = self.model.K
+        estim = np.zeros((n, K), np.float32)
+        crlb = np.zeros((n, K), np.float32)
+        roipos = np.zeros((n, 2), np.int32)
+        res = np.zeros(n, EstimResultDType)
+        got = L.EstimQueue_GetResults(self.inst, n, _p(estim), None, _p(crlb), _p(roipos), None, _p(res))
+        return estim[:got], crlb[:got], res["id"][:got], res["chisq"][:got], res["iterations"][:got]
+
+    def close(self):
+        if self.inst:
+            lib().EstimQueue_Delete(self.inst)
+            self.inst = None
 
 
 def spline_compute(data, border=0):

@@ -3,21 +3,24 @@
 // lines 317-420) with the same C API and results.
 //
 // Layout and flow.
-//  * Spots are packed into Batches of batchSize spots, each one pinned host allocation holding
-//    ids, samples, constants, roipos, initial values / estimates, CRLB, chi-square and
-//    iteration counts (the reference's Batch, EstimationQueue.h:54-66).
+//  * Spots are packed into Batches of batchSize spots (the reference's Batch,
+//    EstimationQueue.h:54-66). A batch's inputs (samples, constants, initial values) go into a
+//    pinned Stage taken from a bounded pool of pinned buffers that are allocated once and
+//    reused; its per-spot results live in ordinary host memory. Large Schedule calls copy
+//    into the stages with several host threads.
 //  * A full (or flushed) batch goes to the `todo` list. One worker thread takes the waiting
 //    batches in order and launches them on the first free Lane (one CUDA stream with device
-//    buffers): all waiting batches with the same initial-value mode, up to the lane's
-//    capacity, become ONE fit launch, so small batches (the reference's default is 256 spots)
-//    do not each pay a kernel launch and a CRLB launch. Per batch the lane issues one H2D copy
-//    per input array into consecutive slices of its device buffers, one
-//    PB200_EstimateDevice call over all of them (LM fit, Fisher rows, FP64 CRLB, chi-square),
-//    then one D2H copy per output array back into each batch.
-//  * Completion is signalled by a host function enqueued behind the copies
-//    (cudaLaunchHostFunc): it moves the lane's batches to `finished` and frees the lane under
-//    the queue mutex. It makes no CUDA call. Nothing polls.
-//  * GetResults copies whole finished batches out and recycles their pinned memory.
+//    buffers and pinned result buffers): all waiting batches with the same initial-value mode,
+//    up to the lane's capacity, become ONE fit launch, so small batches (the reference's
+//    default is 256 spots) do not each pay a kernel launch and a CRLB launch. The lane issues
+//    one H2D copy per batch input array into consecutive slices of its device buffers, one
+//    PB200_EstimateDeviceDiag call over all of them (LM fit, Fisher rows, FP64 CRLB,
+//    chi-square, GLRT diagnostics) and one D2H copy per result array.
+//  * Completion is a host function enqueued behind the copies (cudaLaunchHostFunc): it
+//    scatters the lane's pinned results into the batches, returns their stages to the pool,
+//    moves the batches to `finished` and frees the lane, under the queue mutex. It makes no
+//    CUDA call. Nothing polls.
+//  * GetResults copies whole finished batches out and recycles them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,54 +43,64 @@ struct QueueError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
-#define PBQ_CUDA(call)                                                                           \
-    do {                                                                                         \
-        cudaError_t err_ = (call);                                                               \
-        if (err_ != cudaSuccess)                                                                 \
+#define PBQ_CUDA(call)                                                                               \
+    do {                                                                                             \
+        cudaError_t err_ = (call);                                                                   \
+        if (err_ != cudaSuccess)                                                                     \
             throw QueueError(std::string("CUDA error: ") + cudaGetErrorString(err_) + " in " #call); \
     } while (0)
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Host side of up to `cap` spots in one pinned allocation.
-struct Batch {
-    int cap = 0, n = 0;
-    bool hasInitial = false;
+// One pinned allocation split into consecutive 256-byte aligned arrays of the given sizes.
+struct PinnedBlock {
     void* mem = nullptr;
-    int* ids = nullptr;
-    float* smp = nullptr;
-    float* consts = nullptr;
-    int* roipos = nullptr;
-    float* params = nullptr;  // initial values on the way in, estimates on the way out
-    float* crlb = nullptr;
-    float* chisq = nullptr;
-    int* iters = nullptr;
-
-    Batch(int cap_, int K, int NC, int npix, int dims) : cap(cap_) {
-        size_t off[8], o = 0;
-        const size_t sz[8] = {sizeof(int) * cap, sizeof(float) * (size_t)npix * cap, sizeof(float) * (size_t)NC * cap,
-                              sizeof(int) * (size_t)dims * cap, sizeof(float) * (size_t)K * cap,
-                              sizeof(float) * (size_t)K * cap, sizeof(float) * cap, sizeof(int) * cap};
-        for (int i = 0; i < 8; i++) {
-            off[i] = o;
-            o = align_up(o + sz[i], 256);
+    std::vector<char*> parts;
+    PinnedBlock(std::initializer_list<size_t> sizes) {
+        size_t o = 0;
+        std::vector<size_t> off;
+        for (size_t s : sizes) {
+            off.push_back(o);
+            o = align_up(o + s, 256);
         }
-        PBQ_CUDA(cudaHostAlloc(&mem, o, cudaHostAllocPortable));
-        char* b = static_cast<char*>(mem);
-        ids = reinterpret_cast<int*>(b + off[0]);
-        smp = reinterpret_cast<float*>(b + off[1]);
-        consts = reinterpret_cast<float*>(b + off[2]);
-        roipos = reinterpret_cast<int*>(b + off[3]);
-        params = reinterpret_cast<float*>(b + off[4]);
-        crlb = reinterpret_cast<float*>(b + off[5]);
-        chisq = reinterpret_cast<float*>(b + off[6]);
-        iters = reinterpret_cast<int*>(b + off[7]);
+        PBQ_CUDA(cudaHostAlloc(&mem, o ? o : 256, cudaHostAllocPortable));
+        for (size_t x : off) parts.push_back(static_cast<char*>(mem) + x);
     }
-    ~Batch() {
+    ~PinnedBlock() {
         if (mem) cudaFreeHost(mem);
     }
-    Batch(const Batch&) = delete;
-    Batch& operator=(const Batch&) = delete;
+    PinnedBlock(const PinnedBlock&) = delete;
+    PinnedBlock& operator=(const PinnedBlock&) = delete;
+    template <class T>
+    T* part(int i) const { return reinterpret_cast<T*>(parts[i]); }
+};
+
+// Pinned inputs of one batch.
+struct Stage {
+    PinnedBlock block;
+    float* smp;
+    float* consts;
+    float* initial;
+    Stage(int cap, int K, int NC, int npix)
+        : block({sizeof(float) * (size_t)npix * cap, sizeof(float) * (size_t)NC * cap, sizeof(float) * (size_t)K * cap}) {
+        smp = block.part<float>(0);
+        consts = block.part<float>(1);
+        initial = block.part<float>(2);
+    }
+};
+
+// Host side of up to `cap` spots: ids and roipos as scheduled, results after the launch.
+struct Batch {
+    int n = 0;
+    bool hasInitial = false;
+    Stage* stage = nullptr;
+    std::vector<int> ids, roipos, iters;
+    std::vector<float> params, crlb, chisq, diag, samples;
+    Batch(int cap, int K, int dims, int numDiag, int npix, bool keepSamples)
+        : ids(cap), roipos((size_t)dims * cap), iters(cap), params((size_t)K * cap), crlb((size_t)K * cap),
+          chisq(cap), diag((size_t)numDiag * cap) {
+        if (keepSamples) samples.resize((size_t)npix * cap);
+    }
 };
 
 struct DeviceArray {
@@ -103,17 +116,39 @@ struct DeviceArray {
     T* as() const { return static_cast<T*>(p); }
 };
 
+// Copies `bytes` with up to `threads` host threads (one when the copy is small).
+void copy_parallel(void* dst, const void* src, size_t bytes, int threads) {
+    const size_t kMinPerThread = 2u << 20;
+    const int t = (int)std::min<size_t>((size_t)threads, bytes / kMinPerThread);
+    if (t <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t chunk = align_up((bytes + t - 1) / t, 4096);
+    for (int i = 1; i < t; i++) {
+        const size_t a = i * chunk;
+        if (a >= bytes) break;
+        const size_t b = std::min(bytes, a + chunk);
+        pool.emplace_back(
+            [=]() { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+    }
+    std::memcpy(dst, src, std::min(bytes, chunk));
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace
 
 struct EstimQueue;
 
 namespace {
 
-// One CUDA stream with device buffers for up to `cap` spots.
+// One CUDA stream with device buffers and pinned result buffers for up to `cap` spots.
 struct Lane {
     EstimQueue* q = nullptr;
     cudaStream_t stream = nullptr;
-    DeviceArray smp, consts, initial, params, crlb, chisq, iters;
+    DeviceArray smp, consts, initial, params, crlb, chisq, iters, diag;
+    PinnedBlock* out = nullptr;  // params, crlb, chisq, iters, diag
     std::vector<Batch*> inflight;
     int spots = 0;
     bool busy = false;
@@ -121,6 +156,7 @@ struct Lane {
     Lane(const Lane&) = delete;
     ~Lane() {
         if (stream) cudaStreamDestroy(stream);
+        delete out;
     }
 };
 
@@ -129,15 +165,18 @@ struct Lane {
 struct EstimQueue {
     Estimator* est = nullptr;
     Context* ctx = nullptr;
-    int K = 0, NC = 0, npix = 0, dims = 2;
-    int batchSize = 0, limitSpots = 0, launchCap = 0;
+    int K = 0, NC = 0, npix = 0, dims = 2, numDiag = 0;
+    int batchSize = 0, limitSpots = 0, launchCap = 0, batchesPerLaunch = 1;
     bool keepSamples = false;
     int device = 0;
+    int copyThreads = 1;
 
-    std::mutex m;                 // todo, finished, recycle, counters, lanes' busy state
-    std::condition_variable cv;   // any change of the above
+    std::mutex m;                // everything below up to schedMtx
+    std::condition_variable cv;  // any change of it
     std::deque<Batch*> todo, finished, recycle;
     size_t recycleMax = 0;
+    std::vector<Stage*> stageFree;
+    int stageCount = 0, stageMax = 0;
     long long queuedSpots = 0, activeSpots = 0;
     std::deque<Lane> lanes;  // deque: lanes never move (host functions hold their address)
     bool stop = false;
@@ -158,6 +197,7 @@ struct EstimQueue {
         NC = p.numConst;
         npix = p.sampleCount;
         dims = p.sampleIndexDims;
+        numDiag = p.numDiag;
         if (K <= 0 || npix <= 0) throw QueueError("EstimQueue_Create: not a valid estimator");
         if (numStreams < 0) numStreams = 3;  // the reference's default (EstimationQueue.cpp:16-17)
         if (numStreams == 0) numStreams = 1;
@@ -165,9 +205,14 @@ struct EstimQueue {
         // Launch capacity: whole batches, at most 64 MiB of samples and 65536 spots per launch.
         const long long bySmp = (64ll << 20) / ((long long)npix * 4 * batchSize);
         const long long byCount = 65536ll / batchSize;
-        const long long nb = std::max(1ll, std::min(bySmp, byCount));
-        launchCap = (int)(nb * batchSize);
-        recycleMax = (size_t)(numStreams * nb + limitSpots / batchSize + 2);
+        batchesPerLaunch = (int)std::max(1ll, std::min(bySmp, byCount));
+        launchCap = batchesPerLaunch * batchSize;
+        // Pinned stages: enough for every lane's launch plus a full launch waiting, and for
+        // the spots the queue limit admits.
+        stageMax = std::max((numStreams + 1) * batchesPerLaunch + 2, limitSpots / batchSize + 2);
+        recycleMax = (size_t)stageMax;
+        const unsigned hw = std::thread::hardware_concurrency();
+        copyThreads = (int)std::max(1u, std::min(8u, hw / 2));
         PBQ_CUDA(cudaGetDevice(&device));
         for (int i = 0; i < numStreams; i++) {
             Lane& L = lanes.emplace_back();
@@ -181,6 +226,9 @@ struct EstimQueue {
             L.crlb.alloc(sizeof(float) * K * cap);
             L.chisq.alloc(sizeof(float) * cap);
             L.iters.alloc(sizeof(int) * cap);
+            if (numDiag) L.diag.alloc(sizeof(float) * numDiag * cap);
+            L.out = new PinnedBlock({sizeof(float) * K * cap, sizeof(float) * K * cap, sizeof(float) * cap,
+                                     sizeof(int) * cap, sizeof(float) * numDiag * cap});
         }
         worker = std::thread([this]() { run(); });
     }
@@ -196,27 +244,58 @@ struct EstimQueue {
         // Work already issued completes (its host functions need `m`, which is free now).
         for (auto& L : lanes)
             if (L.stream) cudaStreamSynchronize(L.stream);
-        for (auto* b : todo) delete b;
-        for (auto* b : finished) delete b;
-        for (auto* b : recycle) delete b;
-        delete next;
+        auto drop = [&](Batch* b) {
+            if (b && b->stage) stageFree.push_back(b->stage);
+            delete b;
+        };
+        for (auto* b : todo) drop(b);
+        for (auto* b : finished) drop(b);
+        for (auto* b : recycle) drop(b);
+        drop(next);
+        for (auto* s : stageFree) delete s;
     }
 
-    // ---------------------------------------------------------------- worker thread
+    // ---------------------------------------------------------------- completion
     static void CUDART_CB lane_done(void* arg) {
         Lane* L = static_cast<Lane*>(arg);
         EstimQueue* q = L->q;
+        const int K = q->K, ND = q->numDiag;
+        const float* hp = L->out->part<float>(0);
+        const float* hc = L->out->part<float>(1);
+        const float* hx = L->out->part<float>(2);
+        const int* hi = L->out->part<int>(3);
+        const float* hd = L->out->part<float>(4);
+        int off = 0;
+        for (auto* b : L->inflight) {
+            const int n = b->n;
+            std::memcpy(b->params.data(), hp + (size_t)off * K, sizeof(float) * K * n);
+            std::memcpy(b->crlb.data(), hc + (size_t)off * K, sizeof(float) * K * n);
+            std::memcpy(b->chisq.data(), hx + off, sizeof(float) * n);
+            std::memcpy(b->iters.data(), hi + off, sizeof(int) * n);
+            if (ND) std::memcpy(b->diag.data(), hd + (size_t)off * ND, sizeof(float) * ND * n);
+            off += n;
+        }
+        q->retire(L);
+    }
+
+    // Moves the lane's batches to `finished`, returns their stages and frees the lane.
+    void retire(Lane* L) {
         {
-            std::lock_guard<std::mutex> g(q->m);
-            for (auto* b : L->inflight) q->finished.push_back(b);
-            q->activeSpots -= L->spots;
+            std::lock_guard<std::mutex> g(m);
+            for (auto* b : L->inflight) {
+                stageFree.push_back(b->stage);
+                b->stage = nullptr;
+                finished.push_back(b);
+            }
+            activeSpots -= L->spots;
             L->inflight.clear();
             L->spots = 0;
             L->busy = false;
         }
-        q->cv.notify_all();
+        cv.notify_all();
     }
 
+    // ---------------------------------------------------------------- worker thread
     int free_lane() const {
         for (size_t i = 0; i < lanes.size(); i++)
             if (!lanes[i].busy) return (int)i;
@@ -253,17 +332,19 @@ struct EstimQueue {
                 // as failed (NaN estimates, 0 iterations) and hand the batches back.
                 cudaStreamSynchronize(L.stream);
                 cudaGetLastError();
+                const float nan = std::numeric_limits<float>::quiet_NaN();
                 for (auto* b : L.inflight) {
-                    std::fill(b->params, b->params + (size_t)K * b->n, std::numeric_limits<float>::quiet_NaN());
-                    std::fill(b->crlb, b->crlb + (size_t)K * b->n, std::numeric_limits<float>::quiet_NaN());
-                    std::fill(b->chisq, b->chisq + b->n, std::numeric_limits<float>::quiet_NaN());
-                    std::fill(b->iters, b->iters + b->n, 0);
+                    std::fill(b->params.begin(), b->params.end(), nan);
+                    std::fill(b->crlb.begin(), b->crlb.end(), nan);
+                    std::fill(b->chisq.begin(), b->chisq.end(), nan);
+                    std::fill(b->diag.begin(), b->diag.end(), nan);
+                    std::fill(b->iters.begin(), b->iters.end(), 0);
                 }
                 {
                     std::lock_guard<std::mutex> g(m);
                     if (failure.empty()) failure = "EstimQueue: " + err;
                 }
-                lane_done(&L);
+                retire(&L);
             }
             lk.lock();
         }
@@ -273,34 +354,32 @@ struct EstimQueue {
         cudaStream_t s = L.stream;
         int off = 0;
         for (auto* b : L.inflight) {
-            PBQ_CUDA(cudaMemcpyAsync(L.smp.as<float>() + (size_t)off * npix, b->smp, sizeof(float) * npix * b->n,
-                                     cudaMemcpyHostToDevice, s));
+            PBQ_CUDA(cudaMemcpyAsync(L.smp.as<float>() + (size_t)off * npix, b->stage->smp,
+                                     sizeof(float) * npix * b->n, cudaMemcpyHostToDevice, s));
             if (NC)
-                PBQ_CUDA(cudaMemcpyAsync(L.consts.as<float>() + (size_t)off * NC, b->consts,
+                PBQ_CUDA(cudaMemcpyAsync(L.consts.as<float>() + (size_t)off * NC, b->stage->consts,
                                          sizeof(float) * NC * b->n, cudaMemcpyHostToDevice, s));
             if (init)
-                PBQ_CUDA(cudaMemcpyAsync(L.initial.as<float>() + (size_t)off * K, b->params, sizeof(float) * K * b->n,
-                                         cudaMemcpyHostToDevice, s));
+                PBQ_CUDA(cudaMemcpyAsync(L.initial.as<float>() + (size_t)off * K, b->stage->initial,
+                                         sizeof(float) * K * b->n, cudaMemcpyHostToDevice, s));
             off += b->n;
         }
         PB200_ClearError();
-        PB200_EstimateDevice(est, total, L.smp.as<float>(), NC ? L.consts.as<float>() : nullptr,
-                             init ? L.initial.as<float>() : nullptr, L.params.as<float>(), L.iters.as<int>(), nullptr,
-                             0, L.crlb.as<float>(), L.chisq.as<float>(), s);
+        PB200_EstimateDeviceDiag(est, total, L.smp.as<float>(), NC ? L.consts.as<float>() : nullptr,
+                                 init ? L.initial.as<float>() : nullptr, L.params.as<float>(),
+                                 numDiag ? L.diag.as<float>() : nullptr, L.iters.as<int>(), L.crlb.as<float>(),
+                                 L.chisq.as<float>(), s);
         const char* msg = PB200_GetLastError();
         if (msg && msg[0]) throw QueueError(msg);
-        off = 0;
-        for (auto* b : L.inflight) {
-            PBQ_CUDA(cudaMemcpyAsync(b->params, L.params.as<float>() + (size_t)off * K, sizeof(float) * K * b->n,
+        PBQ_CUDA(cudaMemcpyAsync(L.out->part<float>(0), L.params.p, sizeof(float) * K * total,
+                                 cudaMemcpyDeviceToHost, s));
+        PBQ_CUDA(cudaMemcpyAsync(L.out->part<float>(1), L.crlb.p, sizeof(float) * K * total,
+                                 cudaMemcpyDeviceToHost, s));
+        PBQ_CUDA(cudaMemcpyAsync(L.out->part<float>(2), L.chisq.p, sizeof(float) * total, cudaMemcpyDeviceToHost, s));
+        PBQ_CUDA(cudaMemcpyAsync(L.out->part<int>(3), L.iters.p, sizeof(int) * total, cudaMemcpyDeviceToHost, s));
+        if (numDiag)
+            PBQ_CUDA(cudaMemcpyAsync(L.out->part<float>(4), L.diag.p, sizeof(float) * numDiag * total,
                                      cudaMemcpyDeviceToHost, s));
-            PBQ_CUDA(cudaMemcpyAsync(b->crlb, L.crlb.as<float>() + (size_t)off * K, sizeof(float) * K * b->n,
-                                     cudaMemcpyDeviceToHost, s));
-            PBQ_CUDA(cudaMemcpyAsync(b->chisq, L.chisq.as<float>() + off, sizeof(float) * b->n,
-                                     cudaMemcpyDeviceToHost, s));
-            PBQ_CUDA(cudaMemcpyAsync(b->iters, L.iters.as<int>() + off, sizeof(int) * b->n, cudaMemcpyDeviceToHost,
-                                     s));
-            off += b->n;
-        }
         PBQ_CUDA(cudaLaunchHostFunc(s, &EstimQueue::lane_done, &L));
     }
 
@@ -314,18 +393,42 @@ struct EstimQueue {
         if (!f.empty()) pb200::set_last_error(f);
     }
 
+    // An empty batch with a stage; waits for a stage when the pool is exhausted (the launches
+    // in flight return theirs).
     Batch* take_batch() {
+        Batch* b = nullptr;
+        Stage* st = nullptr;
+        bool allocate = false;
         {
-            std::lock_guard<std::mutex> g(m);
+            std::unique_lock<std::mutex> lk(m);
+            cv.wait(lk, [&]() { return stop || !stageFree.empty() || stageCount < stageMax; });
+            if (stop) throw QueueError("EstimQueue: queue is being deleted");
+            if (!stageFree.empty()) {
+                st = stageFree.back();
+                stageFree.pop_back();
+            } else {
+                stageCount++;
+                allocate = true;
+            }
             if (!recycle.empty()) {
-                Batch* b = recycle.back();
+                b = recycle.back();
                 recycle.pop_back();
-                b->n = 0;
-                b->hasInitial = false;
-                return b;
             }
         }
-        return new Batch(batchSize, K, NC, npix, dims);
+        try {
+            if (allocate) st = new Stage(batchSize, K, NC, npix);
+            if (!b) b = new Batch(batchSize, K, dims, numDiag, npix, keepSamples);
+        } catch (...) {
+            std::lock_guard<std::mutex> g(m);
+            if (allocate) stageCount--;
+            else stageFree.push_back(st);
+            if (b) recycle.push_back(b);
+            throw;
+        }
+        b->n = 0;
+        b->hasInitial = false;
+        b->stage = st;
+        return b;
     }
 
     // Moves the batch being filled to `todo` (caller holds schedMtx).
@@ -360,18 +463,23 @@ struct EstimQueue {
             if (!next) next = take_batch();
             Batch* b = next;
             b->hasInitial = init;
-            const int m_ = std::min(b->cap - b->n, count - i);
+            const int m_ = std::min(batchSize - b->n, count - i);
             const int o = b->n;
-            if (ids) std::memcpy(b->ids + o, ids + i, sizeof(int) * m_);
-            else std::fill(b->ids + o, b->ids + o + m_, 0);
-            std::memcpy(b->smp + (size_t)o * npix, smp + (size_t)i * npix, sizeof(float) * npix * m_);
-            if (NC) std::memcpy(b->consts + (size_t)o * NC, consts + (size_t)i * NC, sizeof(float) * NC * m_);
-            if (roipos) std::memcpy(b->roipos + (size_t)o * dims, roipos + (size_t)i * dims, sizeof(int) * dims * m_);
-            else std::fill(b->roipos + (size_t)o * dims, b->roipos + (size_t)(o + m_) * dims, 0);
-            if (init) std::memcpy(b->params + (size_t)o * K, initial + (size_t)i * K, sizeof(float) * K * m_);
+            if (ids) std::memcpy(b->ids.data() + o, ids + i, sizeof(int) * m_);
+            else std::fill(b->ids.begin() + o, b->ids.begin() + o + m_, 0);
+            copy_parallel(b->stage->smp + (size_t)o * npix, smp + (size_t)i * npix, sizeof(float) * npix * m_,
+                          copyThreads);
+            if (keepSamples)
+                std::memcpy(b->samples.data() + (size_t)o * npix, smp + (size_t)i * npix, sizeof(float) * npix * m_);
+            if (NC) std::memcpy(b->stage->consts + (size_t)o * NC, consts + (size_t)i * NC, sizeof(float) * NC * m_);
+            if (roipos)
+                std::memcpy(b->roipos.data() + (size_t)o * dims, roipos + (size_t)i * dims, sizeof(int) * dims * m_);
+            else
+                std::fill(b->roipos.begin() + (size_t)o * dims, b->roipos.begin() + (size_t)(o + m_) * dims, 0);
+            if (init) std::memcpy(b->stage->initial + (size_t)o * K, initial + (size_t)i * K, sizeof(float) * K * m_);
             b->n += m_;
             i += m_;
-            if (b->n == b->cap) flush_next();
+            if (b->n == batchSize) flush_next();
         }
     }
 
@@ -403,7 +511,6 @@ struct EstimQueue {
 
     int results(int maxresults, float* estim, float* diag, float* crlb, int* roipos, float* samples,
                 EstimatorResult* res) {
-        (void)diag;  // numDiag is 0
         report_failure();
         int copied = 0;
         for (;;) {
@@ -417,10 +524,13 @@ struct EstimQueue {
             const int n = b->n;
             if (res)
                 for (int i = 0; i < n; i++) res[copied + i] = EstimatorResult{b->ids[i], b->chisq[i], b->iters[i]};
-            if (estim) std::memcpy(estim + (size_t)copied * K, b->params, sizeof(float) * K * n);
-            if (crlb) std::memcpy(crlb + (size_t)copied * K, b->crlb, sizeof(float) * K * n);
-            if (roipos) std::memcpy(roipos + (size_t)copied * dims, b->roipos, sizeof(int) * dims * n);
-            if (samples && keepSamples) std::memcpy(samples + (size_t)copied * npix, b->smp, sizeof(float) * npix * n);
+            if (estim) std::memcpy(estim + (size_t)copied * K, b->params.data(), sizeof(float) * K * n);
+            if (crlb) std::memcpy(crlb + (size_t)copied * K, b->crlb.data(), sizeof(float) * K * n);
+            if (diag && numDiag)
+                std::memcpy(diag + (size_t)copied * numDiag, b->diag.data(), sizeof(float) * numDiag * n);
+            if (roipos) std::memcpy(roipos + (size_t)copied * dims, b->roipos.data(), sizeof(int) * dims * n);
+            if (samples && keepSamples)
+                std::memcpy(samples + (size_t)copied * npix, b->samples.data(), sizeof(float) * npix * n);
             copied += n;
             b->n = 0;
             bool keep;

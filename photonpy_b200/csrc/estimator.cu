@@ -196,7 +196,7 @@ void set_last_error(const std::string& msg) {
 
 struct Slot {
     cudaStream_t stream = nullptr;
-    DevBuf smp, consts, initial, params, iters, trace, crlb, chisq, fisher;
+    DevBuf smp, consts, initial, params, iters, trace, crlb, chisq, fisher, glrt;
 };
 
 struct Estimator {
@@ -210,6 +210,10 @@ struct Estimator {
     int lanes = 0, threads = 256;
     int variant = 0;  // 0: column-blocked Gaussian kernel, 1: generic table kernel
     int device = 0;
+    // Likelihood-ratio test estimator (GLRT_CreatePSF): diagnostics = {ll_on, ll_off, mean} per spot.
+    bool glrt = false;
+    bool glrtRefMean = false;  // every spot's mean from the call's first ROI, as the reference
+    DevBuf glrtRoi0;
     std::mutex mtx;
     Slot slots[2];
 
@@ -304,11 +308,16 @@ struct Chunking {
 // before D2H(c-1), so copies of one chunk overlap the fit of the other.
 void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, const float* h_initial,
               float* h_params, int* h_iters, float* h_trace, int traceLen, float* h_crlb, float* h_chisq,
-              int flags) {
+              int flags, float* h_glrt = nullptr) {
     std::lock_guard<std::mutex> g(e->mtx);
     PB_CUDA(cudaSetDevice(e->device));
     const int K = e->K, NC = e->numconst, npix = e->npix();
     const bool fisherOnly = (flags & FIT_CRLB_ONLY) != 0;
+    const bool wantGlrt = h_glrt && e->glrt && !fisherOnly;
+    if (wantGlrt && e->glrtRefMean) {
+        e->glrtRoi0.ensure(sizeof(float) * npix);
+        PB_CUDA(cudaMemcpy(e->glrtRoi0.p, h_smp, sizeof(float) * npix, cudaMemcpyHostToDevice));
+    }
     int chunk = n;
     if (n > 65536) chunk = std::max(32768, (n + 7) / 8);
     const int nchunks = (n + chunk - 1) / chunk;
@@ -334,6 +343,9 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
                                     cudaMemcpyDeviceToHost, s.stream));
         if (h_chisq)
             PB_CUDA(cudaMemcpyAsync(h_chisq + p.start, s.chisq.as<float>(), sizeof(float) * p.count,
+                                    cudaMemcpyDeviceToHost, s.stream));
+        if (wantGlrt)
+            PB_CUDA(cudaMemcpyAsync(h_glrt + (size_t)p.start * 3, s.glrt.as<float>(), sizeof(float) * 3 * p.count,
                                     cudaMemcpyDeviceToHost, s.stream));
     };
     for (int c = 0; c < nchunks; c++) {
@@ -381,6 +393,11 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         a.lambda = e->lm.lambda;
         a.flags = flags;
         a.fisher = h_crlb ? s.fisher.as<float>() : nullptr;
+        if (wantGlrt) {
+            s.glrt.ensure(sizeof(float) * 3 * count);
+            a.glrt = s.glrt.as<float>();
+            a.glrtMeanRoi = e->glrtRefMean ? e->glrtRoi0.as<float>() : nullptr;
+        }
         fl(e->desc, a, e->threads, s.stream);
         if (h_crlb) launch_crlb(K, a.fisher, a.crlb, a.chisq, count, s.stream);
         pend.push_back({c & 1, start, count});
@@ -823,6 +840,51 @@ void CSpline_Evaluate(const int* shape, const float* splineCoefs, const float* s
         });
 }
 
+// GLRT_PSF.cu:156-170. The reference wraps the model estimator; here the GLRT estimator is an
+// independent copy of it (same model, calibration, LM and kernel settings) that also writes
+// the three diagnostics per spot, so deleting the model estimator does not affect it.
+Estimator* GLRT_CreatePSF(Estimator* model, Context* ctx) {
+    return guarded([&]() -> Estimator* {
+        if (!model) throw Error("GLRT_CreatePSF: model estimator is null");
+        PB_CUDA(cudaSetDevice(model->device));
+        auto* e = new Estimator();
+        try {
+            e->desc = model->desc;
+            e->K = model->K;
+            e->numconst = model->numconst;
+            e->format = model->format;
+            e->limits = model->limits;
+            e->lm = model->lm;
+            e->lanes = model->lanes;
+            e->threads = model->threads;
+            e->variant = model->variant;
+            e->glrt = true;
+            if (model->desc.model == MODEL_CSPLINE) {
+                const size_t ncoef = (size_t)model->desc.spline_shape[0] * model->desc.spline_shape[1] *
+                                     model->desc.spline_shape[2] * 64;
+                e->coefs.ensure(sizeof(float) * ncoef);
+                PB_CUDA(cudaMemcpy(e->coefs.p, model->coefs.p, sizeof(float) * ncoef, cudaMemcpyDeviceToDevice));
+                e->desc.coefs = e->coefs.as<float>();
+            }
+        } catch (...) {
+            delete e;
+            throw;
+        }
+        attach(e, ctx);
+        return e;
+    }, (Estimator*)nullptr);
+}
+
+int PB200_SetGLRTReferenceMean(Estimator* e, int on) {
+    return guarded([&]() -> int {
+        check_estimator(e);
+        if (!e->glrt) throw Error("PB200_SetGLRTReferenceMean: not a GLRT estimator");
+        std::lock_guard<std::mutex> g(e->mtx);
+        e->glrtRefMean = on != 0;
+        return 0;
+    }, -1);
+}
+
 void Estimator_Delete(Estimator* e) {
     if (!e) return;
     detach(e);
@@ -835,7 +897,7 @@ void Estimator_GetProperties(Estimator* e, EstimatorProperties* p) {
     if (!e || !p) return;
     p->numParams = e->K;
     p->sampleCount = e->npix();
-    p->numDiag = 0;
+    p->numDiag = e->glrt ? 3 : 0;
     p->numConst = e->numconst;
     p->sampleIndexDims = 2;
 }
@@ -879,11 +941,10 @@ void Estimator_ComputeDerivatives(Estimator* e, int numspots, const float* param
 void Estimator_Estimate(Estimator* e, int numspots, const float* sample, const float* constants, const int*,
                         const float* initial, float* params, float* diagnostics, int* iterations, float* trace,
                         int traceBufLen) {
-    (void)diagnostics;
     if (numspots == 0) return;
     guarded_void([&]() {check_estimator(e); if (numspots < 0 || !sample || !params) throw Error("Estimate: bad arguments");
            host_fit(e, numspots, sample, constants, initial, params, iterations, trace, traceBufLen, nullptr, nullptr,
-                    0);
+                    0, e->glrt ? diagnostics : nullptr);
            });
 }
 
@@ -915,6 +976,23 @@ void PB200_EstimateDevice(Estimator* e, int numspots, const float* d_sample, con
         a.iterations = d_iterations; a.trace = traceBufLen > 0 ? d_trace : nullptr;
         a.traceLen = traceBufLen > 0 && d_trace ? traceBufLen : 0; a.crlb = d_crlb; a.chisq = d_chisq;
         a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda; a.flags = 0;
+        run_fit_device(e, a, (cudaStream_t)stream);});
+}
+
+void PB200_EstimateDeviceDiag(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                              const float* d_initial, float* d_params, float* d_diag, int* d_iterations,
+                              float* d_crlb, float* d_chisq, void* stream) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e); if (numspots < 0 || !d_sample || !d_params) throw Error("EstimateDeviceDiag: bad arguments");
+        if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+        FitArgs a{}; a.smp = d_sample; a.consts = d_constants; a.initial = d_initial; a.params = d_params;
+        a.iterations = d_iterations; a.crlb = d_crlb; a.chisq = d_chisq;
+        a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda; a.flags = 0;
+        if (e->glrt && d_diag) {
+            a.glrt = d_diag;
+            a.glrtMeanRoi = e->glrtRefMean ? d_sample : nullptr;
+        }
         run_fit_device(e, a, (cudaStream_t)stream);});
 }
 

@@ -32,6 +32,9 @@ struct FitArgs {
     int* diag;             // [n] or null: 1 when an FP64 re-solve happened for the spot
     float* fisher;         // [n][K(K+1)/2 + 1] scratch: packed FP32 Fisher matrix + chi-square, inverted
                            // afterwards by crlb_kernel; null = invert in the fit kernel (lane 0)
+    float* glrt;           // [n][3] or null: {ll_on, ll_off, mean} of the likelihood-ratio test
+    const float* glrtMeanRoi;  // null: each spot's own mean; else every spot's mean comes from these npix
+                               // samples (the reference's behaviour, see glrt_store)
     int n;
     int maxIter;
     float lambda;
@@ -248,6 +251,30 @@ __device__ __forceinline__ bool lm_rescue(const float (&acc)[NACC], const float 
     for (int q = 0; q < K; q++) step[q] = xs[q];
     __syncwarp(mask);
     return ok;
+}
+
+// Likelihood-ratio test against a background-only model (GLRT_PSF.cu:104-131), evaluated
+// after the Fisher pass at the final parameters. With d = max(x, 1e-8), mu8 = max(mu, 1e-8):
+//   ll_on  = sum_p d log(mu8) - mu8     (summed over the pixels by the caller: llOn)
+//   mean   = sum_p x / npix              (sumRaw; exact for integer counts in any order)
+//   ll_off = sum_p d log(mean) - mean = log(mean) sum_p d - npix mean   (sumD = sum_p d)
+// The reference computes `mean` from the first ROI of each call for every spot (its loop
+// variable shadows the spot index, GLRT_PSF.cu:107-109); a non-null a.glrtMeanRoi reproduces
+// that, summing those samples sequentially as the reference does. By default each spot uses
+// its own mean.
+__device__ __forceinline__ void glrt_store(float llOn, float sumD, float sumRaw, const FitArgs& a, int roi, int npix,
+                                           int lane) {
+    if (lane != 0) return;
+    float mean = sumRaw;
+    if (a.glrtMeanRoi) {
+        mean = 0.0f;
+        for (int i = 0; i < npix; i++) mean += a.glrtMeanRoi[i];
+    }
+    mean = __fdiv_rn(mean, (float)npix);
+    float* o = a.glrt + (size_t)roi * 3;
+    o[0] = llOn;
+    o[1] = sumD * logf(mean) - (float)npix * mean;
+    o[2] = mean;
 }
 
 // Fisher pass epilogue, deferred form: the group's lanes store the packed FP32 Fisher matrix

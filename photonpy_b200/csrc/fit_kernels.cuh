@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
     constexpr int NA = K * (K + 1) / 2;
     constexpr int NACC = NA + K + 1;
     constexpr int NC = model_num_consts(M::kId);
-    enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3 };
+    enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3, MODE_IDLE = 4 };
     extern __shared__ __align__(16) float sm[];
 
     const int lane = threadIdx.x & (G - 1);
@@ -64,6 +64,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
     const int x0 = lane % R, y0 = lane / R;
     const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
     const bool haveSmp = a.smp != nullptr;
+    const bool glrt = a.glrt != nullptr;  // needs samples (checked by the host)
     const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
 
     int roi = blockIdx.x * gpb + gib;
@@ -74,9 +75,9 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
     bool rescuedAny = false;
 
     while (true) {
+        if (mode == MODE_LOAD && roi >= a.n) mode = MODE_IDLE;
         if (mode == MODE_LOAD) {
             // ---- load the next ROI into shared memory and set the start parameters ----
-            if (roi >= a.n) break;
             __syncwarp(mask);  // previous ROI's readers are done with spix/tab
             const float* src = haveSmp ? a.smp + (size_t)roi * npix : nullptr;
             if (haveSmp) {
@@ -115,11 +116,15 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
             it = 0;
             rescuedAny = false;
             if (fisherOnly) mode = MODE_FISHER;
-            else if (a.maxIter <= 0) mode = a.crlb ? MODE_FISHER : MODE_SKIP;  // start value, iterations = 1
+            else if (a.maxIter <= 0) mode = (a.crlb || a.glrt) ? MODE_FISHER : MODE_SKIP;  // start value, iterations = 1
             else mode = MODE_LM;
         }
+        // The groups of a warp leave together (an idle group waits for its warp-mates), so every
+        // lane passes this point once per trip and the warp reconverges before the pixel pass.
+        if (__all_sync(0xffffffffu, mode == MODE_IDLE)) break;
+        __syncwarp();
 
-        if (mode != MODE_SKIP) {
+        if (mode == MODE_LM || mode == MODE_FISHER) {
             if (mode == MODE_LM && a.trace && lane == 0 && it < a.traceLen) {
 #pragma unroll
                 for (int k = 0; k < K; k++) a.trace[((size_t)roi * a.traceLen + it) * K + k] = th[k];
@@ -206,17 +211,38 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                     }
                 }
                 if (!done) continue;
-                if (a.crlb) {
+                if (a.crlb || a.glrt) {
                     mode = MODE_FISHER;
                     continue;
                 }
             } else {
                 // ---- Fisher pass: deferred FP64 inverse (crlb_kernel), or on lane 0 ----
+                if (glrt) {
+                    // likelihood-ratio terms at the final parameters (GLRT_PSF.cu:112-124), in a
+                    // pass of their own so that the LM pixel loop stays free of them
+                    float on = 0.0f, sd = 0.0f, sr = 0.0f;
+                    int gx = x0, gy = y0;
+                    for (int p = lane; p < npix; p += G) {
+                        float mu, J[K];
+                        m.pixel(d, tab, gx, gy, mu, J);
+                        const float s = spix[p];
+                        const float mu8 = fmaxf(mu, 1e-8f), d8 = fmaxf(s, 1e-8f);
+                        on += d8 * logf(mu8) - mu8;
+                        sd += d8;
+                        sr += s;
+                        gx += dx;
+                        gy += dy;
+                        if (gx >= R) { gx -= R; gy++; }
+                    }
+                    glrt_store(group_sum<G>(on, mask), group_sum<G>(sd, mask), group_sum<G>(sr, mask), a, roi, npix,
+                               lane);
+                }
                 if (a.fisher) fisher_store<K, NACC, G>(acc, a.fisher + (size_t)roi * (NA + 1), lane);
-                else fisher_finish<K, NACC>(acc, tab, lane, mask, a.crlb + (size_t)roi * K,
-                                            a.chisq ? a.chisq + roi : nullptr);
+                else if (a.crlb) fisher_finish<K, NACC>(acc, tab, lane, mask, a.crlb + (size_t)roi * K,
+                                                        a.chisq ? a.chisq + roi : nullptr);
             }
         }
+        if (mode == MODE_IDLE) continue;
         // ---- ROI finished: write results, move to the next ROI ----
         if (lane == 0 && !fisherOnly) {
 #pragma unroll

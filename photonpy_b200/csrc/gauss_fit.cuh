@@ -24,9 +24,9 @@ namespace pb200 {
 // Shared-memory floats of one group: pixels, then max(y-terms, FP64 re-solve scratch,
 // Fisher scratch when the pixel area cannot hold it). Stride = 16 mod 32 so that the
 // 16-byte row loads of two neighbouring groups fall in complementary bank quads.
-template <int K, int NE = 3>
+template <int K>
 __host__ __device__ constexpr int gauss_group_floats(int R) {
-    return round_up(round_up(R * R, 4) + cmax(cmax(cmax(4 * R, 2 * (R + 1) * NE), rescue_floats(K)),
+    return round_up(round_up(R * R, 4) + cmax(cmax(4 * R, rescue_floats(K)),
                                               (round_up(R * R, 4) >= 4 * K * K) ? 0 : 4 * K * K),
                     32) + 16;
 }
@@ -40,7 +40,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
     constexpr int NA = K * (K + 1) / 2;
     constexpr int NACC = NA + K + 1;
     constexpr int NC = model_num_consts(M::kId);
-    enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3 };
+    enum { MODE_LM = 0, MODE_FISHER = 1, MODE_SKIP = 2, MODE_LOAD = 3, MODE_IDLE = 4 };
     const int R = d.roisize;
     const int npix = R * R;
     const int npix4 = round_up(npix, 4);
@@ -50,6 +50,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
     const int c0 = lane * CPL;
     const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
     const bool haveSmp = a.smp != nullptr;
+    const bool glrt = a.glrt != nullptr;  // needs samples (checked by the host)
     const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
     const bool rowVec4 = (CPL == 4) && ((R & 3) == 0) && (c0 + 4 <= R);
 
@@ -60,8 +61,8 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
     bool rescuedAny = false;
 
     while (true) {
+        if (mode == MODE_LOAD && roi >= roiEnd) mode = MODE_IDLE;
         if (mode == MODE_LOAD) {
-            if (roi >= roiEnd) break;
             __syncwarp(mask);  // the previous ROI's readers are done with spix/aux
             if (haveSmp) {
                 const float* src = a.smp + (size_t)roi * npix;
@@ -102,33 +103,27 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
             it = 0;
             rescuedAny = false;
             if (fisherOnly) mode = MODE_FISHER;
-            else if (a.maxIter <= 0) mode = a.crlb ? MODE_FISHER : MODE_SKIP;
+            else if (a.maxIter <= 0) mode = (a.crlb || a.glrt) ? MODE_FISHER : MODE_SKIP;
             else mode = MODE_LM;
         }
+        // The groups of a warp leave together: a group without ROIs idles until its warp-mates
+        // are done. So every lane of the warp passes this point once per trip, and the warp is
+        // reconverged here before the pixel pass (groups that loaded a ROI this trip would
+        // otherwise run the pass apart from the others).
+        if (__all_sync(0xffffffffu, mode == MODE_IDLE)) break;
+        __syncwarp();
 
-        if (mode != MODE_SKIP) {
+        if (mode == MODE_LM || mode == MODE_FISHER) {
             if (mode == MODE_LM && a.trace && lane == 0 && it < a.traceLen) {
 #pragma unroll
                 for (int k = 0; k < K; k++) a.trace[((size_t)roi * a.traceLen + it) * K + k] = th[k];
             }
             M m;
             m.begin(d, th, cs);
-            // erf/exp at the 2(R+1) pixel edges, lane-strided so that neighbouring lanes (and the
-            // same lane of every group in the warp) evaluate neighbouring edges: erff's branches
-            // stay coherent across the warp
-            constexpr int NE = M::kEdgeFloats;
-            float* ex = aux;
-            float* ey = aux + (R + 1) * NE;
-            __syncwarp(mask);  // previous readers of ytab / scratch are done
-            for (int e = lane; e < 2 * (R + 1); e += G) {
-                if (e <= R) m.edge(e, m.tx, m.cx1, m.sigx, ex + e * NE);
-                else m.edge(e - (R + 1), m.ty, m.cy1, m.sigy, ey + (e - (R + 1)) * NE);
-            }
-            __syncwarp(mask);
             float4 X[CPL], Yown[CPL];
-            m.template terms_from_edges<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, ex, R, X);
-            m.template terms_from_edges<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, ey, R, Yown);
-            __syncwarp(mask);  // every lane has read its edges before ytab overwrites them
+            m.template term_block<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, X);
+            m.template term_block<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, Yown);
+            __syncwarp(mask);  // previous readers of ytab / scratch are done
 #pragma unroll
             for (int q = 0; q < CPL; q++)
                 if (c0 + q < R) ytab[c0 + q] = Yown[q];
@@ -226,17 +221,40 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                     }
                 }
                 if (!done) continue;
-                if (a.crlb) {
+                if (a.crlb || a.glrt) {
                     mode = MODE_FISHER;
                     continue;
                 }
-            } else if (a.fisher) {
-                fisher_store<K, NACC, G>(acc, a.fisher + (size_t)roi * (NA + 1), lane);
             } else {
-                fisher_finish<K, NACC>(acc, fisherScratch, lane, mask, a.crlb + (size_t)roi * K,
-                                       a.chisq ? a.chisq + roi : nullptr);
+                if (glrt) {
+                    // likelihood-ratio terms at the final parameters (GLRT_PSF.cu:112-124), in a
+                    // pass of their own so that the LM pixel loop stays free of them
+                    float on = 0.0f, sd = 0.0f, sr = 0.0f;
+                    if (c0 < R) {
+                        for (int y = 0; y < R; y++) {
+                            const float4 Y = ytab[y];
+#pragma unroll
+                            for (int q = 0; q < CPL; q++) {
+                                if (c0 + q >= R) continue;
+                                float mu, J[K];
+                                m.pixel_xy(X[q], Y, mu, J);
+                                const float s = spix[y * R + c0 + q];
+                                const float mu8 = fmaxf(mu, 1e-8f), d8 = fmaxf(s, 1e-8f);
+                                on += d8 * logf(mu8) - mu8;
+                                sd += d8;
+                                sr += s;
+                            }
+                        }
+                    }
+                    glrt_store(group_sum<G>(on, mask), group_sum<G>(sd, mask), group_sum<G>(sr, mask), a, roi, npix,
+                               lane);
+                }
+                if (a.fisher) fisher_store<K, NACC, G>(acc, a.fisher + (size_t)roi * (NA + 1), lane);
+                else if (a.crlb) fisher_finish<K, NACC>(acc, fisherScratch, lane, mask, a.crlb + (size_t)roi * K,
+                                                        a.chisq ? a.chisq + roi : nullptr);
             }
         }
+        if (mode == MODE_IDLE) continue;
         if (lane == 0 && !fisherOnly) {
 #pragma unroll
             for (int k = 0; k < K; k++) a.params[(size_t)roi * K + k] = th[k];

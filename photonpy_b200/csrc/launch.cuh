@@ -74,7 +74,7 @@ void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t
 template <class M, int G, int CPL>
 void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
     if (a.n <= 0) return;
-    launch_groups(gauss_fit_kernel<M, G, CPL>, G, threads, gauss_group_floats<M::K, M::kEdgeFloats>(d.roisize), a.n,
+    launch_groups(gauss_fit_kernel<M, G, CPL>, G, threads, gauss_group_floats<M::K>(d.roisize), a.n,
                   d, a, s);
 }
 

@@ -217,70 +217,6 @@ struct GaussModel {
         }
     }
 
-    // Floats stored per pixel edge by edge(): erf, exp (and the G21 exponential for astig).
-    static constexpr int kEdgeFloats = (MID == MODEL_XYZIBG) ? 3 : 2;
-
-    // Edge k of one axis (lower edge of pixel k, k = 0..R): m = (k - t) - 0.5, E = m * c1;
-    // stores erf(E), exp(-E*E) [, exp(-m*m / (2 sig^2))] at out.
-    __device__ __forceinline__ void edge(int k, float t, float c1, float sig, float* out) const {
-        const float mm = SUB(SUB((float)k, t), 0.5f);
-        const float E = MUL(mm, c1);
-        out[0] = erff(E);
-        out[1] = expf(MUL(-E, E));
-        if (MID == MODEL_XYZIBG) out[2 % kEdgeFloats] = expf(DIV(MUL(-mm, mm), MUL(MUL(2.0f, sig), sig)));
-    }
-
-    // term_block() from edge values computed by edge() (any lane of the group) in `ev`
-    // ([R+1][kEdgeFloats]). Identical results: the edge values are the same floats and are
-    // only reused where the arguments agree, as in term_block().
-    template <int N>
-    __device__ __forceinline__ void terms_from_edges(int c0, float t, float c1, float c2, float sig, const float* ev,
-                                                     int R, float4 (&out)[N]) const {
-        float ss2 = 0.0f, ga = 0.0f;
-        if (MID == MODEL_XYZIBG) {
-            ss2 = MUL(MUL(2.0f, sig), sig);
-            ga = DIV(1.0f, MUL(MUL(__fsqrt_rn(MUL(2.0f, PB_PI)), sig), sig));
-        }
-#pragma unroll
-        for (int q = 0; q < N; q++) {
-            const int c = c0 + q;
-            const int cc = c < R ? c : R - 1;  // lanes past the ROI edge compute a harmless copy
-            const float m0 = SUB(SUB((float)cc, t), 0.5f);
-            const float m1 = SUB(SUB((float)(cc + 1), t), 0.5f);
-            const float e1 = MUL(m0, c1);
-            const float erf1 = ev[cc * kEdgeFloats], exp1 = ev[cc * kEdgeFloats + 1];
-            const float p = ADD(SUB((float)cc, t), 0.5f);
-            float e0, erf0, exp0, g0 = 0.0f;
-            if (p == m1) {
-                e0 = MUL(m1, c1);
-                erf0 = ev[(cc + 1) * kEdgeFloats];
-                exp0 = ev[(cc + 1) * kEdgeFloats + 1];
-                if (MID == MODEL_XYZIBG) g0 = ev[(cc + 1) * kEdgeFloats + 2 % kEdgeFloats];
-            } else {
-                e0 = MUL(p, c1);
-                erf0 = erff(e0);
-                exp0 = expf(MUL(-e0, e0));
-                if (MID == MODEL_XYZIBG) g0 = expf(DIV(MUL(-p, p), ss2));
-            }
-            const float delta = SUB(MUL(0.5f, erf0), MUL(0.5f, erf1));
-            const float dE = MUL(c2, SUB(exp1, exp0));
-            float4 r;
-            r.x = delta;
-            r.y = MUL(tI, delta);
-            r.z = MUL(tI, dE);
-            if (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA) {
-                r.w = 0.0f;
-            } else if (MID == MODEL_XYIBG_SIGMA || MID == MODEL_XYIBG_SIGMAXY) {
-                const float dDs = MUL(SUB(MUL(exp1, e1), MUL(exp0, e0)), invSqrtPi);
-                r.w = (MID == MODEL_XYIBG_SIGMAXY) ? MUL(tI, dDs) : dDs;
-            } else {
-                const float g1 = ev[cc * kEdgeFloats + 2 % kEdgeFloats];
-                r.w = MUL(ga, SUB(MUL(m0, g1), MUL(p, g0)));
-            }
-            out[q] = r;
-        }
-    }
-
     // mu and Jacobian of one pixel from its x-term X and y-term Y (see pixel()).
     __device__ __forceinline__ void pixel_xy(const float4& X, const float4& Y, float& mu, float (&J)[K]) const {
         mu = fmaf(X.y, Y.x, tbg);  // tbg + (tI*DeltaX)*DeltaY, one rounding

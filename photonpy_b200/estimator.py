@@ -253,7 +253,7 @@ class Estimator:
                                  f"Given: {initial.shape}")
         if numspots > 0:
             self._Estimator_Estimate(self.inst, numspots, imgs, constants, roipos, initial, params,
-                                     np.zeros(max(1, diag.size), np.float32), iterations, trace, traceBufLen)
+                                     diag if diag.size else np.zeros(1, np.float32), iterations, trace, traceBufLen)
         traces = [trace[k, 0:iterations[k], :] for k in range(numspots)]
         if return_iterations:
             return params, diag, traces, iterations

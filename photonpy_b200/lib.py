@@ -42,6 +42,10 @@ NullableIntArrayType = type("IntArrayType", (IntArrayTypeBase,), {"from_param": 
 
 _load_lock = threading.Lock()
 _cdll = None
+# Every ctypes callback handed to the library stays referenced for the life of the process: the
+# library keeps the last pointer it was given, and an SMLM object that installed it may be
+# garbage-collected while another SMLM object is still in use.
+_callbacks = []
 
 
 def library_path() -> str:
@@ -149,6 +153,7 @@ class SMLM:
 
         self.debugImageCallback = None
         self.debugImageCFunction = self.DebugImageCallbackType(imgcb)
+        _callbacks.append(self.debugImageCFunction)
         self._SetDebugImageCallback(self.debugImageCFunction)
 
     def GetCudaMemUse(self):
@@ -170,6 +175,7 @@ class SMLM:
 
     def SetDebugPrintCallback(self, fn):
         self.dbgPrintCallback = self.DebugPrintCallback(fn)
+        _callbacks.append(self.dbgPrintCallback)
         self._SetDebugPrintCallback(self.dbgPrintCallback)
 
     def SetDebugImageCallback(self, fn):

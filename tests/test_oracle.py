@@ -93,3 +93,23 @@ def test_oracle_derivative_matches_finite_difference():
                 num = num * th[:, k][:, None, None]
             scale = np.abs(d[:, k]).max() + 1e-12
             assert np.abs(num - d[:, k]).max() / scale < 5e-3, (name, k)
+
+
+def test_glrt_restatement_matches_float64_formula():
+    """pso_glrt_f32 (GLRT_PSF.cu:96-131) against the same formula in float64 numpy."""
+    from photonpy_b200 import synth
+    d = synth.xyibg(50, seed=9)
+    m = O.Model(O.XYIBG, d["R"], sigma=d["sigma"])
+    p, _ = m.fit(d["samples"])
+    got = m.glrt(p, d["samples"])
+    ev = m.expected_value(p).astype(np.float64)
+    s = d["samples"].astype(np.float64)
+    mu, dd = np.maximum(ev, 1e-8), np.maximum(s, 1e-8)
+    mean = s.mean(axis=(1, 2))
+    assert np.array_equal(got[:, 2], mean.astype(np.float32))
+    assert np.allclose(got[:, 0], np.sum(dd * np.log(mu) - mu, axis=(1, 2)), rtol=1e-5)
+    ll_off = np.sum(dd * np.log(mean)[:, None, None] - mean[:, None, None], axis=(1, 2))
+    assert np.allclose(got[:, 1], ll_off, rtol=1e-5)
+    # the reference's mean source: first ROI for every spot
+    ref = m.glrt(p, d["samples"], mean_roi=d["samples"][0])
+    assert np.all(ref[:, 2] == got[0, 2])
