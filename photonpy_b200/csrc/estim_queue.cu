@@ -6,8 +6,8 @@
 //  * Spots are packed into Batches of batchSize spots (the reference's Batch,
 //    EstimationQueue.h:54-66). A batch's inputs (samples, constants, initial values) go into a
 //    pinned Stage taken from a bounded pool of pinned buffers that are allocated once and
-//    reused; its per-spot results live in ordinary host memory. Large Schedule calls copy
-//    into the stages with several host threads.
+//    reused; its per-spot results live in ordinary host memory. Schedule copies the samples
+//    into the stages with a small pool of host threads, one launch-sized window at a time.
 //  * A full (or flushed) batch goes to the `todo` list. One worker thread takes the waiting
 //    batches in order and launches them on the first free Lane (one CUDA stream with device
 //    buffers and pinned result buffers): all waiting batches with the same initial-value mode,
@@ -24,10 +24,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -116,26 +118,101 @@ struct DeviceArray {
     T* as() const { return static_cast<T*>(p); }
 };
 
-// Copies `bytes` with up to `threads` host threads (one when the copy is small).
-void copy_parallel(void* dst, const void* src, size_t bytes, int threads) {
-    const size_t kMinPerThread = 2u << 20;
-    const int t = (int)std::min<size_t>((size_t)threads, bytes / kMinPerThread);
-    if (t <= 1) {
-        std::memcpy(dst, src, bytes);
-        return;
+// A fixed set of host threads for the memcpy work of Schedule (the calling thread takes part):
+// copying ROIs into pinned staging buffers is the host-side cost of the queue, and one thread
+// does not reach the bandwidth of the host's memory.
+class CopyPool {
+public:
+    struct Job {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    };
+
+    explicit CopyPool(int threads) {
+        for (int i = 1; i < threads; i++) workers_.emplace_back([this]() { worker(); });
     }
-    std::vector<std::thread> pool;
-    const size_t chunk = align_up((bytes + t - 1) / t, 4096);
-    for (int i = 1; i < t; i++) {
-        const size_t a = i * chunk;
-        if (a >= bytes) break;
-        const size_t b = std::min(bytes, a + chunk);
-        pool.emplace_back(
-            [=]() { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
     }
-    std::memcpy(dst, src, std::min(bytes, chunk));
-    for (auto& th : pool) th.join();
-}
+    CopyPool(const CopyPool&) = delete;
+    CopyPool& operator=(const CopyPool&) = delete;
+
+    // Runs every job; returns when all bytes are copied.
+    void run(const std::vector<Job>& jobs) {
+        size_t total = 0;
+        for (const auto& j : jobs) total += j.bytes;
+        if (workers_.empty() || total < kSerialBytes) {
+            for (const auto& j : jobs) std::memcpy(j.dst, j.src, j.bytes);
+            return;
+        }
+        auto run = std::make_shared<Run>();
+        for (const auto& j : jobs)
+            for (size_t o = 0; o < j.bytes; o += kPiece)
+                run->pieces.push_back({static_cast<char*>(j.dst) + o, static_cast<const char*>(j.src) + o,
+                                       std::min(kPiece, j.bytes - o)});
+        run->remaining = run->pieces.size();
+        {
+            std::lock_guard<std::mutex> g(m_);
+            current_ = run;
+        }
+        cv_.notify_all();
+        work(*run);
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&]() { return run->remaining == 0; });
+        if (current_ == run) current_.reset();
+    }
+
+private:
+    static constexpr size_t kPiece = 1u << 20;
+    static constexpr size_t kSerialBytes = 4u << 20;
+    struct Run {
+        std::vector<Job> pieces;
+        std::atomic<size_t> next{0};
+        size_t remaining = 0;  // guarded by m_
+    };
+
+    void work(Run& r) {
+        size_t done = 0;
+        for (;;) {
+            const size_t i = r.next.fetch_add(1);
+            if (i >= r.pieces.size()) break;
+            std::memcpy(r.pieces[i].dst, r.pieces[i].src, r.pieces[i].bytes);
+            done++;
+        }
+        if (done) {
+            std::lock_guard<std::mutex> g(m_);
+            r.remaining -= done;
+            if (r.remaining == 0) done_.notify_all();
+        }
+    }
+
+    void worker() {
+        std::shared_ptr<Run> seen;
+        for (;;) {
+            std::shared_ptr<Run> r;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&]() { return stop_ || (current_ && current_ != seen); });
+                if (stop_) return;
+                r = current_;
+            }
+            seen = r;
+            work(*r);
+        }
+    }
+
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    std::shared_ptr<Run> current_;
+    bool stop_ = false;
+};
 
 }  // namespace
 
@@ -169,7 +246,7 @@ struct EstimQueue {
     int batchSize = 0, limitSpots = 0, launchCap = 0, batchesPerLaunch = 1;
     bool keepSamples = false;
     int device = 0;
-    int copyThreads = 1;
+    std::unique_ptr<CopyPool> copier;
 
     std::mutex m;                // everything below up to schedMtx
     std::condition_variable cv;  // any change of it
@@ -212,7 +289,7 @@ struct EstimQueue {
         stageMax = std::max((numStreams + 1) * batchesPerLaunch + 2, limitSpots / batchSize + 2);
         recycleMax = (size_t)stageMax;
         const unsigned hw = std::thread::hardware_concurrency();
-        copyThreads = (int)std::max(1u, std::min(8u, hw / 2));
+        copier.reset(new CopyPool((int)std::max(1u, std::min(8u, hw / 2))));
         PBQ_CUDA(cudaGetDevice(&device));
         for (int i = 0; i < numStreams; i++) {
             Lane& L = lanes.emplace_back();
@@ -457,29 +534,62 @@ struct EstimQueue {
         }
         std::lock_guard<std::mutex> g(schedMtx);
         const bool init = initial != nullptr;
+        // Windows of at most one launch (batchesPerLaunch batches, about 64 MiB of samples):
+        // take the batches, copy the window's samples with the copy pool, then hand the full
+        // batches to the worker in order. A window never holds more stages than one launch, so
+        // the stage pool (sized for every lane's launch plus one) cannot run dry inside it.
         int i = 0;
         while (i < count) {
-            if (next && next->n > 0 && next->hasInitial != init) flush_next();
-            if (!next) next = take_batch();
-            Batch* b = next;
-            b->hasInitial = init;
-            const int m_ = std::min(batchSize - b->n, count - i);
-            const int o = b->n;
-            if (ids) std::memcpy(b->ids.data() + o, ids + i, sizeof(int) * m_);
-            else std::fill(b->ids.begin() + o, b->ids.begin() + o + m_, 0);
-            copy_parallel(b->stage->smp + (size_t)o * npix, smp + (size_t)i * npix, sizeof(float) * npix * m_,
-                          copyThreads);
-            if (keepSamples)
-                std::memcpy(b->samples.data() + (size_t)o * npix, smp + (size_t)i * npix, sizeof(float) * npix * m_);
-            if (NC) std::memcpy(b->stage->consts + (size_t)o * NC, consts + (size_t)i * NC, sizeof(float) * NC * m_);
-            if (roipos)
-                std::memcpy(b->roipos.data() + (size_t)o * dims, roipos + (size_t)i * dims, sizeof(int) * dims * m_);
-            else
-                std::fill(b->roipos.begin() + (size_t)o * dims, b->roipos.begin() + (size_t)(o + m_) * dims, 0);
-            if (init) std::memcpy(b->stage->initial + (size_t)o * K, initial + (size_t)i * K, sizeof(float) * K * m_);
-            b->n += m_;
-            i += m_;
-            if (b->n == batchSize) flush_next();
+            std::vector<CopyPool::Job> jobs;
+            std::vector<Batch*> full;
+            int taken = 0;
+            while (i < count && taken < batchesPerLaunch) {
+                if (next && next->n > 0 && next->hasInitial != init) {
+                    full.push_back(next);
+                    next = nullptr;
+                }
+                if (!next) {
+                    next = take_batch();
+                    taken++;
+                }
+                Batch* b = next;
+                b->hasInitial = init;
+                const int m_ = std::min(batchSize - b->n, count - i);
+                const int o = b->n;
+                if (ids) std::memcpy(b->ids.data() + o, ids + i, sizeof(int) * m_);
+                else std::fill(b->ids.begin() + o, b->ids.begin() + o + m_, 0);
+                const size_t nb = sizeof(float) * npix * m_;
+                jobs.push_back({b->stage->smp + (size_t)o * npix, smp + (size_t)i * npix, nb});
+                if (keepSamples) jobs.push_back({b->samples.data() + (size_t)o * npix, smp + (size_t)i * npix, nb});
+                if (NC)
+                    std::memcpy(b->stage->consts + (size_t)o * NC, consts + (size_t)i * NC, sizeof(float) * NC * m_);
+                if (roipos)
+                    std::memcpy(b->roipos.data() + (size_t)o * dims, roipos + (size_t)i * dims,
+                                sizeof(int) * dims * m_);
+                else
+                    std::fill(b->roipos.begin() + (size_t)o * dims, b->roipos.begin() + (size_t)(o + m_) * dims, 0);
+                if (init)
+                    std::memcpy(b->stage->initial + (size_t)o * K, initial + (size_t)i * K, sizeof(float) * K * m_);
+                b->n += m_;
+                i += m_;
+                if (b->n == batchSize) {
+                    full.push_back(b);
+                    next = nullptr;
+                }
+            }
+            copier->run(jobs);
+            if (!full.empty()) {
+                long long spots = 0;
+                {
+                    std::lock_guard<std::mutex> g2(m);
+                    for (auto* b : full) {
+                        todo.push_back(b);
+                        spots += b->n;
+                    }
+                    queuedSpots += spots;
+                }
+                cv.notify_all();
+            }
         }
     }
 
