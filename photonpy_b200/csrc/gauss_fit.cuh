@@ -31,6 +31,158 @@ __host__ __device__ constexpr int gauss_group_floats(int R) {
                     32) + 16;
 }
 
+// ---------------------------------------------------------------------------------------
+// Separable accumulation of the Poisson Hessian and gradient.
+//
+// Every Gaussian model's Jacobian is J = C v over the "virtual" columns
+//   v = [X.z Y.x, X.x Y.z, X.x Y.x, 1, X.w Y.x, X.x Y.w]
+// of x-terms X (the pixel's column) and y-terms Y (its row); V = 4 for the fixed-sigma
+// models, 6 otherwise, and C is a 0/1 selection for XYIBg and SigmaXY, a sum of the two sigma
+// columns (times I) for one free sigma, and a dsigma/dz combination of them for astig. Each
+// sum_p w v_i v_j is (product of y-factors) * sum over the row's columns of w * (product of
+// x-factors); per pixel only the distinct x-factor products are accumulated (10, or 6), and
+// the y-factors are applied once per row. Per pixel that is about 31 FP32 operations for
+// SigmaXY instead of the 44 of a per-pixel Jacobian outer product; the sums are the same
+// terms in another order.
+// ---------------------------------------------------------------------------------------
+__host__ __device__ constexpr int gauss_virtual_cols(int mid) {
+    return (mid == MODEL_XYIBG || mid == MODEL_XYIBG_CONSTSIGMA) ? 4 : 6;
+}
+
+// T (per row): sum over columns of w times the distinct x-factor products, in the order
+//   V = 6: zz, zx, z, zw, xx, x, xw, 1, w, ww       V = 4: zz, zx, z, xx, x, 1
+template <int V>
+__device__ __forceinline__ void row_add_w(float (&T)[V == 6 ? 10 : 6], float w, const float4& X) {
+    const float wz = w * X.z, wx = w * X.x;
+    T[0] += wz * X.z;
+    T[1] += wz * X.x;
+    T[2] += wz;
+    if constexpr (V == 6) {
+        const float ww = w * X.w;
+        T[3] += wz * X.w;
+        T[4] += wx * X.x;
+        T[5] += wx;
+        T[6] += wx * X.w;
+        T[7] += w;
+        T[8] += ww;
+        T[9] += ww * X.w;
+    } else {
+        T[3] += wx * X.x;
+        T[4] += wx;
+        T[5] += w;
+    }
+}
+
+// U (per row): sum over columns of bf = 1 - x/mu times the distinct x-factors z, x, 1 (, w).
+template <int V>
+__device__ __forceinline__ void row_add_b(float (&U)[V == 6 ? 4 : 3], float bf, const float4& X) {
+    U[0] += bf * X.z;
+    U[1] += bf * X.x;
+    U[2] += bf;
+    if constexpr (V == 6) U[3 % (V == 6 ? 4 : 3)] += bf * X.w;
+}
+
+// Applies one row's y-factors. av = [alpha_v packed upper (V(V+1)/2) | beta_v (V) | chi^2].
+template <int V>
+__device__ __forceinline__ void row_finish(float* av, const float (&T)[V == 6 ? 10 : 6],
+                                           const float (&U)[V == 6 ? 4 : 3], const float4& Y) {
+    const float xx = Y.x * Y.x, xz = Y.x * Y.z, zz = Y.z * Y.z;
+    if constexpr (V == 6) {
+        const float xw = Y.x * Y.w, zw = Y.z * Y.w, ww = Y.w * Y.w;
+        av[0] += xx * T[0];
+        av[1] += xz * T[1];
+        av[2] += xx * T[1];
+        av[3] += Y.x * T[2];
+        av[4] += xx * T[3];
+        av[5] += xw * T[1];
+        av[6] += zz * T[4];
+        av[7] += xz * T[4];
+        av[8] += Y.z * T[5];
+        av[9] += xz * T[6];
+        av[10] += zw * T[4];
+        av[11] += xx * T[4];
+        av[12] += Y.x * T[5];
+        av[13] += xx * T[6];
+        av[14] += xw * T[4];
+        av[15] += T[7];
+        av[16] += Y.x * T[8];
+        av[17] += Y.w * T[5];
+        av[18] += xx * T[9];
+        av[19] += xw * T[6];
+        av[20] += ww * T[4];
+        av[21] -= Y.x * U[0];
+        av[22] -= Y.z * U[1];
+        av[23] -= Y.x * U[1];
+        av[24] -= U[2];
+        av[25] -= Y.x * U[3 % (V == 6 ? 4 : 3)];
+        av[26] -= Y.w * U[1];
+    } else {
+        av[0] += xx * T[0];
+        av[1] += xz * T[1];
+        av[2] += xx * T[1];
+        av[3] += Y.x * T[2];
+        av[4] += zz * T[3];
+        av[5] += xz * T[3];
+        av[6] += Y.z * T[4];
+        av[7] += xx * T[3];
+        av[8] += Y.x * T[4];
+        av[9] += T[5];
+        av[10] -= Y.x * U[0];
+        av[11] -= Y.z * U[1];
+        av[12] -= Y.x * U[1];
+        av[13] -= U[2];
+    }
+}
+
+// Model Hessian/gradient (acc = [alpha packed | beta | chi^2], K parameters) from the
+// virtual ones: alpha = C alpha_v C^T, beta = C beta_v.
+template <class M, int NV, int NACC>
+__device__ __forceinline__ void map_virtual(const float (&av)[NV], float (&acc)[NACC], const M& m) {
+    constexpr int MID = M::kId;
+    constexpr int K = M::K;
+    constexpr int V = gauss_virtual_cols(MID);
+    constexpr int NAV = V * (V + 1) / 2;
+    constexpr int NA = K * (K + 1) / 2;
+    if constexpr (MID == MODEL_XYIBG || MID == MODEL_XYIBG_CONSTSIGMA || MID == MODEL_XYIBG_SIGMAXY) {
+#pragma unroll
+        for (int q = 0; q < NACC; q++) acc[q] = av[q];
+    } else {
+        // model column k is virtual column src(k), or (for k == kc) c4 v4 + c5 v5
+        constexpr int kc = (MID == MODEL_XYZIBG) ? 2 : 4;
+        float c4, c5;
+        if constexpr (MID == MODEL_XYZIBG) {
+            c4 = m.tI * m.dsxz;
+            c5 = m.tI * m.dsyz;
+        } else {
+            c4 = m.tI;
+            c5 = m.tI;
+        }
+        auto src = [](int k) constexpr -> int {
+            return (MID == MODEL_XYZIBG) ? (k < 2 ? k : k - 1) : k;  // astig: x, y, (z), I, bg
+        };
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+#pragma unroll
+            for (int j = i; j < K; j++) {
+                const int q = upk(i, j, K);
+                if (i != kc && j != kc) {
+                    acc[q] = av[upk(src(i), src(j), V)];
+                } else if (i == kc && j == kc) {
+                    acc[q] = c4 * c4 * av[upk(4, 4, V)] + 2.0f * c4 * c5 * av[upk(4, 5, V)] +
+                             c5 * c5 * av[upk(5, 5, V)];
+                } else {
+                    const int o = (i == kc) ? src(j) : src(i);
+                    acc[q] = c4 * av[upk(o, 4, V)] + c5 * av[upk(o, 5, V)];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            acc[NA + k] = (k == kc) ? c4 * av[NAV + 4] + c5 * av[NAV + 5] : av[NAV + src(k)];
+        acc[NACC - 1] = av[NV - 1];
+    }
+}
+
 // Fit the ROIs roi, roi + roiStep, ... < roiEnd of one (model, ROI size) with one group of G
 // lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_floats floats).
 template <class M, int G, int CPL>
@@ -129,9 +281,13 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                 if (c0 + q < R) ytab[c0 + q] = Yown[q];
             __syncwarp(mask);
 
-            float acc[NACC];
+            constexpr int V = gauss_virtual_cols(M::kId);
+            constexpr int NV = V * (V + 1) / 2 + V + 1;
+            constexpr int NT = (V == 6) ? 10 : 6;
+            constexpr int NU = (V == 6) ? 4 : 3;
+            float av[NV];
 #pragma unroll
-            for (int q = 0; q < NACC; q++) acc[q] = 0.0f;
+            for (int q = 0; q < NV; q++) av[q] = 0.0f;
             const bool lm = (mode == MODE_LM);
             if (c0 < R) {
                 for (int y = 0; y < R; y++) {
@@ -150,11 +306,15 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
 #pragma unroll
                         for (int q = 0; q < CPL; q++) sv[q] = (c0 + q < R) ? spix[y * R + c0 + q] : 0.0f;
                     }
+                    float T[NT], U[NU];
+#pragma unroll
+                    for (int q = 0; q < NT; q++) T[q] = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < NU; q++) U[q] = 0.0f;
 #pragma unroll
                     for (int q = 0; q < CPL; q++) {
                         if (CPL > 1 && c0 + q >= R) continue;
-                        float mu, J[K];
-                        m.pixel_xy(X[q], Y, mu, J);
+                        const float mu = fmaf(X[q].y, Y.x, m.tbg);  // tbg + (tI*DeltaX)*DeltaY
                         const float s = sv[q];
                         float w;
                         if (lm) {
@@ -164,30 +324,25 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                             const float invmu = rcp_fast(muc);
                             const float t = __fmul_rn(sval, invmu);
                             w = __fmul_rn(t, invmu);
-                            const float bf = __fsub_rn(1.0f, t);
-#pragma unroll
-                            for (int k = 0; k < K; k++) acc[NA + k] -= bf * J[k];
+                            row_add_b<V>(U, __fsub_rn(1.0f, t), X[q]);
                         } else {
                             // ComputeChiSquareAndCRLB (Estimation.h:76-95)
                             const float mu8 = fmaxf(1e-8f, mu);
                             w = rcp_nr(mu8);
                             if (haveSmp) {
                                 const float e = s - mu8;
-                                acc[NACC - 1] += __fdiv_rn(e * e, mu8);
+                                av[NV - 1] += __fdiv_rn(e * e, mu8);
                             }
                         }
-                        int qa = 0;
-#pragma unroll
-                        for (int i = 0; i < K; i++) {
-                            const float wi = J[i] * w;
-#pragma unroll
-                            for (int j = i; j < K; j++) acc[qa++] += wi * J[j];
-                        }
+                        row_add_w<V>(T, w, X[q]);
                     }
+                    row_finish<V>(av, T, U, Y);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < NACC; q++) acc[q] = group_sum<G>(acc[q], mask);
+            for (int q = 0; q < NV; q++) av[q] = group_sum<G>(av[q], mask);
+            float acc[NACC];
+            map_virtual<M>(av, acc, m);
 
             if (lm) {
                 float step[K], dk[K];
