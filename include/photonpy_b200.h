@@ -88,6 +88,13 @@ Estimator* Gauss2D_CreatePSF_XYIBgSigmaXY(int roisize, float initialSigmaX, floa
 /* Estimators/Gaussian/GaussianPSF.cu:36-59 (the calibration is passed by reference in C++,
  * i.e. as a pointer in the ABI) */
 Estimator* Gauss2D_CreatePSF_XYZIBg(int roisize, const Gauss3D_Calibration* calib, bool cuda, Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:62-85: theta = (x, y, I, bg, bgx, bgy), sigma_x/sigma_y as
+ * 2 per-spot constants, mu = bg + bgx (x - W/2) + bgy (y - H/2) + I PSF. */
+Estimator* Gauss2D_CreatePSF_XYITiltedBg(int roisize, bool cuda, Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:187-212: theta = (x, y, I, bg, bgx, bgy, sx, sy). As in the
+ * reference, the tilt is in the Jacobian but not in mu (GaussianPSFModels.h:542 vs 549). */
+Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int roisize, float initialSigmaX, float initialSigmaY, bool cuda,
+                                                Context* ctx);
 /* Extension (no reference counterpart): astigmatic model with the quartic B term. */
 Estimator* Gauss2D_CreatePSF_XYZIBgB(int roisize, const Gauss3D_CalibrationB* calib, bool cuda, Context* ctx);
 /* Estimators/CSpline/CubicSplinePSF.cu:55-107. Only mode 0 (flat background) is supported;
@@ -118,7 +125,7 @@ void Estimator_ComputeExpectedValue(Estimator* e, int numspots, const float* par
                                     const int* spotpos, float* ev);
 /* Fit (centre-of-mass start when initial == NULL). params[n][K], iterations[n] (nullable;
  * = i+1 at the stop, maxIterations+1 when capped), trace[n][traceBufLen][K] (nullable),
- * diagnostics: numDiag == 0 floats per spot (untouched). */
+ * diagnostics: numDiag floats per spot (3 for GLRT estimators; none, untouched, otherwise). */
 void Estimator_Estimate(Estimator* e, int numspots, const float* sample, const float* constants, const int* spotpos,
                         const float* initial, float* params, float* diagnostics, int* iterations, float* trace,
                         int traceBufLen);
@@ -192,8 +199,6 @@ void DrawROIs(float* image, int width, int height, const float* rois, int numroi
 void Gauss2D_Draw(double* image, int imgw, int imgh, float* spotList, int nspots, float addSigma);
 void Gauss2D_EstimateIntensityBg(const float* imageData, float* IBg, float* IBg_crlb, int numspots, const float* xy,
                                  const int* roipos, const float* sigma, int imgw, int maxIterations, int cuda);
-Estimator* Gauss2D_CreatePSF_XYITiltedBg(int roisize, bool cuda, Context* ctx);
-Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int roisize, float sx, float sy, bool cuda, Context* ctx);
 
 /* ---- Extensions (no reference counterpart) ------------------------------------------ */
 /* Message of the last error on this thread ("" if none); cleared by PB200_ClearError. */

@@ -20,7 +20,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define PSO_MAXK 6
+#define PSO_MAXK 8
 
 enum {
     PSO_XYIBG = 0,            /* Gauss2D_Model_XYIBg            (GaussianPSFModels.h:35-152)  */
@@ -28,7 +28,9 @@ enum {
     PSO_XYIBG_SIGMA = 2,      /* Gauss2D_Model_XYIBgSigma       (GaussianPSFModels.h:308-387) */
     PSO_XYIBG_SIGMAXY = 3,    /* Gauss2D_Model_XYIBgSigmaXY     (GaussianPSFModels.h:391-471) */
     PSO_XYZIBG = 4,           /* Gauss2D_Model_XYZIBg (astig)   (GaussianPSFModels.h:636-751) */
-    PSO_CSPLINE = 5           /* CSpline_Model_XYZIBg           (CubicSplinePSFModels.h:14-154) */
+    PSO_CSPLINE = 5,          /* CSpline_Model_XYZIBg           (CubicSplinePSFModels.h:14-154) */
+    PSO_XYITILTEDBG = 6,      /* Gauss2D_Model_XYITiltedBg      (GaussianPSFModels.h:228-304) */
+    PSO_XYITILTEDBG_SIGMAXY = 7 /* Gauss2D_Model_XYITiltedBgSigmaXY (GaussianPSFModels.h:474-558) */
 };
 
 typedef struct {
@@ -47,12 +49,13 @@ int pso_num_params(int model)
 {
     switch (model) {
     case PSO_XYIBG: case PSO_XYIBG_CONSTSIGMA: return 4;
-    case PSO_XYIBG_SIGMAXY: return 6;
+    case PSO_XYIBG_SIGMAXY: case PSO_XYITILTEDBG: return 6;
+    case PSO_XYITILTEDBG_SIGMAXY: return 8;
     default: return 5;
     }
 }
 
-int pso_num_constants(int model) { return model == PSO_XYIBG_CONSTSIGMA ? 2 : 0; }
+int pso_num_constants(int model) { return (model == PSO_XYIBG_CONSTSIGMA || model == PSO_XYITILTEDBG) ? 2 : 0; }
 
 int pso_sizeof_model(void) { return (int)sizeof(pso_model_t); }
 

@@ -14,6 +14,7 @@
  *   LUPDecompose / LUPInvert  SolveMatrix.h:267-318, 344-367; InvertMatrix 411-452
  *   Gaussian models           Estimators/Gaussian/GaussianPSFModels.h:35-471, 636-751
  *   Cubic spline model        Estimators/CSpline/CubicSplinePSFModels.h:14-154
+ *   Tilted-background models  Estimators/Gaussian/GaussianPSFModels.h:228-304, 474-558
  */
 
 #define FN(name) CAT(name, SUFFIX)
@@ -152,6 +153,52 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
         }
         break;
     }
+    case PSO_XYITILTEDBG:
+    case PSO_XYITILTEDBG_SIGMAXY: {
+        /* mu = bg + bgx (x - W/2) + bgy (y - H/2) + I DeltaX DeltaY for XYITiltedBg (sigma from the
+         * spot's constants). XYITiltedBgSigmaXY has the tilt in its Jacobian but, as in the
+         * reference (GaussianPSFModels.h:542 vs 549), not in mu. */
+        const int free = m->model == PSO_XYITILTEDBG_SIGMAXY;
+        REAL tx = theta[0], ty = theta[1], tI = theta[2], tbg = theta[3], bgx = theta[4], bgy = theta[5];
+        REAL tsx = free ? theta[6] : (REAL)consts[0];
+        REAL tsy = free ? theta[7] : (REAL)consts[1];
+        const REAL halfw = (REAL)((float)W * 0.5f), halfh = (REAL)((float)H * 0.5f);
+        const REAL invSqrtPi = (REAL)1 / SQRT(PI_);
+        const REAL OneOverSqrt2PiSigmaX = (REAL)1 / (SQRT(2 * PI_) * tsx);
+        const REAL OneOverSqrt2SigmaX = (REAL)1 / (SQRT((REAL)2) * tsx);
+        const REAL OneOverSqrt2PiSigmaY = (REAL)1 / (SQRT(2 * PI_) * tsy);
+        const REAL OneOverSqrt2SigmaY = (REAL)1 / (SQRT((REAL)2) * tsy);
+        for (int y = 0; y < H; y++) {
+            REAL Yexp0 = ((REAL)y - ty + (REAL)0.5) * OneOverSqrt2SigmaY;
+            REAL Yexp1 = ((REAL)y - ty - (REAL)0.5) * OneOverSqrt2SigmaY;
+            REAL DeltaY = (REAL)0.5 * ERF(Yexp0) - (REAL)0.5 * ERF(Yexp1);
+            REAL expY1 = EXP(-Yexp1 * Yexp1), expY0 = EXP(-Yexp0 * Yexp0);
+            REAL dEy = OneOverSqrt2PiSigmaY * (expY1 - expY0);
+            REAL dDeltaY_dsigma = (expY1 * Yexp1 - expY0 * Yexp0) * invSqrtPi;
+            for (int x = 0; x < W; x++) {
+                REAL Xexp0 = ((REAL)x - tx + (REAL)0.5) * OneOverSqrt2SigmaX;
+                REAL Xexp1 = ((REAL)x - tx - (REAL)0.5) * OneOverSqrt2SigmaX;
+                REAL DeltaX = (REAL)0.5 * ERF(Xexp0) - (REAL)0.5 * ERF(Xexp1);
+                REAL expX1 = EXP(-Xexp1 * Xexp1), expX0 = EXP(-Xexp0 * Xexp0);
+                REAL dEx = OneOverSqrt2PiSigmaX * (expX1 - expX0);
+                REAL dDeltaX_dsigma = (expX1 * Xexp1 - expX0 * Xexp0) * invSqrtPi;
+                int p = y * W + x;
+                if (free) mu[p] = tbg + tI * DeltaX * DeltaY;
+                else mu[p] = tbg + bgx * ((REAL)x - halfw) + bgy * ((REAL)y - halfh) + tI * DeltaX * DeltaY;
+                jac[0 * npix + p] = tI * dEx * DeltaY;
+                jac[1 * npix + p] = tI * dEy * DeltaX;
+                jac[2 * npix + p] = DeltaX * DeltaY;
+                jac[3 * npix + p] = 1;
+                jac[4 * npix + p] = (REAL)x - halfw;
+                jac[5 * npix + p] = (REAL)y - halfh;
+                if (free) {
+                    jac[6 * npix + p] = tI * dDeltaX_dsigma * DeltaY;
+                    jac[7 * npix + p] = tI * dDeltaY_dsigma * DeltaX;
+                }
+            }
+        }
+        break;
+    }
     case PSO_CSPLINE: {
         const int Nz = m->spline_shape[0], Ny = m->spline_shape[1], Nx = m->spline_shape[2];
         const float du_f = (m->spline_zmax - m->spline_zmin) / (float)Nz;
@@ -250,6 +297,20 @@ static void FN(check_limits)(const pso_model_t* m, REAL* t)
         t[3] = FMAX(t[3], 10);
         t[4] = FMAX(t[4], 0);
         break;
+    case PSO_XYITILTEDBG:
+        t[0] = FN(o_clamp)(t[0], (REAL)1.5f, (REAL)((float)R - 1.5f - 1));
+        t[1] = FN(o_clamp)(t[1], (REAL)1.5f, (REAL)((float)R - 1.5f - 1));
+        if (t[2] < 25) t[2] = 25;
+        if (t[3] < 0) t[3] = 0;
+        break;
+    case PSO_XYITILTEDBG_SIGMAXY:
+        t[0] = FN(o_clamp)(t[0], (REAL)1.5f, (REAL)((float)R - 1.5f - 1));
+        t[1] = FN(o_clamp)(t[1], (REAL)1.5f, (REAL)((float)R - 1.5f - 1));
+        if (t[2] < 10) t[2] = 10;
+        if (t[3] < 0) t[3] = 0;
+        t[6] = FN(o_clamp)(t[6], 1, (REAL)(R * 0.5f));
+        t[7] = FN(o_clamp)(t[7], 1, (REAL)(R * 0.5f));
+        break;
     case PSO_CSPLINE:
         t[0] = FN(o_clamp)(t[0], (REAL)1.5f, (REAL)((float)R - 1.0f - 1.5f));
         t[1] = FN(o_clamp)(t[1], (REAL)1.5f, (REAL)((float)R - 1.0f - 1.5f));
@@ -284,6 +345,11 @@ static void FN(initial_estimate)(const pso_model_t* m, const float* smp, REAL* t
         t[0] = comx; t[1] = comy; t[2] = 0; t[3] = sum; t[4] = (REAL)0.01f; break;
     case PSO_CSPLINE:
         t[0] = comx; t[1] = comy; t[2] = 0; t[3] = sum; t[4] = 0; break;
+    case PSO_XYITILTEDBG:
+        t[0] = comx; t[1] = comy; t[2] = sum * (REAL)0.7f; t[3] = 0; t[4] = 0; t[5] = 0; break;
+    case PSO_XYITILTEDBG_SIGMAXY:
+        t[0] = comx; t[1] = comy; t[2] = sum; t[3] = 0; t[4] = 0; t[5] = 0;
+        t[6] = m->sigma[0]; t[7] = m->sigma[1]; break;
     }
 }
 
@@ -294,11 +360,15 @@ static const float* FN(stop_limits)(int model)
     static const float g6[] = {1e-5f, 1e-5f, 1e-1f, 1e-4f, 1e-5f, 1e-5f};
     static const float a5[] = {1e-4f, 1e-4f, 1e-1f, 1e-4f, 1e-4f};
     static const float s5[] = {1e-4f, 1e-4f, 1e-7f, 1e-4f, 1e-4f};
+    static const float t6[] = {1e-5f, 1e-5f, 1e-1f, 1e-5f, 1e-5f, 1e-5f};
+    static const float t8[] = {1e-5f, 1e-5f, 1e-1f, 1e-4f, 1e-4f, 1e-4f, 1e-5f, 1e-5f};
     switch (model) {
     case PSO_XYIBG: case PSO_XYIBG_CONSTSIGMA: return g4;
     case PSO_XYIBG_SIGMA: return g5;
     case PSO_XYIBG_SIGMAXY: return g6;
     case PSO_XYZIBG: return a5;
+    case PSO_XYITILTEDBG: return t6;
+    case PSO_XYITILTEDBG_SIGMAXY: return t8;
     default: return s5;
     }
 }

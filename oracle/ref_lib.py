@@ -56,6 +56,8 @@ def lib():
             ("Gauss2D_CreatePSF_XYIBgSigmaXY", [ct.c_int, ct.c_float, ct.c_float, ct.c_bool, vp]),
             ("Gauss2D_CreatePSF_XYZIBg", [ct.c_int, ct.POINTER(Gauss3DCalib), ct.c_bool, vp]),
             ("CSpline_CreatePSF", [ct.c_int, ct.POINTER(CSplineCalib), vp, ct.c_int, ct.c_bool, vp]),
+            ("Gauss2D_CreatePSF_XYITiltedBg", [ct.c_int, ct.c_bool, vp]),
+            ("Gauss2D_CreatePSF_XYITiltedBgSigmaXY", [ct.c_int, ct.c_float, ct.c_float, ct.c_bool, vp]),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -107,6 +109,10 @@ class RefEstimator:
             inst = L.Gauss2D_CreatePSF_XYIBgSigma(roisize, sigma[0], cuda, self.ctx)
         elif kind == "XYIBgSigmaXY":
             inst = L.Gauss2D_CreatePSF_XYIBgSigmaXY(roisize, sigma[0], sigma[1], cuda, self.ctx)
+        elif kind == "XYITiltedBg":
+            inst = L.Gauss2D_CreatePSF_XYITiltedBg(roisize, cuda, self.ctx)
+        elif kind == "XYITiltedBgSigmaXY":
+            inst = L.Gauss2D_CreatePSF_XYITiltedBgSigmaXY(roisize, sigma[0], sigma[1], cuda, self.ctx)
         elif kind == "XYZIBg":
             c = Gauss3DCalib()
             for i in range(4):

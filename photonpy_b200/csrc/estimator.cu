@@ -122,6 +122,8 @@ FitLaunch fit_launcher_for(int model, int G, int CPL, int variant) {
     case MODEL_XYIBG_SIGMAXY: return fit_launcher_sigmaxy(G, CPL, variant);
     case MODEL_XYZIBG: return fit_launcher_astig(G, CPL, variant);
     case MODEL_CSPLINE: return fit_launcher_spline(G, CPL, variant);
+    case MODEL_XYITILTEDBG: return fit_launcher_tilted(G, CPL, variant);
+    case MODEL_XYITILTEDBG_SIGMAXY: return fit_launcher_tilted_sxy(G, CPL, variant);
     }
     throw Error("unknown model");
 }
@@ -134,6 +136,8 @@ AdjointLaunch adjoint_launcher_for(int model) {
     case MODEL_XYIBG_SIGMAXY: return adjoint_launcher_sigmaxy();
     case MODEL_XYZIBG: return adjoint_launcher_astig();
     case MODEL_CSPLINE: return adjoint_launcher_spline();
+    case MODEL_XYITILTEDBG:
+    case MODEL_XYITILTEDBG_SIGMAXY: throw Error("PoissonNLLAdjoint: not provided for the tilted-background models");
     }
     throw Error("unknown model");
 }
@@ -146,6 +150,8 @@ EvalLaunch eval_launcher_for(int model, int G) {
     case MODEL_XYIBG_SIGMAXY: return eval_launcher_sigmaxy(G);
     case MODEL_XYZIBG: return eval_launcher_astig(G);
     case MODEL_CSPLINE: return eval_launcher_spline(G);
+    case MODEL_XYITILTEDBG: return eval_launcher_tilted(G);
+    case MODEL_XYITILTEDBG_SIGMAXY: return eval_launcher_tilted_sxy(G);
     }
     throw Error("unknown model");
 }
@@ -227,7 +233,7 @@ struct Estimator {
     FitLaunch fit_launch() const {
         int G = lanes_for();
         const int R = desc.roisize;
-        if (desc.model != MODEL_CSPLINE && variant == 0) {
+        if (desc.model <= MODEL_XYZIBG && variant == 0) {  // column-blocked kernel: flat-background Gaussians
             while (G < 32 && (R + G - 1) / G > 4) G *= 2;
             const int cpl = (R + G - 1) / G;
             if (cpl <= (G == 32 ? 2 : 4)) return fit_launcher_for(desc.model, G, cpl, 0);
@@ -294,6 +300,15 @@ Estimator* make_gauss(int model, int roisize, float s0, float s1, const float* a
     case MODEL_XYZIBG:
         e->format = "x,y,z,I,bg";
         e->limits = {{border, xyhi}, {border, xyhi}, {minz, maxz}, {10.0f, 1e9f}, {1e-6f, 1e9f}};
+        break;
+    case MODEL_XYITILTEDBG:  // GaussianPSF.cu:67-74
+        e->format = "x,y,I,bg,bgx,bgy";
+        e->limits = {{border, xyhi}, {border, xyhi}, {10.0f, 1e9f}, {1e-6f, 1e9f}, {-1e9f, 1e9f}, {-1e9f, 1e9f}};
+        break;
+    case MODEL_XYITILTEDBG_SIGMAXY:  // GaussianPSF.cu:193-202
+        e->format = "x,y,I,bg,bgx,bgy,sx,sy";
+        e->limits = {{border, xyhi}, {border, xyhi}, {10.0f, 1e9f}, {1e-6f, 1e9f}, {-1e9f, 1e9f}, {-1e9f, 1e9f},
+                     {1.0f, roisize * 2.0f}, {1.0f, roisize * 2.0f}};
         break;
     }
     attach(e, ctx);
@@ -1138,7 +1153,7 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     check_estimator(e);
                     const int R = e->desc.roisize;
                     const int cpl = (R + G - 1) / G;
-                    if (e->desc.model == MODEL_CSPLINE || cpl > 4)
+                    if (e->desc.model > MODEL_XYZIBG || cpl > 4)
                         throw Error("MixedPlanCreate: buckets must be Gaussian models with ROI size <= 16");
                     if (counts[b] < 0) throw Error("MixedPlanCreate: negative count");
                     if (e->numconst && counts[b] > 0 && (!d_constants || !d_constants[b]))
@@ -1375,13 +1390,15 @@ void Gauss2D_EstimateIntensityBg(const float*, float*, float*, int, const float*
                                  int) {
     not_provided("Gauss2D_EstimateIntensityBg");
 }
-Estimator* Gauss2D_CreatePSF_XYITiltedBg(int, bool, Context*) {
-    not_provided("Gauss2D_CreatePSF_XYITiltedBg");
-    return nullptr;
+Estimator* Gauss2D_CreatePSF_XYITiltedBg(int roisize, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {
+        return make_gauss(MODEL_XYITILTEDBG, roisize, 0, 0, nullptr, nullptr, 0, 0, ctx);
+    }, (Estimator*)nullptr);
 }
-Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int, float, float, bool, Context*) {
-    not_provided("Gauss2D_CreatePSF_XYITiltedBgSigmaXY");
-    return nullptr;
+Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int roisize, float sx, float sy, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* {
+        return make_gauss(MODEL_XYITILTEDBG_SIGMAXY, roisize, sx, sy, nullptr, nullptr, 0, 0, ctx);
+    }, (Estimator*)nullptr);
 }
 
 }  // extern "C"

@@ -167,6 +167,7 @@ inline void launch_crlb(int K, const float* fisher, float* crlb, float* chisq, i
     case 4: crlb_kernel<4><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     case 5: crlb_kernel<5><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     case 6: crlb_kernel<6><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
+    case 8: crlb_kernel<8><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     default: throw std::runtime_error("crlb: unsupported number of parameters");
     }
     check_launch("crlb kernel launch");
@@ -197,5 +198,9 @@ PB_DECLARE_MODEL_LAUNCHERS(sigmaxy)
 PB_DECLARE_MODEL_LAUNCHERS(astig)
 PB_DECLARE_MODEL_LAUNCHERS(spline)
 #undef PB_DECLARE_MODEL_LAUNCHERS
+FitLaunch fit_launcher_tilted(int G, int CPL, int variant);
+FitLaunch fit_launcher_tilted_sxy(int G, int CPL, int variant);
+EvalLaunch eval_launcher_tilted(int G);
+EvalLaunch eval_launcher_tilted_sxy(int G);
 
 }  // namespace pb200

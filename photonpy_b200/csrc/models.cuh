@@ -8,6 +8,8 @@
 //   Gauss2D XYIBgSigmaXY         Estimators/Gaussian/GaussianPSFModels.h:391-471
 //   Gauss2D XYZIBg (astigmatic)  Estimators/Gaussian/GaussianPSFModels.h:636-751
 //   CSpline XYZIBg (flat bg)     Estimators/CSpline/CubicSplinePSFModels.h:14-154
+//   Gauss2D XYITiltedBg          Estimators/Gaussian/GaussianPSFModels.h:228-304
+//   Gauss2D XYITiltedBgSigmaXY   Estimators/Gaussian/GaussianPSFModels.h:474-558
 //
 // B200 layout: the reference recomputes erf/exp for every pixel although they depend
 // only on the column (x) or the row (y). Here a group of lanes first builds a small
@@ -29,7 +31,9 @@ enum ModelId : int {
     MODEL_XYIBG_SIGMAXY = 3,
     MODEL_XYZIBG = 4,
     MODEL_CSPLINE = 5,
-    MODEL_COUNT = 6
+    MODEL_XYITILTEDBG = 6,
+    MODEL_XYITILTEDBG_SIGMAXY = 7,
+    MODEL_COUNT = 8
 };
 
 // Plain-old-data description of one estimator instance, passed by value to kernels.
@@ -46,9 +50,14 @@ struct ModelDesc {
 };
 
 __host__ __device__ constexpr int model_num_params(int m) {
-    return (m == MODEL_XYIBG || m == MODEL_XYIBG_CONSTSIGMA) ? 4 : (m == MODEL_XYIBG_SIGMAXY ? 6 : 5);
+    return (m == MODEL_XYIBG || m == MODEL_XYIBG_CONSTSIGMA)            ? 4
+           : (m == MODEL_XYIBG_SIGMAXY || m == MODEL_XYITILTEDBG)       ? 6
+           : (m == MODEL_XYITILTEDBG_SIGMAXY)                           ? 8
+                                                                        : 5;
 }
-__host__ __device__ constexpr int model_num_consts(int m) { return m == MODEL_XYIBG_CONSTSIGMA ? 2 : 0; }
+__host__ __device__ constexpr int model_num_consts(int m) {
+    return (m == MODEL_XYIBG_CONSTSIGMA || m == MODEL_XYITILTEDBG) ? 2 : 0;
+}
 
 // MATH_PI in the reference is the float literal 3.141592653589793f (MathUtils.h:95).
 #define PB_PI 3.141592653589793f
@@ -342,6 +351,124 @@ struct GaussModel {
             t[2] = 0.0f;
             t[3] = sum;
             t[4 % K] = 0.01f;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------------
+// Gaussian spot on a tilted background plane (generic table kernel only).
+//   XYITiltedBg          theta = (x, y, I, bg, bgx, bgy), sigma_x/sigma_y from the spot's two
+//                        constants; mu = ((bg + bgx (x - W/2)) + bgy (y - H/2)) + I DeltaX DeltaY
+//   XYITiltedBgSigmaXY   theta = (x, y, I, bg, bgx, bgy, sx, sy); the reference keeps the tilt
+//                        columns x - W/2, y - H/2 in the Jacobian but leaves the tilt out of mu
+//                        (GaussianPSFModels.h:542 vs 549), reproduced here
+// Table: x-terms [R] then y-terms [R] of float4 (Delta, I*Delta, I*dE, I*dDelta/dsigma).
+// ---------------------------------------------------------------------------------------
+template <int MID>
+struct TiltedGaussModel {
+    static constexpr int K = model_num_params(MID);
+    static constexpr int kId = MID;
+    static constexpr bool kFreeSigma = (MID == MODEL_XYITILTEDBG_SIGMAXY);
+    static __host__ __device__ constexpr int table_floats(int R) { return 8 * R; }
+
+    float tx, ty, tI, tbg, bgx, bgy;
+    float cx1, cx2, cy1, cy2, invSqrtPi, half;
+
+    __device__ __forceinline__ void begin(const ModelDesc& d, const float* th, const float* consts) {
+        tx = th[0];
+        ty = th[1];
+        tI = th[2];
+        tbg = th[3];
+        bgx = th[4];
+        bgy = th[5];
+        const float sx = kFreeSigma ? th[6 % K] : consts[0];
+        const float sy = kFreeSigma ? th[7 % K] : consts[1];
+        const float s2pi = __fsqrt_rn(MUL(2.0f, PB_PI)), s2 = __fsqrt_rn(2.0f);
+        invSqrtPi = DIV(1.0f, __fsqrt_rn(PB_PI));
+        cx2 = DIV(1.0f, MUL(s2pi, sx));
+        cy2 = DIV(1.0f, MUL(s2pi, sy));
+        cx1 = DIV(1.0f, MUL(s2, sx));
+        cy1 = DIV(1.0f, MUL(s2, sy));
+        half = MUL((float)d.roisize, 0.5f);
+    }
+
+    __device__ __forceinline__ void term(int c, float t, float c1, float c2, float4* out) const {
+        const float d0 = SUB((float)c, t);
+        const float e0 = MUL(ADD(d0, 0.5f), c1);
+        const float e1 = MUL(SUB(d0, 0.5f), c1);
+        const float delta = SUB(MUL(0.5f, erff(e0)), MUL(0.5f, erff(e1)));
+        const float ex1 = expf(MUL(-e1, e1));
+        const float ex0 = expf(MUL(-e0, e0));
+        float4 r;
+        r.x = delta;
+        r.y = MUL(tI, delta);
+        r.z = MUL(tI, MUL(c2, SUB(ex1, ex0)));
+        r.w = kFreeSigma ? MUL(tI, MUL(SUB(MUL(ex1, e1), MUL(ex0, e0)), invSqrtPi)) : 0.0f;
+        *out = r;
+    }
+
+    __device__ __forceinline__ void build_table(const ModelDesc& d, float* tab, int lane, int G) const {
+        const int R = d.roisize;
+        float4* t4 = reinterpret_cast<float4*>(tab);
+        for (int i = lane; i < 2 * R; i += G) {
+            if (i < R) term(i, tx, cx1, cx2, &t4[i]);
+            else term(i - R, ty, cy1, cy2, &t4[i]);
+        }
+    }
+
+    __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
+                                          float (&J)[K]) const {
+        const float4 X = reinterpret_cast<const float4*>(tab)[x];
+        const float4 Y = reinterpret_cast<const float4*>(tab)[d.roisize + y];
+        const float px = SUB((float)x, half), py = SUB((float)y, half);
+        if (kFreeSigma) mu = ADD(tbg, MUL(X.y, Y.x));
+        else mu = ADD(ADD(ADD(tbg, MUL(bgx, px)), MUL(bgy, py)), MUL(X.y, Y.x));
+        J[0] = MUL(X.z, Y.x);  // (I dEx) DeltaY
+        J[1] = MUL(Y.z, X.x);  // (I dEy) DeltaX
+        J[2] = MUL(X.x, Y.x);
+        J[3] = 1.0f;
+        J[4] = px;
+        J[5] = py;
+        if (kFreeSigma) {
+            J[6 % K] = MUL(X.w, Y.x);
+            J[7 % K] = MUL(Y.w, X.x);
+        }
+    }
+
+    // CheckLimits (GaussianPSFModels.h:251-258, 495-505)
+    __device__ __forceinline__ static void check_limits(const ModelDesc& d, float (&t)[K]) {
+        const int R = d.roisize;
+        const float hi = gauss_xy_max(R);
+        t[0] = pb_clamp(t[0], 1.5f, hi);
+        t[1] = pb_clamp(t[1], 1.5f, hi);
+        if (t[2] < (kFreeSigma ? 10.0f : 25.0f)) t[2] = kFreeSigma ? 10.0f : 25.0f;
+        if (t[3] < 0.0f) t[3] = 0.0f;
+        if (kFreeSigma) {
+            const float smax = MUL((float)R, 0.5f);
+            t[6 % K] = pb_clamp(t[6 % K], 1.0f, smax);
+            t[7 % K] = pb_clamp(t[7 % K], 1.0f, smax);
+        }
+    }
+
+    // StopLimit (GaussianPSFModels.h:242-246, 486-490)
+    __device__ __forceinline__ static float stop_limit(int k) {
+        if (k == 2) return 1e-1f;
+        if (kFreeSigma && k >= 3 && k <= 5) return 1e-4f;
+        return 1e-5f;
+    }
+
+    // Initial value (GaussianPSFModels.h:299-303, 553-557)
+    __device__ __forceinline__ static void initial(const ModelDesc& d, float comx, float comy, float sum,
+                                                   float (&t)[K]) {
+        t[0] = comx;
+        t[1] = comy;
+        t[2] = kFreeSigma ? sum : MUL(sum, 0.7f);
+        t[3] = 0.0f;
+        t[4] = 0.0f;
+        t[5] = 0.0f;
+        if (kFreeSigma) {
+            t[6 % K] = d.sigma[0];
+            t[7 % K] = d.sigma[1];
         }
     }
 };

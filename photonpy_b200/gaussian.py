@@ -88,6 +88,13 @@ class GaussianPSFMethods:
         self._Gauss2D_CreatePSF_XYZIBgB.argtypes = [ctypes.c_int32, ctypes.POINTER(Gauss3D_CalibrationB),
                                                     ctypes.c_int32, vp]
         self._Gauss2D_CreatePSF_XYZIBgB.restype = vp
+        self._Gauss2D_CreatePSF_XYITiltedBg = smlmlib.Gauss2D_CreatePSF_XYITiltedBg
+        self._Gauss2D_CreatePSF_XYITiltedBg.argtypes = [ctypes.c_int32, ctypes.c_int32, vp]
+        self._Gauss2D_CreatePSF_XYITiltedBg.restype = vp
+        self._Gauss2D_CreatePSF_XYITiltedBgSigmaXY = smlmlib.Gauss2D_CreatePSF_XYITiltedBgSigmaXY
+        self._Gauss2D_CreatePSF_XYITiltedBgSigmaXY.argtypes = [ctypes.c_int32, ctypes.c_float, ctypes.c_float,
+                                                               ctypes.c_int32, vp]
+        self._Gauss2D_CreatePSF_XYITiltedBgSigmaXY.restype = vp
 
     def CreatePSF_XYIBg(self, roisize, sigma, cuda=True) -> Estimator:
         """[x,y,I,bg] (px, px, photons, photons/px). sigma: scalar or (sx, sy); None passes
@@ -112,6 +119,21 @@ class GaussianPSFMethods:
         if np.isscalar(initialSigma):
             initialSigma = [initialSigma, initialSigma]
         inst = self._Gauss2D_CreatePSF_XYIBgSigmaXY(roisize, initialSigma[0], initialSigma[1], cuda, self.ctx.inst)
+        return Estimator(self.ctx, inst, initialSigma)
+
+    def CreatePSF_XYITiltedBg(self, roisize, cuda=True) -> Estimator:
+        """[x,y,I,bg,bgx,bgy] (photonpy/cpp/gaussian.py:193-200): mu = bg + bgx (x - R/2) +
+        bgy (y - R/2) + I Gaussian(x, y); sigma_x/sigma_y per spot as 2 constants."""
+        inst = self._Gauss2D_CreatePSF_XYITiltedBg(roisize, cuda, self.ctx.inst)
+        return Estimator(self.ctx, inst)
+
+    def CreatePSF_XYITiltedBgSigmaXY(self, roisize, initialSigma, cuda=True) -> Estimator:
+        """[x,y,I,bg,bgx,bgy,sigmaX,sigmaY] (photonpy/cpp/gaussian.py:223-232). As in photonpy,
+        the tilt enters the Jacobian but not the expected value."""
+        if np.isscalar(initialSigma):
+            initialSigma = [initialSigma, initialSigma]
+        inst = self._Gauss2D_CreatePSF_XYITiltedBgSigmaXY(roisize, initialSigma[0], initialSigma[1], cuda,
+                                                          self.ctx.inst)
         return Estimator(self.ctx, inst, initialSigma)
 
     def CreatePSF_XYZIBg(self, roisize, calib, cuda=True) -> Estimator:

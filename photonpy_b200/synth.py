@@ -16,6 +16,9 @@ Workloads (distributions as stated in each generator):
                    (z in micrometres), z~U[-0.38,0.38] um
   * ``mixed``      sizes {7,9,11,16} p={.2,.3,.3,.2}; 50% XYIBg, 30% SigmaXY, 20% astig;
                    x,y re-centred at (R-1)/2 +- 1 px
+  * ``tilted``     11x11 tilted background bg + bgx (x - R/2) + bgy (y - R/2), bgx,bgy~U[-0.15,0.15],
+                   per-spot sigma constants~U[1.2,1.8] (XYITiltedBg), or free sigma_x/sigma_y
+                   ~U[1.2,2.0] (XYITiltedBgSigmaXY, initial sigma 1.6)
 """
 from __future__ import annotations
 
@@ -147,6 +150,36 @@ def constsigma(n, seed=11, R=9, sig=(1.2, 1.8)):
     consts = np.stack([sx, sy], 1).astype(np.float32)
     smp = _poisson(rng, gauss2d_ev(R, x, y, I, bg, sx, sy))
     return dict(kind="XYIBgConstSigma", R=R, samples=smp, truth=truth, constants=consts)
+
+
+def tilted(n, seed=13, R=11, free_sigma=False, init_sigma=1.6):
+    """Tilted-background Gaussian spots (GaussianPSFModels.h:228-304, 474-558). Truth rows are
+    (x, y, I, bg, bgx, bgy) for the per-spot-sigma model, (x, y, I, bg, bgx, bgy, sx, sy) for
+    the free-sigma one; the expectation always includes the tilt."""
+    rng = np.random.default_rng(seed)
+    c = (R - 1) / 2
+    x = rng.uniform(c - 1, c + 1, n)
+    y = rng.uniform(c - 1, c + 1, n)
+    I = rng.uniform(500, 5000, n)
+    bg = rng.uniform(2, 10, n)
+    bgx = rng.uniform(-0.15, 0.15, n)
+    bgy = rng.uniform(-0.15, 0.15, n)
+    if free_sigma:
+        sx = rng.uniform(1.2, 2.0, n)
+        sy = rng.uniform(1.2, 2.0, n)
+    else:
+        sx = rng.uniform(1.2, 1.8, n)
+        sy = rng.uniform(1.2, 1.8, n)
+    pix = np.arange(R, dtype=np.float64) - R * 0.5
+    ev = gauss2d_ev(R, x, y, I, bg, sx, sy) + bgx[:, None, None] * pix[None, None, :] + \
+        bgy[:, None, None] * pix[None, :, None]
+    smp = _poisson(rng, ev)
+    if free_sigma:
+        truth = np.stack([x, y, I, bg, bgx, bgy, sx, sy], 1).astype(np.float32)
+        return dict(kind="XYITiltedBgSigmaXY", R=R, sigma=(init_sigma, init_sigma), samples=smp, truth=truth)
+    truth = np.stack([x, y, I, bg, bgx, bgy], 1).astype(np.float32)
+    consts = np.stack([sx, sy], 1).astype(np.float32)
+    return dict(kind="XYITiltedBg", R=R, samples=smp, truth=truth, constants=consts)
 
 
 def sigma1(n, seed=12, R=11, init_sigma=1.5):

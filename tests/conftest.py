@@ -27,7 +27,8 @@ def load_golden(name):
     return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
 
 
-GOLDEN_SETS = ["xyibg_r10", "constsigma_r9", "sigma_r11", "sigmaxy_r16", "astig_r12", "spline_r13"]
+GOLDEN_SETS = ["xyibg_r10", "constsigma_r9", "sigma_r11", "sigmaxy_r16", "astig_r12", "spline_r13", "tiltedbg_r11",
+               "tiltedsxy_r11"]
 
 
 @pytest.fixture(scope="session")

@@ -44,9 +44,22 @@ def _fit_and_save(name, est, data, constants=None, extra=None):
     print(f"{name}: n={len(smp)} mean it={its.mean():.2f} capped={capped:.3f}")
 
 
-def main():
+def main(only=None):
+    """Writes every golden set, or only those named in `only`."""
     if not ref_lib.available():
         raise SystemExit("build the reference first: oracle/build_ref.sh")
+    want = (lambda name: only is None or name in only)
+    if want("tiltedbg_r11"):
+        d = synth.tilted(300, seed=113)
+        e = ref_lib.RefEstimator("XYITiltedBg", d["R"])
+        _fit_and_save("tiltedbg_r11", e, d, constants=d["constants"])
+    if want("tiltedsxy_r11"):
+        d = synth.tilted(300, seed=114, free_sigma=True)
+        e = ref_lib.RefEstimator("XYITiltedBgSigmaXY", d["R"], sigma=d["sigma"])
+        _fit_and_save("tiltedsxy_r11", e, d, extra=dict(sigma=np.float32(d["sigma"])))
+    if only is not None and not ({"xyibg_r10", "constsigma_r9", "sigma_r11", "sigmaxy_r16", "astig_r12",
+                                  "spline_r13"} & set(only)):
+        return
 
     d = synth.xyibg(400, seed=101)
     e = ref_lib.RefEstimator("XYIBg", d["R"], sigma=d["sigma"])
@@ -85,4 +98,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -21,6 +21,10 @@ def oracle_model(name, g):
     if name.startswith("spline"):
         coefs = O.spline_compute(g["zstack"], border=1)
         return O.Model(O.CSPLINE, R, coefs=coefs, spline_zrange=tuple(g["spline_zrange"]))
+    if name.startswith("tiltedbg"):
+        return O.Model(O.XYITILTEDBG, R)
+    if name.startswith("tiltedsxy"):
+        return O.Model(O.XYITILTEDBG_SIGMAXY, R, sigma=tuple(g["sigma"]))
     raise KeyError(name)
 
 
@@ -45,6 +49,10 @@ def cuda_estimator(name, g, ctx):
         est = sm.CreatePSF_XYZIBg(R, calib, sm.FlatBg, True)
         est._keep = calib
         return est
+    if name.startswith("tiltedbg"):
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYITiltedBg(R, True)
+    if name.startswith("tiltedsxy"):
+        return pb.GaussianPSFMethods(ctx).CreatePSF_XYITiltedBgSigmaXY(R, tuple(g["sigma"]), True)
     raise KeyError(name)
 
 

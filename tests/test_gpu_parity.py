@@ -24,6 +24,9 @@ FLOORS = {
     "sigmaxy_r16": dict(it_match=0.75, pos_ok_converged=0.95, phot_ok_converged=0.85),
     "astig_r12": dict(it_match=0.40, pos_ok_converged=0.97, phot_ok_converged=0.85),
     "spline_r13": dict(it_match=0.40, pos_ok_converged=0.95, phot_ok_converged=0.85),
+    "tiltedbg_r11": dict(it_match=0.90, pos_ok_converged=0.99, phot_ok_converged=0.90),
+    # every spot runs to the iteration cap in the reference (its tilt columns move mu not at all)
+    "tiltedsxy_r11": dict(conv_flag_match=0.99, pos_ok=0.5),
 }
 
 
