@@ -48,8 +48,8 @@ def report(ctx):
         rows.append((name, st, crlb_ok, q(e_ref), q(e_cuda)))
         est.Destroy()
     out = ["| golden set | spots | ref capped | iteration match | converged flag match | converged: pos ok | "
-           "converged: I/bg ok | max pos diff (converged) | CRLB within 1e-4 | median pos err vs FP64: ref | "
-           "median pos err vs FP64: CUDA |",
+           "converged: I/bg ok | max pos diff (converged) | CRLB within 1e-4 | p90 pos err vs FP64: ref | "
+           "p90 pos err vs FP64: CUDA |",
            "|---|---|---|---|---|---|---|---|---|---|---|"]
     for name, st, cok, er, ec in rows:
         out.append(f"| {name} | {st['n']} | {100 * st['frac_capped_ref']:.1f}% | {100 * st['it_match']:.2f}% | "
