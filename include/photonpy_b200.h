@@ -95,6 +95,13 @@ Estimator* Gauss2D_CreatePSF_XYITiltedBg(int roisize, bool cuda, Context* ctx);
  * reference, the tilt is in the Jacobian but not in mu (GaussianPSFModels.h:542 vs 549). */
 Estimator* Gauss2D_CreatePSF_XYITiltedBgSigmaXY(int roisize, float initialSigmaX, float initialSigmaY, bool cuda,
                                                 Context* ctx);
+/* Estimators/Gaussian/GaussianPSF.cu:216-240: intensity and background of numspots ROIs
+ * imageData[n][imgw][imgw] with the spot at xy[n][2]: LM fit of mu = I*DeltaX*DeltaY + bg from
+ * (1, 0), lambda 1e-15, maxIterations iterations; IBg[n][2] = (I, bg), IBg_crlb[n][2] =
+ * sqrt(|diag(Fisher^-1)|) (nullable). Spot i's sigma is sigma[i] of the flat array, as in the
+ * reference (photonpy passes [n][2] floats). roipos is unused, as in the reference. */
+void Gauss2D_EstimateIntensityBg(const float* imageData, float* IBg, float* IBg_crlb, int numspots, const float* xy,
+                                 const int* roipos, const float* sigma, int imgw, int maxIterations, bool cuda);
 /* Extension (no reference counterpart): astigmatic model with the quartic B term. */
 Estimator* Gauss2D_CreatePSF_XYZIBgB(int roisize, const Gauss3D_CalibrationB* calib, bool cuda, Context* ctx);
 /* Estimators/CSpline/CubicSplinePSF.cu:55-107. Only mode 0 (flat background) is supported;
@@ -197,8 +204,6 @@ void FFT(const void* src, void* dst, int batchsize, int siglen, int forward);
 void FFT2(const void* src, void* dst, int batchsize, int sigw, int sigh, int forward);
 void DrawROIs(float* image, int width, int height, const float* rois, int numrois, int roisize, const int* roiposYX);
 void Gauss2D_Draw(double* image, int imgw, int imgh, float* spotList, int nspots, float addSigma);
-void Gauss2D_EstimateIntensityBg(const float* imageData, float* IBg, float* IBg_crlb, int numspots, const float* xy,
-                                 const int* roipos, const float* sigma, int imgw, int maxIterations, int cuda);
 
 /* ---- Extensions (no reference counterpart) ------------------------------------------ */
 /* Message of the last error on this thread ("" if none); cleared by PB200_ClearError. */

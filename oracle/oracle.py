@@ -24,9 +24,10 @@ BUILD_DIR = os.path.join(HERE, "_build")
 LIB_PATH = os.path.join(BUILD_DIR, "liboracle.so")
 SOURCES = [os.path.join(HERE, "psf_oracle.c"), os.path.join(HERE, "psf_oracle_impl.h")]
 
-XYIBG, XYIBG_CONSTSIGMA, XYIBG_SIGMA, XYIBG_SIGMAXY, XYZIBG, CSPLINE, XYITILTEDBG, XYITILTEDBG_SIGMAXY = range(8)
+XYIBG, XYIBG_CONSTSIGMA, XYIBG_SIGMA, XYIBG_SIGMAXY, XYZIBG, CSPLINE, XYITILTEDBG, XYITILTEDBG_SIGMAXY, \
+    INTENSITYBG = range(9)
 NUM_PARAMS = {XYIBG: 4, XYIBG_CONSTSIGMA: 4, XYIBG_SIGMA: 5, XYIBG_SIGMAXY: 6, XYZIBG: 5, CSPLINE: 5, XYITILTEDBG: 6,
-              XYITILTEDBG_SIGMAXY: 8}
+              XYITILTEDBG_SIGMAXY: 8, INTENSITYBG: 2}
 
 
 class PsoModel(ct.Structure):
@@ -106,7 +107,7 @@ class Model:
         self.model = model
         self.roisize = int(roisize)
         self.K = NUM_PARAMS[model]
-        self.numconst = 2 if model in (XYIBG_CONSTSIGMA, XYITILTEDBG) else 0
+        self.numconst = 2 if model in (XYIBG_CONSTSIGMA, XYITILTEDBG) else (3 if model == INTENSITYBG else 0)
         s = PsoModel()
         s.model = model
         s.roisize = self.roisize

@@ -30,7 +30,9 @@ enum {
     PSO_XYZIBG = 4,           /* Gauss2D_Model_XYZIBg (astig)   (GaussianPSFModels.h:636-751) */
     PSO_CSPLINE = 5,          /* CSpline_Model_XYZIBg           (CubicSplinePSFModels.h:14-154) */
     PSO_XYITILTEDBG = 6,      /* Gauss2D_Model_XYITiltedBg      (GaussianPSFModels.h:228-304) */
-    PSO_XYITILTEDBG_SIGMAXY = 7 /* Gauss2D_Model_XYITiltedBgSigmaXY (GaussianPSFModels.h:474-558) */
+    PSO_XYITILTEDBG_SIGMAXY = 7, /* Gauss2D_Model_XYITiltedBgSigmaXY (GaussianPSFModels.h:474-558) */
+    PSO_INTENSITYBG = 8       /* IntensityBgModel (GaussianPSFModels.h:562-615): theta = (I, bg),
+                                 constants = (x, y, sigma), mu = I * DeltaX DeltaY + bg */
 };
 
 typedef struct {
@@ -51,11 +53,16 @@ int pso_num_params(int model)
     case PSO_XYIBG: case PSO_XYIBG_CONSTSIGMA: return 4;
     case PSO_XYIBG_SIGMAXY: case PSO_XYITILTEDBG: return 6;
     case PSO_XYITILTEDBG_SIGMAXY: return 8;
+    case PSO_INTENSITYBG: return 2;
     default: return 5;
     }
 }
 
-int pso_num_constants(int model) { return (model == PSO_XYIBG_CONSTSIGMA || model == PSO_XYITILTEDBG) ? 2 : 0; }
+int pso_num_constants(int model)
+{
+    if (model == PSO_INTENSITYBG) return 3;
+    return (model == PSO_XYIBG_CONSTSIGMA || model == PSO_XYITILTEDBG) ? 2 : 0;
+}
 
 int pso_sizeof_model(void) { return (int)sizeof(pso_model_t); }
 

@@ -15,6 +15,8 @@
  *   Gaussian models           Estimators/Gaussian/GaussianPSFModels.h:35-471, 636-751
  *   Cubic spline model        Estimators/CSpline/CubicSplinePSFModels.h:14-154
  *   Tilted-background models  Estimators/Gaussian/GaussianPSFModels.h:228-304, 474-558
+ *   Intensity/background fit  Estimators/Gaussian/GaussianPSFModels.h:562-615 (IntensityBgModel),
+ *                             Estimators/Gaussian/GaussianPSF.cu:216-240, Estimation.h:318-333
  */
 
 #define FN(name) CAT(name, SUFFIX)
@@ -199,6 +201,28 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
         }
         break;
     }
+    case PSO_INTENSITYBG: {
+        /* psf = DeltaX DeltaY at the fixed position (constants x, y) and sigma (constant 2),
+         * precomputed once per spot in the reference (ComputeGaussianPSF); mu = I psf + bg */
+        const REAL cx = (REAL)1 / (SQRT((REAL)2) * (REAL)consts[2]);
+        const REAL tx = (REAL)consts[0], ty = (REAL)consts[1];
+        for (int y = 0; y < H; y++) {
+            REAL Yexp0 = ((REAL)y - ty + (REAL)0.5) * cx;
+            REAL Yexp1 = ((REAL)y - ty - (REAL)0.5) * cx;
+            REAL DeltaY = (REAL)0.5 * ERF(Yexp0) - (REAL)0.5 * ERF(Yexp1);
+            for (int x = 0; x < W; x++) {
+                REAL Xexp0 = ((REAL)x - tx + (REAL)0.5) * cx;
+                REAL Xexp1 = ((REAL)x - tx - (REAL)0.5) * cx;
+                REAL DeltaX = (REAL)0.5 * ERF(Xexp0) - (REAL)0.5 * ERF(Xexp1);
+                const REAL psf = DeltaX * DeltaY;
+                int p = y * W + x;
+                mu[p] = theta[0] * psf + theta[1];
+                jac[0 * npix + p] = psf;
+                jac[1 * npix + p] = 1;
+            }
+        }
+        break;
+    }
     case PSO_CSPLINE: {
         const int Nz = m->spline_shape[0], Ny = m->spline_shape[1], Nx = m->spline_shape[2];
         const float du_f = (m->spline_zmax - m->spline_zmin) / (float)Nz;
@@ -311,6 +335,10 @@ static void FN(check_limits)(const pso_model_t* m, REAL* t)
         t[6] = FN(o_clamp)(t[6], 1, (REAL)(R * 0.5f));
         t[7] = FN(o_clamp)(t[7], 1, (REAL)(R * 0.5f));
         break;
+    case PSO_INTENSITYBG:
+        if (t[0] < (REAL)1e-5f) t[0] = (REAL)1e-5f;
+        if (t[1] < (REAL)1e-8f) t[1] = (REAL)1e-8f;
+        break;
     case PSO_CSPLINE:
         t[0] = FN(o_clamp)(t[0], (REAL)1.5f, (REAL)((float)R - 1.0f - 1.5f));
         t[1] = FN(o_clamp)(t[1], (REAL)1.5f, (REAL)((float)R - 1.0f - 1.5f));
@@ -347,6 +375,8 @@ static void FN(initial_estimate)(const pso_model_t* m, const float* smp, REAL* t
         t[0] = comx; t[1] = comy; t[2] = 0; t[3] = sum; t[4] = 0; break;
     case PSO_XYITILTEDBG:
         t[0] = comx; t[1] = comy; t[2] = sum * (REAL)0.7f; t[3] = 0; t[4] = 0; t[5] = 0; break;
+    case PSO_INTENSITYBG:
+        t[0] = 1; t[1] = 0; break;  /* GaussianPSF.cu:226 starts every spot at (1, 0) */
     case PSO_XYITILTEDBG_SIGMAXY:
         t[0] = comx; t[1] = comy; t[2] = sum; t[3] = 0; t[4] = 0; t[5] = 0;
         t[6] = m->sigma[0]; t[7] = m->sigma[1]; break;
@@ -362,6 +392,7 @@ static const float* FN(stop_limits)(int model)
     static const float s5[] = {1e-4f, 1e-4f, 1e-7f, 1e-4f, 1e-4f};
     static const float t6[] = {1e-5f, 1e-5f, 1e-1f, 1e-5f, 1e-5f, 1e-5f};
     static const float t8[] = {1e-5f, 1e-5f, 1e-1f, 1e-4f, 1e-4f, 1e-4f, 1e-5f, 1e-5f};
+    static const float ib[] = {1e-2f, 1e-4f};
     switch (model) {
     case PSO_XYIBG: case PSO_XYIBG_CONSTSIGMA: return g4;
     case PSO_XYIBG_SIGMA: return g5;
@@ -369,6 +400,7 @@ static const float* FN(stop_limits)(int model)
     case PSO_XYZIBG: return a5;
     case PSO_XYITILTEDBG: return t6;
     case PSO_XYITILTEDBG_SIGMAXY: return t8;
+    case PSO_INTENSITYBG: return ib;
     default: return s5;
     }
 }
@@ -619,7 +651,11 @@ int FN(pso_crlb)(const pso_model_t* m, int n, const float* params, const float* 
             for (int q = 0; q < K * K; q++) fisher_out[(size_t)s * K * K + q] = (double)fi[q];
         int ok = FN(invert)(K, fi, inv);
         for (int k = 0; k < K; k++)
-            crlb[(size_t)s * K + k] = ok ? (float)SQRT(inv[k * (K + 1)]) : INFINITY;
+            /* ComputeCRLB (Estimation.h:318-333), used by the intensity/background fit, takes
+             * fabs of the diagonal; ComputeChiSquareAndCRLB does not */
+            crlb[(size_t)s * K + k] = ok ? (float)SQRT(m->model == PSO_INTENSITYBG ? FABS(inv[k * (K + 1)])
+                                                                                  : inv[k * (K + 1)])
+                                         : INFINITY;
         if (chisq) chisq[s] = (float)cs;
     }
     free(mu); free(jac);

@@ -70,6 +70,8 @@ def lib():
         L.Estimator_ComputeDerivatives.argtypes = [vp, ct.c_int, vp, vp, vp, vp, vp]
         L.Estimator_ComputeExpectedValue.argtypes = [vp, ct.c_int, vp, vp, vp, vp]
         L.CSpline_Compute.argtypes = [vp, vp, vp, ct.c_int]
+        L.Gauss2D_EstimateIntensityBg.argtypes = [vp, vp, vp, ct.c_int, vp, vp, vp, ct.c_int, ct.c_int, ct.c_bool]
+        L.Gauss2D_EstimateIntensityBg.restype = None
         if hasattr(L, "GLRT_CreatePSF"):
             L.GLRT_CreatePSF.argtypes = [vp, vp]
             L.GLRT_CreatePSF.restype = vp
@@ -273,6 +275,23 @@ class RefQueue:
         if self.inst:
             lib().EstimQueue_Delete(self.inst)
             self.inst = None
+
+
+def estimate_intensity_bg(images, xy, sigma, max_iterations=100):
+    """The reference's Gauss2D_EstimateIntensityBg (GaussianPSF.cu:216-240) on the CPU:
+    images [n][w][w], xy [n][2], sigma as passed by photonpy's EstimateIBg ([n][2] floats, of
+    which the reference reads the flat element i for spot i). Returns (IBg [n][2], crlb [n][2])."""
+    L = lib()
+    images = np.ascontiguousarray(images, dtype=np.float32)
+    n, w = images.shape[0], images.shape[1]
+    xy = np.ascontiguousarray(xy, dtype=np.float32)
+    sigma = np.ascontiguousarray(sigma, dtype=np.float32)
+    roipos = np.zeros((n, 2), np.int32)
+    ibg = np.zeros((n, 2), np.float32)
+    crlb = np.zeros((n, 2), np.float32)
+    L.Gauss2D_EstimateIntensityBg(_p(images), _p(ibg), _p(crlb), n, _p(xy), _p(roipos), _p(sigma), w,
+                                  int(max_iterations), False)
+    return ibg, crlb
 
 
 def spline_compute(data, border=0):

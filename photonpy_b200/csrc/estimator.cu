@@ -124,6 +124,7 @@ FitLaunch fit_launcher_for(int model, int G, int CPL, int variant) {
     case MODEL_CSPLINE: return fit_launcher_spline(G, CPL, variant);
     case MODEL_XYITILTEDBG: return fit_launcher_tilted(G, CPL, variant);
     case MODEL_XYITILTEDBG_SIGMAXY: return fit_launcher_tilted_sxy(G, CPL, variant);
+    case MODEL_INTENSITYBG: return fit_launcher_intensity_bg(G);
     }
     throw Error("unknown model");
 }
@@ -220,6 +221,7 @@ struct Estimator {
     bool glrt = false;
     bool glrtRefMean = false;  // every spot's mean from the call's first ROI, as the reference
     DevBuf glrtRoi0;
+    bool crlbAbs = false;  // CRLB = sqrt(|diag of the inverse|) (the intensity/background fit)
     std::mutex mtx;
     Slot slots[2];
 
@@ -414,7 +416,7 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
             a.glrtMeanRoi = e->glrtRefMean ? e->glrtRoi0.as<float>() : nullptr;
         }
         fl(e->desc, a, e->threads, s.stream);
-        if (h_crlb) launch_crlb(K, a.fisher, a.crlb, a.chisq, count, s.stream);
+        if (h_crlb) launch_crlb(K, a.fisher, a.crlb, a.chisq, count, s.stream, e->crlbAbs);
         pend.push_back({c & 1, start, count});
         if (pend.size() == 2) {
             d2h(pend.front());
@@ -670,7 +672,7 @@ void run_fit_device(Estimator* e, FitArgs a, cudaStream_t s) {
         a.fisher = static_cast<float*>(scratch);
         try {
             e->fit_launch()(e->desc, a, e->threads, s);
-            launch_crlb(e->K, a.fisher, a.crlb, a.chisq, a.n, s);
+            launch_crlb(e->K, a.fisher, a.crlb, a.chisq, a.n, s, e->crlbAbs);
         } catch (...) {
             cudaFreeAsync(scratch, s);
             throw;
@@ -1386,9 +1388,37 @@ void FFT(const void*, void*, int, int, int) { not_provided("FFT"); }
 void FFT2(const void*, void*, int, int, int, int) { not_provided("FFT2"); }
 void DrawROIs(float*, int, int, const float*, int, int, const int*) { not_provided("DrawROIs"); }
 void Gauss2D_Draw(double*, int, int, float*, int, float) { not_provided("Gauss2D_Draw"); }
-void Gauss2D_EstimateIntensityBg(const float*, float*, float*, int, const float*, const int*, const float*, int, int,
-                                 int) {
-    not_provided("Gauss2D_EstimateIntensityBg");
+// GaussianPSF.cu:216-240: intensity and background of each spot at a known position xy[i]
+// and width, by the LM fit of mu = I * DeltaX DeltaY + bg from (1, 0) with lambda 1e-15 and
+// maxIterations iterations, and their CRLB (sqrt of the |diagonal| of the inverse Fisher
+// matrix, inverted here in FP64). As in the reference, spot i's sigma is sigma[i] of the flat array
+// (photonpy passes [n][2] floats, so spot i gets element i of that array), and roipos is
+// unused. One fused fit + CRLB launch on the current device.
+void Gauss2D_EstimateIntensityBg(const float* imageData, float* IBg, float* IBg_crlb, int numspots, const float* xy,
+                                 const int* roipos, const float* sigma, int imgw, int maxIterations, bool cuda) {
+    (void)roipos;
+    (void)cuda;
+    if (numspots <= 0) return;
+    guarded_void([&]() {
+        if (!imageData || !IBg || !xy || !sigma) throw Error("Gauss2D_EstimateIntensityBg: null argument");
+        if (imgw < 3 || imgw > 64) throw Error("Gauss2D_EstimateIntensityBg: imgw must be in [3, 64]");
+        Estimator e;
+        e.desc.model = MODEL_INTENSITYBG;
+        e.desc.roisize = imgw;
+        e.K = 2;
+        e.numconst = 3;
+        e.lm = LMParams{maxIterations, 1e-15f, 0.0f};  // LevMarOptimize's default step (Estimation.h:196)
+        e.crlbAbs = true;
+        std::vector<float> consts((size_t)3 * numspots), init((size_t)2 * numspots);
+        for (int i = 0; i < numspots; i++) {
+            consts[3 * (size_t)i] = xy[2 * (size_t)i];
+            consts[3 * (size_t)i + 1] = xy[2 * (size_t)i + 1];
+            consts[3 * (size_t)i + 2] = sigma[i];
+            init[2 * (size_t)i] = 1.0f;
+            init[2 * (size_t)i + 1] = 0.0f;
+        }
+        host_fit(&e, numspots, imageData, consts.data(), init.data(), IBg, nullptr, nullptr, 0, IBg_crlb, nullptr, 0);
+    });
 }
 Estimator* Gauss2D_CreatePSF_XYITiltedBg(int roisize, bool, Context* ctx) {
     return guarded([&]() -> Estimator* {

@@ -290,8 +290,9 @@ __device__ __forceinline__ void fisher_store(const float (&acc)[NACC], float* ro
 
 // One thread per ROI: FP64 LUP inverse of the packed Fisher matrix (reference algorithm and
 // 1e-9 tolerance, SolveMatrix.h:219-318, 344-392), CRLB = sqrt(diag) (+Inf when singular, as
-// Estimation.h:101 via InvertMatrix), chi-square copied out.
-template <int K>
+// Estimation.h:101 via InvertMatrix), chi-square copied out. ABS: sqrt(|diag|), as
+// ComputeCRLB (Estimation.h:318-333) does for the intensity/background fit.
+template <int K, bool ABS = false>
 __global__ void __launch_bounds__(128) crlb_kernel(const float* __restrict__ fisher, float* __restrict__ crlb,
                                                    float* __restrict__ chisq, int n) {
     constexpr int NA = K * (K + 1) / 2;
@@ -360,7 +361,7 @@ __global__ void __launch_bounds__(128) crlb_kernel(const float* __restrict__ fis
                 for (int k = i + 1; k < K; k++) v -= A[i][k] * x[k];
                 x[i] = v / A[i][i];
             }
-            out[j] = ok ? (float)sqrt(x[j]) : __int_as_float(0x7f800000);
+            out[j] = ok ? (float)sqrt(ABS ? fabs(x[j]) : x[j]) : __int_as_float(0x7f800000);
         }
         if (chisq) chisq[roi] = row[NA];
     }

@@ -1,5 +1,5 @@
-// Launchers of the tilted-background Gaussian models' kernels (generic table kernel; the
-// column-blocked kernel covers the flat-background Gaussians only).
+// Launchers of the tilted-background Gaussian models' kernels and of the intensity/background
+// fit (generic table kernel; the column-blocked kernel covers the flat-background Gaussians).
 #include "launch.cuh"
 
 namespace pb200 {
@@ -19,5 +19,7 @@ FitLaunch fit_launcher_tilted_sxy(int G, int CPL, int variant) {
 EvalLaunch eval_launcher_tilted(int G) { return eval_table<TiltedGaussModel<MODEL_XYITILTEDBG>>(G); }
 
 EvalLaunch eval_launcher_tilted_sxy(int G) { return eval_table<TiltedGaussModel<MODEL_XYITILTEDBG_SIGMAXY>>(G); }
+
+FitLaunch fit_launcher_intensity_bg(int G) { return generic_fit_table<IntensityBgModel>(G); }
 
 }  // namespace pb200

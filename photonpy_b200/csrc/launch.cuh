@@ -159,10 +159,18 @@ EvalLaunch eval_table(int G) {
 }
 
 // FP64 CRLB from the packed Fisher scratch rows (one thread per ROI).
-inline void launch_crlb(int K, const float* fisher, float* crlb, float* chisq, int n, cudaStream_t s) {
+inline void launch_crlb(int K, const float* fisher, float* crlb, float* chisq, int n, cudaStream_t s,
+                        bool absDiag = false) {
     if (n <= 0) return;
     const int threads = 128;
     const int grid = (n + threads - 1) / threads < 65535 * 4 ? (n + threads - 1) / threads : 65535 * 4;
+    if (absDiag) {
+        if (K != 2) throw std::runtime_error("crlb: |diag| form is provided for 2 parameters only");
+        crlb_kernel<2, true><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n);
+        check_launch("crlb kernel launch");
+        count_launch();
+        return;
+    }
     switch (K) {
     case 4: crlb_kernel<4><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     case 5: crlb_kernel<5><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
@@ -200,6 +208,7 @@ PB_DECLARE_MODEL_LAUNCHERS(spline)
 #undef PB_DECLARE_MODEL_LAUNCHERS
 FitLaunch fit_launcher_tilted(int G, int CPL, int variant);
 FitLaunch fit_launcher_tilted_sxy(int G, int CPL, int variant);
+FitLaunch fit_launcher_intensity_bg(int G);
 EvalLaunch eval_launcher_tilted(int G);
 EvalLaunch eval_launcher_tilted_sxy(int G);
 

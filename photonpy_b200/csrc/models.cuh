@@ -10,6 +10,7 @@
 //   CSpline XYZIBg (flat bg)     Estimators/CSpline/CubicSplinePSFModels.h:14-154
 //   Gauss2D XYITiltedBg          Estimators/Gaussian/GaussianPSFModels.h:228-304
 //   Gauss2D XYITiltedBgSigmaXY   Estimators/Gaussian/GaussianPSFModels.h:474-558
+//   IntensityBgModel             Estimators/Gaussian/GaussianPSFModels.h:562-615
 //
 // B200 layout: the reference recomputes erf/exp for every pixel although they depend
 // only on the column (x) or the row (y). Here a group of lanes first builds a small
@@ -33,7 +34,8 @@ enum ModelId : int {
     MODEL_CSPLINE = 5,
     MODEL_XYITILTEDBG = 6,
     MODEL_XYITILTEDBG_SIGMAXY = 7,
-    MODEL_COUNT = 8
+    MODEL_INTENSITYBG = 8,  // intensity and background at a known position and sigma
+    MODEL_COUNT = 9
 };
 
 // Plain-old-data description of one estimator instance, passed by value to kernels.
@@ -53,10 +55,11 @@ __host__ __device__ constexpr int model_num_params(int m) {
     return (m == MODEL_XYIBG || m == MODEL_XYIBG_CONSTSIGMA)            ? 4
            : (m == MODEL_XYIBG_SIGMAXY || m == MODEL_XYITILTEDBG)       ? 6
            : (m == MODEL_XYITILTEDBG_SIGMAXY)                           ? 8
+           : (m == MODEL_INTENSITYBG)                                   ? 2
                                                                         : 5;
 }
 __host__ __device__ constexpr int model_num_consts(int m) {
-    return (m == MODEL_XYIBG_CONSTSIGMA || m == MODEL_XYITILTEDBG) ? 2 : 0;
+    return (m == MODEL_XYIBG_CONSTSIGMA || m == MODEL_XYITILTEDBG) ? 2 : (m == MODEL_INTENSITYBG ? 3 : 0);
 }
 
 // MATH_PI in the reference is the float literal 3.141592653589793f (MathUtils.h:95).
@@ -470,6 +473,59 @@ struct TiltedGaussModel {
             t[6 % K] = d.sigma[0];
             t[7 % K] = d.sigma[1];
         }
+    }
+};
+
+// ---------------------------------------------------------------------------------------
+// Intensity and background of a spot at a known position and width (the model behind
+// Gauss2D_EstimateIntensityBg, GaussianPSF.cu:216-240): theta = (I, bg), constants =
+// (x, y, sigma), mu = I * DeltaX DeltaY + bg. Table: DeltaX [R] then DeltaY [R].
+// ---------------------------------------------------------------------------------------
+struct IntensityBgModel {
+    static constexpr int K = 2;
+    static constexpr int kId = MODEL_INTENSITYBG;
+    static __host__ __device__ constexpr int table_floats(int R) { return 2 * R; }
+
+    float tI, tbg, tx, ty, c1;
+
+    __device__ __forceinline__ void begin(const ModelDesc&, const float* th, const float* consts) {
+        tI = th[0];
+        tbg = th[1];
+        tx = consts[0];
+        ty = consts[1];
+        c1 = DIV(1.0f, MUL(__fsqrt_rn(2.0f), consts[2]));
+    }
+
+    __device__ __forceinline__ void build_table(const ModelDesc& d, float* tab, int lane, int G) const {
+        const int R = d.roisize;
+        for (int i = lane; i < 2 * R; i += G) {
+            const bool isx = i < R;
+            const float d0 = SUB((float)(isx ? i : i - R), isx ? tx : ty);
+            const float e0 = MUL(ADD(d0, 0.5f), c1);
+            const float e1 = MUL(SUB(d0, 0.5f), c1);
+            tab[i] = SUB(MUL(0.5f, erff(e0)), MUL(0.5f, erff(e1)));
+        }
+    }
+
+    __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
+                                          float (&J)[K]) const {
+        const float psf = MUL(tab[x], tab[d.roisize + y]);  // DeltaX * DeltaY
+        mu = ADD(MUL(tI, psf), tbg);
+        J[0] = psf;
+        J[1] = 1.0f;
+    }
+
+    // CheckLimits / StopLimit (GaussianPSFModels.h:587-599)
+    __device__ __forceinline__ static void check_limits(const ModelDesc&, float (&t)[K]) {
+        if (t[0] < 1e-5f) t[0] = 1e-5f;
+        if (t[1] < 1e-8f) t[1] = 1e-8f;
+    }
+    __device__ __forceinline__ static float stop_limit(int k) { return k == 0 ? 1e-2f : 1e-4f; }
+
+    // Every spot starts at (I, bg) = (1, 0) (GaussianPSF.cu:226).
+    __device__ __forceinline__ static void initial(const ModelDesc&, float, float, float, float (&t)[K]) {
+        t[0] = 1.0f;
+        t[1] = 0.0f;
     }
 };
 

@@ -8,6 +8,10 @@ import numpy as np
 
 from .context import Context
 from .estimator import Estimator
+from .lib import check_error
+
+_F32 = np.ctypeslib.ndpointer(np.float32, flags="aligned, c_contiguous")
+_I32 = np.ctypeslib.ndpointer(np.int32, flags="aligned, c_contiguous")
 
 
 class Gauss3D_Calibration(ctypes.Structure):
@@ -88,6 +92,10 @@ class GaussianPSFMethods:
         self._Gauss2D_CreatePSF_XYZIBgB.argtypes = [ctypes.c_int32, ctypes.POINTER(Gauss3D_CalibrationB),
                                                     ctypes.c_int32, vp]
         self._Gauss2D_CreatePSF_XYZIBgB.restype = vp
+        self._EstimateIBg = smlmlib.Gauss2D_EstimateIntensityBg
+        self._EstimateIBg.argtypes = [_F32, _F32, _F32, ctypes.c_int32, _F32, _I32, _F32, ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.c_int32]
+        self._EstimateIBg.restype = None
         self._Gauss2D_CreatePSF_XYITiltedBg = smlmlib.Gauss2D_CreatePSF_XYITiltedBg
         self._Gauss2D_CreatePSF_XYITiltedBg.argtypes = [ctypes.c_int32, ctypes.c_int32, vp]
         self._Gauss2D_CreatePSF_XYITiltedBg.restype = vp
@@ -120,6 +128,29 @@ class GaussianPSFMethods:
             initialSigma = [initialSigma, initialSigma]
         inst = self._Gauss2D_CreatePSF_XYIBgSigmaXY(roisize, initialSigma[0], initialSigma[1], cuda, self.ctx.inst)
         return Estimator(self.ctx, inst, initialSigma)
+
+    def EstimateIBg(self, images, sigma, xy, roipos=None, useCuda=False):
+        """Intensity and background of each ROI with the spot at a known position xy [n, 2] and
+        width sigma (photonpy/cpp/gaussian.py:153-172): returns (IBg [n, 2], crlb [n, 2]).
+        100 LM iterations from (I, bg) = (1, 0). Runs on the GPU whatever useCuda says."""
+        images = np.ascontiguousarray(images, dtype=np.float32)
+        xy = np.ascontiguousarray(xy, dtype=np.float32)
+        assert len(images.shape) == 3
+        numspots = len(images)
+        assert np.array_equal(xy.shape, (numspots, 2))
+        imgw = images.shape[1]
+        result = np.zeros((numspots, 2), dtype=np.float32)
+        crlb = np.zeros((numspots, 2), dtype=np.float32)
+        sigma_ = np.zeros((numspots, 2), dtype=np.float32)
+        sigma_[:] = sigma
+        if roipos is None:
+            roipos = np.zeros((numspots, 2))
+        assert np.array_equal(roipos.shape, (numspots, 2))
+        roipos = np.ascontiguousarray(roipos, dtype=np.int32)
+        if numspots > 0:
+            self._EstimateIBg(images, result, crlb, numspots, xy, roipos, sigma_, imgw, 100, useCuda)
+            check_error("EstimateIBg")
+        return result, crlb
 
     def CreatePSF_XYITiltedBg(self, roisize, cuda=True) -> Estimator:
         """[x,y,I,bg,bgx,bgy] (photonpy/cpp/gaussian.py:193-200): mu = bg + bgx (x - R/2) +

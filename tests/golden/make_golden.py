@@ -57,6 +57,18 @@ def main(only=None):
         d = synth.tilted(300, seed=114, free_sigma=True)
         e = ref_lib.RefEstimator("XYITiltedBgSigmaXY", d["R"], sigma=d["sigma"])
         _fit_and_save("tiltedsxy_r11", e, d, extra=dict(sigma=np.float32(d["sigma"])))
+    if want("intensitybg_r9"):
+        # Gauss2D_EstimateIntensityBg: spots at known positions; sigma given per spot as [n][2]
+        # with distinct values, so the reference's flat indexing of it (GaussianPSF.cu:225) is pinned
+        d = synth.xyibg(300, seed=115, R=9, xy=(3.0, 5.0))
+        rng = np.random.default_rng(116)
+        sig = rng.uniform(1.3, 1.7, size=(300, 2)).astype(np.float32)
+        xy = d["truth"][:, :2] + rng.normal(0, 0.05, size=(300, 2)).astype(np.float32)
+        ibg, crlb = ref_lib.estimate_intensity_bg(d["samples"], xy, sig, 100)
+        np.savez_compressed(os.path.join(HERE, "intensitybg_r9.npz"), samples=d["samples"], truth=d["truth"],
+                            xy=xy.astype(np.float32), sigma=sig, ibg=ibg, ibg_crlb=crlb, max_iterations=np.int32(100),
+                            roisize=np.int32(9))
+        print(f"intensitybg_r9: n=300 I mean={ibg[:, 0].mean():.1f}")
     if only is not None and not ({"xyibg_r10", "constsigma_r9", "sigma_r11", "sigmaxy_r16", "astig_r12",
                                   "spline_r13"} & set(only)):
         return

@@ -123,3 +123,22 @@ def test_glrt_restatement_matches_float64_formula():
     # the reference's mean source: first ROI for every spot
     ref = m.glrt(p, d["samples"], mean_roi=d["samples"][0])
     assert np.all(ref[:, 2] == got[0, 2])
+
+
+def _intensity_bg_inputs(g):
+    n = len(g["samples"])
+    flat = g["sigma"].reshape(-1)  # the reference reads sigma[i] of the flat [n][2] array
+    consts = np.stack([g["xy"][:, 0], g["xy"][:, 1], flat[:n]], 1).astype(np.float32)
+    return consts, np.tile(np.float32([1.0, 0.0]), (n, 1))
+
+
+def test_oracle_intensity_bg_bit_exact():
+    """Gauss2D_EstimateIntensityBg (GaussianPSF.cu:216-240) restated: fit and CRLB equal the
+    reference's CPU output bit for bit, including its flat indexing of sigma."""
+    g = load_golden("intensitybg_r9")
+    consts, init = _intensity_bg_inputs(g)
+    m = O.Model(O.INTENSITYBG, int(g["roisize"]))
+    p, _ = m.fit(g["samples"], constants=consts, initial=init, iterations=int(g["max_iterations"]), lambda_=1e-15)
+    assert np.array_equal(p, g["ibg"])
+    crlb, _ = m.crlb(p, None, constants=consts)
+    assert np.array_equal(crlb, g["ibg_crlb"])
