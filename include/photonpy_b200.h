@@ -104,9 +104,10 @@ void Gauss2D_EstimateIntensityBg(const float* imageData, float* IBg, float* IBg_
                                  const int* roipos, const float* sigma, int imgw, int maxIterations, bool cuda);
 /* Extension (no reference counterpart): astigmatic model with the quartic B term. */
 Estimator* Gauss2D_CreatePSF_XYZIBgB(int roisize, const Gauss3D_CalibrationB* calib, bool cuda, Context* ctx);
-/* Estimators/CSpline/CubicSplinePSF.cu:55-107. Only mode 0 (flat background) is supported;
- * other modes report an error and return NULL. coefs (nullable) overrides calib->coefs. The
- * coefficients are copied to the device at creation. */
+/* Estimators/CSpline/CubicSplinePSF.cu:55-107. mode 0 flat background (x,y,z,I,bg), 1 tilted
+ * background (x,y,z,I,bg,bgx,bgy), 2 background image (x,y,z,I,bg with mu = I psf + bg * image;
+ * the image is the spot's roisize*roisize constants). coefs (nullable) overrides calib->coefs.
+ * The coefficients are copied to the device at creation. */
 Estimator* CSpline_CreatePSF(int roisize, const CSpline_Calibration* calib, const float* coefs, int mode, bool cuda,
                              Context* ctx);
 /* Estimators/CSpline/CubicSplinePSF.cu:135-146: z-stack file (header v1) -> coefficients (border 0). */

@@ -25,9 +25,9 @@ LIB_PATH = os.path.join(BUILD_DIR, "liboracle.so")
 SOURCES = [os.path.join(HERE, "psf_oracle.c"), os.path.join(HERE, "psf_oracle_impl.h")]
 
 XYIBG, XYIBG_CONSTSIGMA, XYIBG_SIGMA, XYIBG_SIGMAXY, XYZIBG, CSPLINE, XYITILTEDBG, XYITILTEDBG_SIGMAXY, \
-    INTENSITYBG = range(9)
+    INTENSITYBG, CSPLINE_TILTED, CSPLINE_BGIMAGE = range(11)
 NUM_PARAMS = {XYIBG: 4, XYIBG_CONSTSIGMA: 4, XYIBG_SIGMA: 5, XYIBG_SIGMAXY: 6, XYZIBG: 5, CSPLINE: 5, XYITILTEDBG: 6,
-              XYITILTEDBG_SIGMAXY: 8, INTENSITYBG: 2}
+              XYITILTEDBG_SIGMAXY: 8, INTENSITYBG: 2, CSPLINE_TILTED: 7, CSPLINE_BGIMAGE: 5}
 
 
 class PsoModel(ct.Structure):
@@ -108,6 +108,8 @@ class Model:
         self.roisize = int(roisize)
         self.K = NUM_PARAMS[model]
         self.numconst = 2 if model in (XYIBG_CONSTSIGMA, XYITILTEDBG) else (3 if model == INTENSITYBG else 0)
+        if model == CSPLINE_BGIMAGE:
+            self.numconst = self.roisize * self.roisize
         s = PsoModel()
         s.model = model
         s.roisize = self.roisize

@@ -31,8 +31,10 @@ enum {
     PSO_CSPLINE = 5,          /* CSpline_Model_XYZIBg           (CubicSplinePSFModels.h:14-154) */
     PSO_XYITILTEDBG = 6,      /* Gauss2D_Model_XYITiltedBg      (GaussianPSFModels.h:228-304) */
     PSO_XYITILTEDBG_SIGMAXY = 7, /* Gauss2D_Model_XYITiltedBgSigmaXY (GaussianPSFModels.h:474-558) */
-    PSO_INTENSITYBG = 8       /* IntensityBgModel (GaussianPSFModels.h:562-615): theta = (I, bg),
+    PSO_INTENSITYBG = 8,      /* IntensityBgModel (GaussianPSFModels.h:562-615): theta = (I, bg),
                                  constants = (x, y, sigma), mu = I * DeltaX DeltaY + bg */
+    PSO_CSPLINE_TILTED = 9,   /* CSpline_Model_XYZITiltedBg     (CubicSplinePSFModels.h:157-298) */
+    PSO_CSPLINE_BGIMAGE = 10  /* CSpline_Model_XYZIBgImage      (CubicSplinePSFModels.h:300-443) */
 };
 
 typedef struct {
@@ -54,6 +56,7 @@ int pso_num_params(int model)
     case PSO_XYIBG_SIGMAXY: case PSO_XYITILTEDBG: return 6;
     case PSO_XYITILTEDBG_SIGMAXY: return 8;
     case PSO_INTENSITYBG: return 2;
+    case PSO_CSPLINE_TILTED: return 7;
     default: return 5;
     }
 }
@@ -62,6 +65,13 @@ int pso_num_constants(int model)
 {
     if (model == PSO_INTENSITYBG) return 3;
     return (model == PSO_XYIBG_CONSTSIGMA || model == PSO_XYITILTEDBG) ? 2 : 0;
+}
+
+/* Constants per spot of a model instance: the background-image spline takes a whole image. */
+int pso_model_constants(const pso_model_t* m)
+{
+    if (m->model == PSO_CSPLINE_BGIMAGE) return m->roisize * m->roisize;
+    return pso_num_constants(m->model);
 }
 
 int pso_sizeof_model(void) { return (int)sizeof(pso_model_t); }
@@ -171,7 +181,7 @@ int pso_spline_compute(const int* shape, const float* data, float* coefs, int bo
 int pso_glrt_f32(const pso_model_t* m, int n, const float* params, const float* samples, const float* constants,
                  const float* mean_roi, float* out)
 {
-    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_num_constants(m->model);
+    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_model_constants(m);
     float* ev = (float*)malloc(sizeof(float) * npix);
     for (int s = 0; s < n; s++) {
         const float* smp = samples + (size_t)s * npix;

@@ -223,13 +223,27 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
         }
         break;
     }
-    case PSO_CSPLINE: {
+    case PSO_CSPLINE:
+    case PSO_CSPLINE_TILTED:
+    case PSO_CSPLINE_BGIMAGE: {
+        /* flat background (CubicSplinePSFModels.h:14-154), tilted background (:157-298:
+         * mu += bgx (x - W/2) + bgy (y - W/2)) and background image (:300-443: mu = I psf + bg *
+         * image, the image being the spot's constants, with its own centring of tx, ty) */
         const int Nz = m->spline_shape[0], Ny = m->spline_shape[1], Nx = m->spline_shape[2];
         const float du_f = (m->spline_zmax - m->spline_zmin) / (float)Nz;
         const REAL du = (REAL)du_f;
         REAL tx = theta[0], ty = theta[1], tz = theta[2], tI = theta[3], tbg = theta[4];
-        tx -= (REAL)(Nx * 0.5f);
-        ty -= (REAL)(Ny * 0.5f);
+        if (m->model == PSO_CSPLINE_BGIMAGE) {
+            const float wf = (float)W;
+            tx = tx - (REAL)(wf / 2.0f) + (REAL)((wf - (float)Nx + 1) / 2.0f);
+            ty = ty - (REAL)(wf / 2.0f) + (REAL)((wf - (float)Ny + 1) / 2.0f);
+            tx += (REAL)0.5f;
+            ty += (REAL)0.5f;
+        } else {
+            tx -= (REAL)(Nx * 0.5f);
+            ty -= (REAL)(Ny * 0.5f);
+        }
+        const REAL halfw = (REAL)((float)W * 0.5f);
         REAL df[64], dxf[64], dyf[64], dzf[64];
         for (int i = 0; i < 64; i++) df[i] = dxf[i] = dyf[i] = dzf[i] = 0;
         REAL spx = -tx; spx -= (REAL)(int)spx;
@@ -274,12 +288,20 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
                 dz *= tI / du;
                 if (psf < 0) psf = 0;
                 int p = y * W + x;
-                mu[p] = tI * psf + tbg;
+                if (m->model == PSO_CSPLINE_TILTED) {
+                    mu[p] = tI * psf + tbg + theta[5] * ((REAL)x - halfw) + theta[6] * ((REAL)y - halfw);
+                    jac[5 * npix + p] = (REAL)x - halfw;
+                    jac[6 * npix + p] = (REAL)y - halfw;
+                } else if (m->model == PSO_CSPLINE_BGIMAGE) {
+                    mu[p] = tI * psf + tbg * (REAL)consts[p];
+                } else {
+                    mu[p] = tI * psf + tbg;
+                }
                 jac[0 * npix + p] = dx;
                 jac[1 * npix + p] = dy;
                 jac[2 * npix + p] = dz;
                 jac[3 * npix + p] = psf;
-                jac[4 * npix + p] = 1;
+                jac[4 * npix + p] = m->model == PSO_CSPLINE_BGIMAGE ? (REAL)consts[p] : 1;
             }
         }
         break;
@@ -340,6 +362,8 @@ static void FN(check_limits)(const pso_model_t* m, REAL* t)
         if (t[1] < (REAL)1e-8f) t[1] = (REAL)1e-8f;
         break;
     case PSO_CSPLINE:
+    case PSO_CSPLINE_TILTED:
+    case PSO_CSPLINE_BGIMAGE:
         t[0] = FN(o_clamp)(t[0], (REAL)1.5f, (REAL)((float)R - 1.0f - 1.5f));
         t[1] = FN(o_clamp)(t[1], (REAL)1.5f, (REAL)((float)R - 1.0f - 1.5f));
         t[2] = FN(o_clamp)(t[2], (REAL)(m->spline_zmin + 1e-3f), (REAL)(m->spline_zmax - 1e-3f));
@@ -372,7 +396,10 @@ static void FN(initial_estimate)(const pso_model_t* m, const float* smp, REAL* t
     case PSO_XYZIBG:
         t[0] = comx; t[1] = comy; t[2] = 0; t[3] = sum; t[4] = (REAL)0.01f; break;
     case PSO_CSPLINE:
+    case PSO_CSPLINE_BGIMAGE:
         t[0] = comx; t[1] = comy; t[2] = 0; t[3] = sum; t[4] = 0; break;
+    case PSO_CSPLINE_TILTED:
+        t[0] = comx; t[1] = comy; t[2] = 0; t[3] = sum; t[4] = 0; t[5] = 0; t[6] = 0; break;
     case PSO_XYITILTEDBG:
         t[0] = comx; t[1] = comy; t[2] = sum * (REAL)0.7f; t[3] = 0; t[4] = 0; t[5] = 0; break;
     case PSO_INTENSITYBG:
@@ -393,6 +420,7 @@ static const float* FN(stop_limits)(int model)
     static const float t6[] = {1e-5f, 1e-5f, 1e-1f, 1e-5f, 1e-5f, 1e-5f};
     static const float t8[] = {1e-5f, 1e-5f, 1e-1f, 1e-4f, 1e-4f, 1e-4f, 1e-5f, 1e-5f};
     static const float ib[] = {1e-2f, 1e-4f};
+    static const float s7[] = {1e-4f, 1e-4f, 1e-7f, 1e-4f, 1e-4f, 1e-4f, 1e-4f};
     switch (model) {
     case PSO_XYIBG: case PSO_XYIBG_CONSTSIGMA: return g4;
     case PSO_XYIBG_SIGMA: return g5;
@@ -401,6 +429,7 @@ static const float* FN(stop_limits)(int model)
     case PSO_XYITILTEDBG: return t6;
     case PSO_XYITILTEDBG_SIGMAXY: return t8;
     case PSO_INTENSITYBG: return ib;
+    case PSO_CSPLINE_TILTED: return s7;
     default: return s5;
     }
 }
@@ -553,7 +582,7 @@ static void* FN(fit_worker)(void* arg)
 {
     FN(fit_job_t)* job = (FN(fit_job_t)*)arg;
     const pso_model_t* m = job->m;
-    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_num_constants(m->model);
+    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_model_constants(m);
     REAL* mu = (REAL*)malloc(sizeof(REAL) * npix);
     REAL* jac = (REAL*)malloc(sizeof(REAL) * npix * K);
     REAL* tr = job->traceBufLen > 0 ? (REAL*)malloc(sizeof(REAL) * K * job->traceBufLen) : NULL;
@@ -604,7 +633,7 @@ int FN(pso_fit)(const pso_model_t* m, int n, const float* samples, const float* 
 int FN(pso_derivatives)(const pso_model_t* m, int n, const float* params, const float* constants,
                         float* deriv, float* ev)
 {
-    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_num_constants(m->model);
+    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_model_constants(m);
     REAL* mu = (REAL*)malloc(sizeof(REAL) * npix);
     REAL* jac = (REAL*)malloc(sizeof(REAL) * npix * K);
     for (int s = 0; s < n; s++) {
@@ -626,7 +655,7 @@ int FN(pso_derivatives)(const pso_model_t* m, int n, const float* params, const 
 int FN(pso_crlb)(const pso_model_t* m, int n, const float* params, const float* samples,
                  const float* constants, float* crlb, float* chisq, double* fisher_out)
 {
-    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_num_constants(m->model);
+    const int K = pso_num_params(m->model), npix = m->roisize * m->roisize, nc = pso_model_constants(m);
     REAL* mu = (REAL*)malloc(sizeof(REAL) * npix);
     REAL* jac = (REAL*)malloc(sizeof(REAL) * npix * K);
     for (int s = 0; s < n; s++) {

@@ -99,7 +99,7 @@ class RefEstimator:
     """One reference estimator instance (host pointers; cuda selects the reference's GPU kernels)."""
 
     def __init__(self, kind: str, roisize: int, cuda: bool = False, sigma=(1.5, 1.5), astig=None, zrange=(-1, 1),
-                 coefs=None, spline_zrange=(0, 1)):
+                 coefs=None, spline_zrange=(0, 1), spline_mode=0):
         L = lib()
         self.ctx = L.Context_Create()
         self.roisize = roisize
@@ -128,7 +128,7 @@ class RefEstimator:
             c.shape[0], c.shape[1], c.shape[2] = self._coefs.shape[:3]
             c.z_min, c.z_max = spline_zrange
             c.coefs = self._coefs.ctypes.data
-            inst = L.CSpline_CreatePSF(roisize, ct.byref(c), None, 0, cuda, self.ctx)
+            inst = L.CSpline_CreatePSF(roisize, ct.byref(c), None, int(spline_mode), cuda, self.ctx)
         else:
             raise ValueError(kind)
         if not inst:

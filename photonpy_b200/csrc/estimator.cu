@@ -125,6 +125,8 @@ FitLaunch fit_launcher_for(int model, int G, int CPL, int variant) {
     case MODEL_XYITILTEDBG: return fit_launcher_tilted(G, CPL, variant);
     case MODEL_XYITILTEDBG_SIGMAXY: return fit_launcher_tilted_sxy(G, CPL, variant);
     case MODEL_INTENSITYBG: return fit_launcher_intensity_bg(G);
+    case MODEL_CSPLINE_TILTED: return fit_launcher_spline_tilted(G);
+    case MODEL_CSPLINE_BGIMAGE: return fit_launcher_spline_bgimage(G);
     }
     throw Error("unknown model");
 }
@@ -138,7 +140,10 @@ AdjointLaunch adjoint_launcher_for(int model) {
     case MODEL_XYZIBG: return adjoint_launcher_astig();
     case MODEL_CSPLINE: return adjoint_launcher_spline();
     case MODEL_XYITILTEDBG:
-    case MODEL_XYITILTEDBG_SIGMAXY: throw Error("PoissonNLLAdjoint: not provided for the tilted-background models");
+    case MODEL_XYITILTEDBG_SIGMAXY:
+    case MODEL_CSPLINE_TILTED:
+    case MODEL_CSPLINE_BGIMAGE:
+        throw Error("PoissonNLLAdjoint: provided for the flat-background models only");
     }
     throw Error("unknown model");
 }
@@ -153,6 +158,8 @@ EvalLaunch eval_launcher_for(int model, int G) {
     case MODEL_CSPLINE: return eval_launcher_spline(G);
     case MODEL_XYITILTEDBG: return eval_launcher_tilted(G);
     case MODEL_XYITILTEDBG_SIGMAXY: return eval_launcher_tilted_sxy(G);
+    case MODEL_CSPLINE_TILTED: return eval_launcher_spline_tilted(G);
+    case MODEL_CSPLINE_BGIMAGE: return eval_launcher_spline_bgimage(G);
     }
     throw Error("unknown model");
 }
@@ -163,7 +170,7 @@ namespace {
 // Lanes per ROI when no tuned value is set: enough ROIs per warp to amortise the redundant
 // K x K solve for small ROIs, enough lanes to keep per-lane pixel loops short for large ones.
 int default_lanes(int model, int R) {
-    if (model == MODEL_CSPLINE) return R * R <= 100 ? 8 : 16;
+    if (model_is_spline(model)) return R * R <= 100 ? 8 : 16;
     if (R <= 16) return 4;
     if (R <= 32) return 8;
     return 16;
@@ -608,14 +615,15 @@ __global__ void spline_evaluate_kernel(const float* __restrict__ coefs, int s0, 
 
 Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const float* h_coefs, int mode, Context* ctx,
                        const float* d_coefs_src) {
-    if (mode != 0) throw Error("CSpline_CreatePSF: only mode 0 (flat background) is provided by photonpy_b200");
+    // modes CSPLINE_FLATBG 0, CSPLINE_TILTEDBG 1, CSPLINE_BGIMAGE 2 (CubicSplinePSF.cu:76-101)
+    if (mode < 0 || mode > 2) throw Error("Invalid model background mode");
     if (roisize < 3 || roisize > 64) throw Error("roisize must be in [3, 64]");
     if (!calib) throw Error("CSpline_CreatePSF: calibration is null");
     const int nz = calib->shape[0], ny = calib->shape[1], nx = calib->shape[2];
     if (nz <= 0 || ny <= 0 || nx <= 0) throw Error("CSpline_CreatePSF: empty coefficient grid");
     auto* e = new Estimator();
     try {
-        e->desc.model = MODEL_CSPLINE;
+        e->desc.model = mode == 0 ? MODEL_CSPLINE : (mode == 1 ? MODEL_CSPLINE_TILTED : MODEL_CSPLINE_BGIMAGE);
         e->desc.roisize = roisize;
         e->desc.spline_shape[0] = nz;
         e->desc.spline_shape[1] = ny;
@@ -632,12 +640,16 @@ Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const floa
             PB_CUDA(cudaMemcpy(e->coefs.p, src, sizeof(float) * ncoef, cudaMemcpyHostToDevice));
         }
         e->desc.coefs = e->coefs.as<float>();
-        e->K = 5;
-        e->numconst = 0;
-        e->format = "x,y,z,I,bg";
+        e->K = model_num_params(e->desc.model);
+        e->numconst = mode == 2 ? roisize * roisize : 0;  // the background image of each spot
+        e->format = mode == 1 ? "x,y,z,I,bg,bgx,bgy" : "x,y,z,I,bg";
         const float border = 1.5f;
         const float xyhi = (float)(roisize - 1) - border;
         e->limits = {{border, xyhi}, {border, xyhi}, {calib->z_min, calib->z_max}, {10.0f, 1e9f}, {1e-6f, 1e9f}};
+        if (mode == 1) {  // CubicSplinePSF.cu:67-70
+            e->limits.push_back({-1e6f, 1e6f});
+            e->limits.push_back({-1e6f, 1e6f});
+        }
     } catch (...) {
         delete e;
         throw;
@@ -876,7 +888,7 @@ Estimator* GLRT_CreatePSF(Estimator* model, Context* ctx) {
             e->threads = model->threads;
             e->variant = model->variant;
             e->glrt = true;
-            if (model->desc.model == MODEL_CSPLINE) {
+            if (model_is_spline(model->desc.model)) {
                 const size_t ncoef = (size_t)model->desc.spline_shape[0] * model->desc.spline_shape[1] *
                                      model->desc.spline_shape[2] * 64;
                 e->coefs.ensure(sizeof(float) * ncoef);

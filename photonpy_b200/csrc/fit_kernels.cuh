@@ -24,10 +24,22 @@
 // FP64; the Fisher matrix is accumulated in FP32 and inverted in FP64 (LUP with partial
 // pivoting and the reference's 1e-9 tolerance, Estimation.h:63-102, SolveMatrix.h:411-452).
 #pragma once
+#include <type_traits>
+
 #include "fit_common.cuh"
 #include "models.cuh"
 
 namespace pb200 {
+
+// Models whose per-spot constants are a whole image (read per pixel, not held in registers).
+template <class M, class = void>
+struct pixel_consts_trait : std::false_type {};
+template <class M>
+struct pixel_consts_trait<M, std::void_t<decltype(M::kPixelConsts)>> : std::integral_constant<bool, M::kPixelConsts> {};
+template <class M>
+__host__ __device__ constexpr bool model_has_pixel_consts() {
+    return pixel_consts_trait<M>::value;
+}
 
 // Shared-memory scratch a group needs besides its pixels: the model table, or the FP64
 // Fisher/LM work area (2*K*K doubles + K doubles), whichever is larger.
@@ -132,6 +144,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
             // ---- per-iteration table, then the pixel pass ----
             M m;
             m.begin(d, th, cs);
+            if constexpr (model_has_pixel_consts<M>()) m.img = a.consts + (size_t)roi * npix;
             __syncwarp(mask);
             m.build_table(d, tab, lane, G);
             __syncwarp(mask);
@@ -277,6 +290,7 @@ __global__ void __launch_bounds__(256) eval_kernel(const ModelDesc d, const floa
         for (int c = 0; c < NC; c++) cs[c] = consts[(size_t)roi * NC + c];
         M m;
         m.begin(d, th, cs);
+        if constexpr (model_has_pixel_consts<M>()) m.img = consts + (size_t)roi * npix;
         __syncwarp(mask);
         m.build_table(d, tab, lane, G);
         __syncwarp(mask);

@@ -175,6 +175,7 @@ inline void launch_crlb(int K, const float* fisher, float* crlb, float* chisq, i
     case 4: crlb_kernel<4><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     case 5: crlb_kernel<5><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     case 6: crlb_kernel<6><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
+    case 7: crlb_kernel<7><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     case 8: crlb_kernel<8><<<grid, threads, 0, s>>>(fisher, crlb, chisq, n); break;
     default: throw std::runtime_error("crlb: unsupported number of parameters");
     }
@@ -209,6 +210,10 @@ PB_DECLARE_MODEL_LAUNCHERS(spline)
 FitLaunch fit_launcher_tilted(int G, int CPL, int variant);
 FitLaunch fit_launcher_tilted_sxy(int G, int CPL, int variant);
 FitLaunch fit_launcher_intensity_bg(int G);
+FitLaunch fit_launcher_spline_tilted(int G);
+FitLaunch fit_launcher_spline_bgimage(int G);
+EvalLaunch eval_launcher_spline_tilted(int G);
+EvalLaunch eval_launcher_spline_bgimage(int G);
 EvalLaunch eval_launcher_tilted(int G);
 EvalLaunch eval_launcher_tilted_sxy(int G);
 

@@ -8,6 +8,8 @@
 //   Gauss2D XYIBgSigmaXY         Estimators/Gaussian/GaussianPSFModels.h:391-471
 //   Gauss2D XYZIBg (astigmatic)  Estimators/Gaussian/GaussianPSFModels.h:636-751
 //   CSpline XYZIBg (flat bg)     Estimators/CSpline/CubicSplinePSFModels.h:14-154
+//   CSpline XYZITiltedBg         Estimators/CSpline/CubicSplinePSFModels.h:157-298
+//   CSpline XYZIBgImage          Estimators/CSpline/CubicSplinePSFModels.h:300-443
 //   Gauss2D XYITiltedBg          Estimators/Gaussian/GaussianPSFModels.h:228-304
 //   Gauss2D XYITiltedBgSigmaXY   Estimators/Gaussian/GaussianPSFModels.h:474-558
 //   IntensityBgModel             Estimators/Gaussian/GaussianPSFModels.h:562-615
@@ -35,8 +37,14 @@ enum ModelId : int {
     MODEL_XYITILTEDBG = 6,
     MODEL_XYITILTEDBG_SIGMAXY = 7,
     MODEL_INTENSITYBG = 8,  // intensity and background at a known position and sigma
-    MODEL_COUNT = 9
+    MODEL_CSPLINE_TILTED = 9,
+    MODEL_CSPLINE_BGIMAGE = 10,
+    MODEL_COUNT = 11
 };
+
+__host__ __device__ constexpr bool model_is_spline(int m) {
+    return m == MODEL_CSPLINE || m == MODEL_CSPLINE_TILTED || m == MODEL_CSPLINE_BGIMAGE;
+}
 
 // Plain-old-data description of one estimator instance, passed by value to kernels.
 struct ModelDesc {
@@ -56,6 +64,7 @@ __host__ __device__ constexpr int model_num_params(int m) {
            : (m == MODEL_XYIBG_SIGMAXY || m == MODEL_XYITILTEDBG)       ? 6
            : (m == MODEL_XYITILTEDBG_SIGMAXY)                           ? 8
            : (m == MODEL_INTENSITYBG)                                   ? 2
+           : (m == MODEL_CSPLINE_TILTED)                                ? 7
                                                                         : 5;
 }
 __host__ __device__ constexpr int model_num_consts(int m) {
@@ -530,15 +539,22 @@ struct IntensityBgModel {
 };
 
 // ---------------------------------------------------------------------------------------
-// Cubic spline (flat background): table = delta_f, delta_dxf, delta_dyf, delta_dzf [4][64].
+// Cubic spline: table = delta_f, delta_dxf, delta_dyf, delta_dzf [4][64]. MODE 0 flat
+// background, 1 tilted background (theta += bgx, bgy; mu += bgx (x - W/2) + bgy (y - W/2)),
+// 2 background image (mu = I psf + bg * image; the image is the spot's R*R constants, read
+// per pixel through `img`; this mode centres tx, ty differently, CubicSplinePSFModels.h:371-374).
 // ---------------------------------------------------------------------------------------
-struct SplineModel {
-    static constexpr int K = 5;
-    static constexpr int kId = MODEL_CSPLINE;
+template <int MODE>
+struct SplineModelT {
+    static constexpr int K = (MODE == 1) ? 7 : 5;
+    static constexpr int kId = (MODE == 0) ? MODEL_CSPLINE : (MODE == 1 ? MODEL_CSPLINE_TILTED : MODEL_CSPLINE_BGIMAGE);
+    static constexpr bool kPixelConsts = (MODE == 2);
     static __host__ __device__ constexpr int table_floats(int) { return 256; }
 
     float tx, ty, tI, tbg, du;
     float spx, spy, spz;
+    float bgx, bgy, halfw;
+    const float* img;  // MODE 2: this spot's background image [R][R]
     int k;  // z slice
     int Nx, Ny;
 
@@ -547,10 +563,20 @@ struct SplineModel {
         Ny = d.spline_shape[1];
         Nx = d.spline_shape[2];
         du = DIV(SUB(d.spline_zmax, d.spline_zmin), (float)Nz);
-        tx = SUB(th[0], MUL((float)Nx, 0.5f));
-        ty = SUB(th[1], MUL((float)Ny, 0.5f));
+        if (MODE == 2) {
+            const float w = (float)d.roisize;
+            tx = ADD(ADD(SUB(th[0], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Nx), 1.0f), 2.0f)), 0.5f);
+            ty = ADD(ADD(SUB(th[1], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Ny), 1.0f), 2.0f)), 0.5f);
+        } else {
+            tx = SUB(th[0], MUL((float)Nx, 0.5f));
+            ty = SUB(th[1], MUL((float)Ny, 0.5f));
+        }
         tI = th[3];
         tbg = th[4];
+        bgx = (MODE == 1) ? th[5 % K] : 0.0f;
+        bgy = (MODE == 1) ? th[6 % K] : 0.0f;
+        halfw = MUL((float)d.roisize, 0.5f);
+        img = nullptr;
         float sx = -tx;
         spx = SUB(sx, (float)(int)sx);
         float sy = -ty;
@@ -587,7 +613,7 @@ struct SplineModel {
     }
 
     __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
-                                          float (&J)[5]) const {
+                                          float (&J)[K]) const {
         const float yy = SUB((float)y, ty);
         const int j = max(0, min((int)yy, Ny - 1));
         const float xx = SUB((float)x, tx);
@@ -608,12 +634,24 @@ struct SplineModel {
         dy = MUL(dy, -tI);
         dz = MUL(dz, DIV(tI, du));
         if (psf < 0.0f) psf = 0.0f;
-        mu = ADD(MUL(tI, psf), tbg);
         J[0] = dx;
         J[1] = dy;
         J[2] = dz;
         J[3] = psf;
-        J[4] = 1.0f;
+        if (MODE == 1) {
+            const float px = SUB((float)x, halfw), py = SUB((float)y, halfw);
+            mu = ADD(ADD(ADD(MUL(tI, psf), tbg), MUL(bgx, px)), MUL(bgy, py));
+            J[4] = 1.0f;
+            J[5 % K] = px;
+            J[6 % K] = py;
+        } else if (MODE == 2) {
+            const float bg = __ldg(img + y * d.roisize + x);
+            mu = ADD(MUL(tI, psf), MUL(tbg, bg));
+            J[4] = bg;
+        } else {
+            mu = ADD(MUL(tI, psf), tbg);
+            J[4] = 1.0f;
+        }
     }
 
     // Offset of the 64 coefficients pixel (x, y) reads (same voxel choice as pixel()).
@@ -623,8 +661,8 @@ struct SplineModel {
         return 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i);
     }
 
-    // CheckLimits (CubicSplinePSFModels.h:44-50)
-    __device__ __forceinline__ static void check_limits(const ModelDesc& d, float (&t)[5]) {
+    // CheckLimits (CubicSplinePSFModels.h:44-50, 185-191, 330-336): bgx, bgy are not clamped
+    __device__ __forceinline__ static void check_limits(const ModelDesc& d, float (&t)[K]) {
         const float hi = SUB(SUB((float)d.roisize, 1.0f), 1.5f);
         t[0] = pb_clamp(t[0], 1.5f, hi);
         t[1] = pb_clamp(t[1], 1.5f, hi);
@@ -636,13 +674,18 @@ struct SplineModel {
     __device__ __forceinline__ static float stop_limit(int k) { return k == 2 ? 1e-7f : 1e-4f; }
 
     __device__ __forceinline__ static void initial(const ModelDesc&, float comx, float comy, float sum,
-                                                   float (&t)[5]) {
+                                                   float (&t)[K]) {
         t[0] = comx;
         t[1] = comy;
         t[2] = 0.0f;
         t[3] = sum;
         t[4] = 0.0f;
+        if (MODE == 1) {
+            t[5 % K] = 0.0f;
+            t[6 % K] = 0.0f;
+        }
     }
 };
+using SplineModel = SplineModelT<0>;
 
 }  // namespace pb200

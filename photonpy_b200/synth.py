@@ -263,6 +263,37 @@ def spline(n, seed=4, R=13, zr=(-0.38, 0.38), A=0.1, B=0.0):
     return dict(kind="CSpline", R=R, samples=smp, truth=truth)
 
 
+def spline_background(n, mode, seed=6, R=13, zr=(-0.38, 0.38), A=0.1):
+    """Spline-workload spots on a tilted background (mode "tilted": truth (x, y, z, I, bg, bgx,
+    bgy), bgx,bgy~U[-0.15,0.15]) or on a per-spot background image (mode "bgimage": truth
+    (x, y, z, I, bg), constants = an image [R, R] with values in [0.5, 1.5] that bg scales)."""
+    rng = np.random.default_rng(seed)
+    cx, cy, _ = astig_calib_nm(A=A)
+    cx = [cx[0], cx[1] * 1e-3, cx[2] * 1e-3, cx[3] * 1e3, cx[4]]
+    cy = [cy[0], cy[1] * 1e-3, cy[2] * 1e-3, cy[3] * 1e3, cy[4]]
+    c = (R - 1) / 2
+    x = rng.uniform(c - 1, c + 1, n)
+    y = rng.uniform(c - 1, c + 1, n)
+    z = rng.uniform(*zr, n)
+    I = np.exp(rng.uniform(math.log(500), math.log(1e4), n))
+    bg = rng.uniform(2, 15, n)
+    ev = gauss2d_ev(R, x, y, I, np.zeros(n), astig_sigma(z, *cx), astig_sigma(z, *cy))
+    pix = np.arange(R, dtype=np.float64) - R * 0.5
+    if mode == "tilted":
+        bgx = rng.uniform(-0.15, 0.15, n)
+        bgy = rng.uniform(-0.15, 0.15, n)
+        ev += bg[:, None, None] + bgx[:, None, None] * pix[None, None, :] + bgy[:, None, None] * pix[None, :, None]
+        truth = np.stack([x, y, z, I, bg, bgx, bgy], 1).astype(np.float32)
+        return dict(kind="CSplineTilted", R=R, samples=_poisson(rng, ev), truth=truth)
+    gx = rng.uniform(-0.5, 0.5, n)[:, None, None] * pix[None, None, :] / (R * 0.5)
+    gy = rng.uniform(-0.5, 0.5, n)[:, None, None] * pix[None, :, None] / (R * 0.5)
+    img = (1.0 + 0.5 * (gx + gy)).astype(np.float32)
+    ev += bg[:, None, None] * img
+    truth = np.stack([x, y, z, I, bg], 1).astype(np.float32)
+    return dict(kind="CSplineBgImage", R=R, samples=_poisson(rng, ev), truth=truth,
+                constants=img.reshape(n, R * R))
+
+
 MIXED_SIZES = (7, 9, 11, 16)
 MIXED_SIZE_P = (0.2, 0.3, 0.3, 0.2)
 MIXED_MODELS = ("XYIBg", "XYIBgSigmaXY", "XYZIBg")

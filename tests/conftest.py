@@ -28,7 +28,7 @@ def load_golden(name):
 
 
 GOLDEN_SETS = ["xyibg_r10", "constsigma_r9", "sigma_r11", "sigmaxy_r16", "astig_r12", "spline_r13", "tiltedbg_r11",
-               "tiltedsxy_r11"]
+               "tiltedsxy_r11", "spline_tilted_r13", "spline_bgimage_r13"]
 
 
 @pytest.fixture(scope="session")

@@ -57,6 +57,19 @@ def main(only=None):
         d = synth.tilted(300, seed=114, free_sigma=True)
         e = ref_lib.RefEstimator("XYITiltedBgSigmaXY", d["R"], sigma=d["sigma"])
         _fit_and_save("tiltedsxy_r11", e, d, extra=dict(sigma=np.float32(d["sigma"])))
+    if want("spline_tilted_r13") or want("spline_bgimage_r13"):
+        # the spline modes CSPLINE_TILTEDBG (1) and CSPLINE_BGIMAGE (2) on the spline_r13 calibration
+        zstack, zr = synth.astig_zstack(shape_xy=24, nz=21, zrange_um=(-0.4, 0.4))
+        coefs = ref_lib.spline_compute(zstack, border=1)
+        if want("spline_tilted_r13"):
+            d = synth.spline_background(300, "tilted", seed=118)
+            e = ref_lib.RefEstimator("CSpline", d["R"], coefs=coefs, spline_zrange=zr, spline_mode=1)
+            _fit_and_save("spline_tilted_r13", e, d, extra=dict(zstack=zstack, spline_zrange=np.float32(zr)))
+        if want("spline_bgimage_r13"):
+            d = synth.spline_background(300, "bgimage", seed=119)
+            e = ref_lib.RefEstimator("CSpline", d["R"], coefs=coefs, spline_zrange=zr, spline_mode=2)
+            _fit_and_save("spline_bgimage_r13", e, d, constants=d["constants"],
+                          extra=dict(zstack=zstack, spline_zrange=np.float32(zr)))
     if want("intensitybg_r9"):
         # Gauss2D_EstimateIntensityBg: spots at known positions; sigma given per spot as [n][2]
         # with distinct values, so the reference's flat indexing of it (GaussianPSF.cu:225) is pinned

@@ -20,7 +20,8 @@ def oracle_model(name, g):
         return O.Model(O.XYZIBG, R, astig_x=g["astig_x"], astig_y=g["astig_y"], zrange=tuple(g["zrange"]))
     if name.startswith("spline"):
         coefs = O.spline_compute(g["zstack"], border=1)
-        return O.Model(O.CSPLINE, R, coefs=coefs, spline_zrange=tuple(g["spline_zrange"]))
+        mid = O.CSPLINE_TILTED if "tilted" in name else (O.CSPLINE_BGIMAGE if "bgimage" in name else O.CSPLINE)
+        return O.Model(mid, R, coefs=coefs, spline_zrange=tuple(g["spline_zrange"]))
     if name.startswith("tiltedbg"):
         return O.Model(O.XYITILTEDBG, R)
     if name.startswith("tiltedsxy"):
@@ -46,7 +47,8 @@ def cuda_estimator(name, g, ctx):
         sm = pb.CSplineMethods(ctx)
         coefs = sm.ComputeSplineCoeff(g["zstack"], border=1)
         calib = pb.CSplineCalibration(float(g["spline_zrange"][0]), float(g["spline_zrange"][1]), coefs)
-        est = sm.CreatePSF_XYZIBg(R, calib, sm.FlatBg, True)
+        mode = sm.TiltedBg if "tilted" in name else (sm.BgImage if "bgimage" in name else sm.FlatBg)
+        est = sm.CreatePSF_XYZIBg(R, calib, mode, True)
         est._keep = calib
         return est
     if name.startswith("tiltedbg"):

@@ -27,6 +27,8 @@ FLOORS = {
     "tiltedbg_r11": dict(it_match=0.90, pos_ok_converged=0.99, phot_ok_converged=0.90),
     # every spot runs to the iteration cap in the reference (its tilt columns move mu not at all)
     "tiltedsxy_r11": dict(conv_flag_match=0.99, pos_ok=0.5),
+    "spline_tilted_r13": dict(it_match=0.40, pos_ok_converged=0.95, phot_ok_converged=0.85),
+    "spline_bgimage_r13": dict(it_match=0.40, pos_ok_converged=0.95, phot_ok_converged=0.85),
 }
 
 
