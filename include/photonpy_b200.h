@@ -190,6 +190,42 @@ int EstimQueue_GetQueueLength(EstimQueue* q);                                  /
 int EstimQueue_GetResults(EstimQueue* q, int maxresults, float* estim, float* diag, float* crlb, int* roipos,
                           float* samples, EstimatorResult* results);
 
+/* ---- Spot detection and ROI extraction, SpotDetection/SpotDetector.h:39-62, 129-137 -----
+ * Detection image D = box(frame - bg, u1) - box(frame - bg, u2) (windows clipped at the border);
+ * a pixel is a spot where D equals its maxFilterSize maximum, its ROI fits the frame, and
+ * minIntensity < D < maxIntensity. Spots come in row-major pixel order. */
+typedef struct SpotDetectorConfig { /* layout of photonpy/cpp/spotdetect.py's SpotDetector */
+    int uniformFilter1Size, uniformFilter2Size, maxFilterSize;
+    int roisize;                    /* border test */
+    float minIntensity, maxIntensity;
+    float* backgroundImage;         /* host [h][w] or NULL; read at every ProcessFrame call */
+} SpotDetectorConfig;
+typedef struct SpotDetectorFactory SpotDetectorFactory; /* opaque; the reference's ISpotDetectorFactory */
+/* SpotDetector.cu:21-28. Filter windows up to 32 pixels. */
+SpotDetectorFactory* SpotDetector_Configure(const SpotDetectorConfig* config);
+void SpotDetector_DestroyFactory(SpotDetectorFactory* factory);
+/* SpotDetector.cu:101-151: detects the spots of one host frame [height][width], returns their
+ * number (at most maxSpots) and writes scores[n], spotZ[n] (0), cornerPosYX[n][2] = (y, x) -
+ * roisize/2 and rois[n][roisize][roisize] (pixels clamped to the frame). calib must be NULL
+ * (camera calibration is not provided). Returns 0 on error. */
+int SpotDetector_ProcessFrame(const float* frame, int width, int height, int roisize, int maxSpots, float* spotScores,
+                              int* spotZ, int* cornerPosYX, float* rois, SpotDetectorFactory* sdf, void* calib);
+/* SpotDetector.cu:155-178: boxes [roiZ][roiY][roiX] at corners startposZYX[n][3] of a frame stack
+ * [depth][height][width], y/x clamped. As in the reference, box slice z is read from frame z of
+ * the stack whatever the corner's z. */
+void ExtractROIs(const float* frames, int width, int height, int depth, int roiX, int roiY, int roiZ,
+                 const int* startposZYX, int numspots, float* rois);
+/* Extension: detection and ROI cut-out of nframes device frames [n][height][width] on a stream,
+ * for feeding the fitter without host copies. d_bg: device [height][width] or NULL (the
+ * configuration's host background image is not used here). Outputs (device): d_found[n] (spots
+ * found per frame, may exceed maxSpotsPerFrame), d_scores[n][maxSpotsPerFrame] (nullable),
+ * d_cornerYX[n][maxSpotsPerFrame][2] and d_rois[n][maxSpotsPerFrame][roisize][roisize] (nullable
+ * together); the first min(found, maxSpotsPerFrame) entries of each frame are written.
+ * Returns 0 or -1. */
+int PB200_DetectSpotsDevice(SpotDetectorFactory* sdf, const float* d_frames, const float* d_bg, int nframes,
+                            int width, int height, int roisize, int maxSpotsPerFrame, int* d_found, int* d_cornerYX,
+                            float* d_scores, float* d_rois, void* stream);
+
 /* ---- Loader-time exports bound eagerly by photonpy/cpp/lib.py ------------------------ */
 int CudaGetNumDevices(void);                                                        /* CudaUtils.cu:12 */
 bool CudaSetDevice(int index);                                                      /* CudaUtils.cu:19 */
@@ -205,6 +241,14 @@ void FFT(const void* src, void* dst, int batchsize, int siglen, int forward);
 void FFT2(const void* src, void* dst, int batchsize, int sigw, int sigh, int forward);
 void DrawROIs(float* image, int width, int height, const float* rois, int numrois, int roisize, const int* roiposYX);
 void Gauss2D_Draw(double* image, int imgw, int imgh, float* spotList, int nspots, float addSigma);
+/* Bound by SpotDetectionMethods.__init__ (photonpy/cpp/spotdetect.py:117,172): the PSF-correlation
+ * detector (PSFCorrelationSpotDetector.cu:13) and the threaded spot-extraction queue
+ * (ImgFilterQueue.cu:346). Both return NULL. */
+void* PSFCorrelationSpotDetector_Configure(const float* bgImage, int imageWidth, int imageHeight,
+                                           const float* psfstack, int roisize, int depth, int maxFilterSizeXY,
+                                           float minPhotons, int bgFilterSize, int debugMode);
+void* SpotExtractionQueue_Create(int width, int height, void* roiQueue, void* spotDetectorFactory, void* calib,
+                                 int numThreads, int sumframes, Context* ctx);
 
 /* ---- Extensions (no reference counterpart) ------------------------------------------ */
 /* Message of the last error on this thread ("" if none); cleared by PB200_ClearError. */

@@ -70,13 +70,15 @@ perl -0pi -e 's/template<typename T>(\s*)PinnedArray\(const DeviceArray<T>& src\
 perl -0pi -e 's/T x = sample\[smpIndex\] \+= readnoiseVG2\[smpIndex\];/T x = sample[smpIndex] + readnoiseVG2[smpIndex];/' Estimators/Estimation.h
 sed -i '/OneOverSqrt2PiSigma3Y = /,/ComputeInitialEstimate/{s/\bimgw\b/Width()/g}' Estimators/Gaussian/GaussianPSFModels.h
 perl -0pi -e 's/\bheight\(\)/Height()/g; s/\bwidth\(\)/Width()/g' Estimators/Gaussian/GaussianPSFModels.h
+# the index-list generator names a predicate that SpotDetector.h defines after including it
+perl -0pi -e 's/#include "SpotIndexListGenerator.h"\n//; s/(struct SpotLocationList)/#include "SpotIndexListGenerator.h"\n\n$1/' SpotDetection/SpotDetector.h
 
 NVCC=${NVCC:-nvcc}
 FLAGS=(-x cu -std=c++17 -O3 -Xcompiler -fPIC,-fpermissive,-w,-O3 --expt-extended-lambda --expt-relaxed-constexpr
        -gencode arch=compute_100a,code=sm_100a -I. -IEstimators -include msvc_compat.h -DNDEBUG)
 SRCS=(Estimators/Estimator.cpp StringUtils.cpp Context.cpp DebugImageCallback.cpp Rendering.cpp CudaUtils.cu
       Estimators/EstimatorImpl.cu Estimators/Gaussian/GaussianPSF.cu Estimators/CSpline/CubicSplinePSF.cu
-      Estimators/EstimationQueue.cpp Estimators/GLRT_PSF.cu)
+      Estimators/EstimationQueue.cpp Estimators/GLRT_PSF.cu SpotDetection/SpotDetector.cu)
 OBJS=()
 pids=()
 for s in "${SRCS[@]}"; do

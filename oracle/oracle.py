@@ -83,6 +83,10 @@ def lib():
                 f.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, fp, fp, dp]
             L.pso_spline_compute.argtypes = [ip, fp, fp, ct.c_int]
             L.pso_glrt_f32.argtypes = [ct.POINTER(PsoModel), ct.c_int, fp, fp, fp, fp, fp]
+            L.pso_detect_spots.argtypes = [fp, fp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int,
+                                           ct.c_float, ct.c_float, ct.c_int, ip, fp]
+            L.pso_detect_spots.restype = ct.c_int
+            L.pso_cut_rois.argtypes = [fp, ct.c_int, ct.c_int, ip, ct.c_int, ct.c_int, ip, fp]
             L.pso_sizeof_model.restype = ct.c_int
             assert L.pso_sizeof_model() == ct.sizeof(PsoModel), "oracle struct layout mismatch"
             _lib = L
@@ -199,3 +203,23 @@ def spline_compute(data, border=0):
     if rc != 0:
         raise RuntimeError("spline basis matrix is singular")
     return out
+
+
+def detect_spots(frame, u1, u2, maxfilter, roisize, min_intensity, max_intensity=np.inf, background=None,
+                 max_spots=100000):
+    """SpotDetector::Detect + SpotDetector_ProcessFrame restated: returns (number found,
+    indices y*w+x [<= max_spots], scores, corner positions [n, 2] (y, x), rois [n, roisize, roisize])."""
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    h, w = frame.shape
+    bg = None if background is None else np.ascontiguousarray(background, dtype=np.float32)
+    idx = np.zeros(max_spots, np.int32)
+    score = np.zeros(max_spots, np.float32)
+    found = lib().pso_detect_spots(_fptr(frame), _fptr(bg), w, h, int(u1), int(u2), int(maxfilter), int(roisize),
+                                   float(min_intensity), float(max_intensity), int(max_spots),
+                                   idx.ctypes.data_as(ct.POINTER(ct.c_int32)), _fptr(score))
+    n = min(found, max_spots)
+    corner = np.zeros((n, 2), np.int32)
+    rois = np.zeros((n, roisize, roisize), np.float32)
+    lib().pso_cut_rois(_fptr(frame), w, h, idx.ctypes.data_as(ct.POINTER(ct.c_int32)), n, int(roisize),
+                       corner.ctypes.data_as(ct.POINTER(ct.c_int32)), _fptr(rois))
+    return found, idx[:n], score[:n], corner, rois

@@ -204,3 +204,104 @@ int pso_glrt_f32(const pso_model_t* m, int n, const float* params, const float* 
     free(ev);
     return 0;
 }
+
+/* ---- Spot detection (SpotDetection/SpotDetector.cu:49-84, 101-151; ImageFilters.h:6-105) ----
+ * Box filter with windows clipped at the image border: X pass then Y pass, each a sequential
+ * float sum over [c - win/2, c - win/2 + win) divided by the number of pixels in the window. */
+static void sd_box(const float* in, float* tmp, float* out, int w, int h, int win)
+{
+    const int back = -win / 2, forw = back + win;
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            int xs = x + back; if (xs < 0) xs = 0;
+            int xe = x + forw; if (xe > w) xe = w;
+            float sum = 0.0f;
+            for (int i = xs; i < xe; i++) sum += in[(size_t)y * w + i];
+            tmp[(size_t)y * w + x] = sum / (float)(xe - xs);
+        }
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            int ys = y + back; if (ys < 0) ys = 0;
+            int ye = y + forw; if (ye > h) ye = h;
+            float sum = 0.0f;
+            for (int i = ys; i < ye; i++) sum += tmp[(size_t)i * w + x];
+            out[(size_t)y * w + x] = sum / (float)(ye - ys);
+        }
+}
+
+/* Maximum filter (ComparisonFilter2DStack with depth 1 and thrust::maximum: a < b ? b : a). */
+static void sd_max(const float* in, float* tmp, float* out, int w, int h, int win)
+{
+    const int back = -win / 2, forw = back + win;
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            int xs = x + back; if (xs < 0) xs = 0;
+            int xe = x + forw; if (xe > w) xe = w;
+            float v = in[(size_t)y * w + xs];
+            for (int i = xs + 1; i < xe; i++) { float b = in[(size_t)y * w + i]; v = v < b ? b : v; }
+            tmp[(size_t)y * w + x] = v;
+        }
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            int ys = y + back; if (ys < 0) ys = 0;
+            int ye = y + forw; if (ye > h) ye = h;
+            float v = tmp[(size_t)ys * w + x];
+            for (int i = ys + 1; i < ye; i++) { float b = tmp[(size_t)i * w + x]; v = v < b ? b : v; }
+            out[(size_t)y * w + x] = v;
+        }
+}
+
+/* Detection of one frame: detection image D = box(src - bg, u1) - box(src - bg, u2); a pixel is
+ * a spot when D equals its max-filtered value, lies more than roisize/2 from the left/top border
+ * and its ROI ends before the last row/column, and min_i < D < max_i. Spots in row-major pixel
+ * order; the first max_spots are written (index y*w + x, score D). Returns the number found. */
+int pso_detect_spots(const float* frame, const float* bg, int w, int h, int u1, int u2, int mf, int roisize,
+                     float min_i, float max_i, int max_spots, int* idx, float* score)
+{
+    const size_t n = (size_t)w * h;
+    float* src = (float*)malloc(sizeof(float) * n);
+    float* tmp = (float*)malloc(sizeof(float) * n);
+    float* f1 = (float*)malloc(sizeof(float) * n);
+    float* f2 = (float*)malloc(sizeof(float) * n);
+    float* mx = (float*)malloc(sizeof(float) * n);
+    for (size_t p = 0; p < n; p++) src[p] = bg ? frame[p] - bg[p] : frame[p];
+    sd_box(src, tmp, f1, w, h, u1);
+    sd_box(src, tmp, f2, w, h, u2);
+    for (size_t p = 0; p < n; p++) f1[p] = f1[p] - f2[p];
+    sd_max(f1, tmp, mx, w, h, mf);
+    int found = 0;
+    const int half = roisize / 2, rest = roisize - roisize / 2;
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            const float a = f1[(size_t)y * w + x], b = mx[(size_t)y * w + x];
+            const int isMax = a == b && x > half && y > half && x + rest < w - 1 && y + rest < h - 1;
+            if (isMax && b > min_i && b < max_i) {
+                if (found < max_spots) {
+                    idx[found] = y * w + x;
+                    score[found] = b;
+                }
+                found++;
+            }
+        }
+    free(src); free(tmp); free(f1); free(f2); free(mx);
+    return found;
+}
+
+/* ROIs of SpotDetector_ProcessFrame: corner = (y, x) - roisize/2, pixels clamped to the frame. */
+void pso_cut_rois(const float* frame, int w, int h, const int* idx, int n, int roisize, int* corner_yx, float* rois)
+{
+    for (int i = 0; i < n; i++) {
+        const int cy = idx[i] / w - roisize / 2, cx = idx[i] % w - roisize / 2;
+        corner_yx[2 * i] = cy;
+        corner_yx[2 * i + 1] = cx;
+        for (int y = 0; y < roisize; y++)
+            for (int x = 0; x < roisize; x++) {
+                int fy = cy + y, fx = cx + x;
+                if (fx < 0) fx = 0;
+                if (fy < 0) fy = 0;
+                if (fx >= w) fx = w - 1;
+                if (fy >= h) fy = h - 1;
+                rois[((size_t)i * roisize + y) * roisize + x] = frame[(size_t)fy * w + fx];
+            }
+    }
+}

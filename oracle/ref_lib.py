@@ -75,6 +75,13 @@ def lib():
         if hasattr(L, "GLRT_CreatePSF"):
             L.GLRT_CreatePSF.argtypes = [vp, vp]
             L.GLRT_CreatePSF.restype = vp
+        if hasattr(L, "SpotDetector_Configure"):
+            L.SpotDetector_Configure.argtypes = [ct.POINTER(SpotDetectorConfig)]
+            L.SpotDetector_Configure.restype = vp
+            L.SpotDetector_DestroyFactory.argtypes = [vp]
+            L.SpotDetector_ProcessFrame.argtypes = [vp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, vp, vp, vp, vp, vp, vp]
+            L.SpotDetector_ProcessFrame.restype = ct.c_int
+            L.ExtractROIs.argtypes = [vp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, vp, ct.c_int, vp]
         if hasattr(L, "EstimQueue_Create"):
             L.EstimQueue_Create.argtypes = [vp, ct.c_int, ct.c_int, ct.c_bool, ct.c_int, vp]
             L.EstimQueue_Create.restype = vp
@@ -93,6 +100,37 @@ def lib():
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+class SpotDetectorConfig(ct.Structure):
+    """SpotDetectorConfig (SpotDetection/SpotDetector.h:39-62), as photonpy/cpp/spotdetect.py lays it out."""
+    _fields_ = [("uniformFilter1Size", ct.c_int32), ("uniformFilter2Size", ct.c_int32), ("maxFilterSize", ct.c_int32),
+                ("roisize", ct.c_int32), ("minIntensity", ct.c_float), ("maxIntensity", ct.c_float),
+                ("backgroundImagePtr", ct.c_void_p)]
+
+
+def process_frame(frame, u1, u2, maxfilter, roisize, min_intensity, max_intensity=np.inf, background=None,
+                  max_spots=10000):
+    """The reference's SpotDetector_ProcessFrame (its CUDA detector; needs a GPU): returns
+    (count, scores, spotz, corner [n, 2] (y, x), rois [n, roisize, roisize])."""
+    L = lib()
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    h, w = frame.shape
+    cfg = SpotDetectorConfig(int(u1), int(u2), int(maxfilter), int(roisize), float(min_intensity),
+                             float(max_intensity), None)
+    bg = None
+    if background is not None:
+        bg = np.ascontiguousarray(background, dtype=np.float32)
+        cfg.backgroundImagePtr = bg.ctypes.data
+    sdf = L.SpotDetector_Configure(ct.byref(cfg))
+    scores = np.zeros(max_spots, np.float32)
+    spotz = np.zeros(max_spots, np.int32)
+    corner = np.zeros((max_spots, 2), np.int32)
+    rois = np.zeros((max_spots, roisize, roisize), np.float32)
+    n = L.SpotDetector_ProcessFrame(_p(frame), w, h, int(roisize), int(max_spots), _p(scores), _p(spotz), _p(corner),
+                                    _p(rois), sdf, None)
+    L.SpotDetector_DestroyFactory(sdf)
+    return n, scores[:n], spotz[:n], corner[:n], rois[:n]
 
 
 class RefEstimator:

@@ -29,6 +29,7 @@
 #include <cstring>
 #include <deque>
 #include <limits>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -54,9 +55,53 @@ struct QueueError : std::runtime_error {
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Process-wide cache of pinned host blocks, keyed by size. Pinning memory costs about as much
+// as copying it, so blocks of deleted queues are kept (up to kPinnedCacheBytes) for the next
+// queue instead of being returned to the driver.
+class PinnedCache {
+public:
+    static PinnedCache& get() {
+        static PinnedCache* c = new PinnedCache();  // never destroyed: outlives every queue
+        return *c;
+    }
+    void* take(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            auto it = free_.find(bytes);
+            if (it != free_.end()) {
+                void* p = it->second;
+                free_.erase(it);
+                held_ -= bytes;
+                return p;
+            }
+        }
+        void* p = nullptr;
+        PBQ_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocPortable));
+        return p;
+    }
+    void give(void* p, size_t bytes) {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            if (held_ + bytes <= kPinnedCacheBytes) {
+                free_.emplace(bytes, p);
+                held_ += bytes;
+                return;
+            }
+        }
+        cudaFreeHost(p);
+    }
+
+private:
+    static constexpr size_t kPinnedCacheBytes = size_t(2) << 30;
+    std::mutex m_;
+    std::multimap<size_t, void*> free_;
+    size_t held_ = 0;
+};
+
 // One pinned allocation split into consecutive 256-byte aligned arrays of the given sizes.
 struct PinnedBlock {
     void* mem = nullptr;
+    size_t bytes = 0;
     std::vector<char*> parts;
     PinnedBlock(std::initializer_list<size_t> sizes) {
         size_t o = 0;
@@ -65,11 +110,12 @@ struct PinnedBlock {
             off.push_back(o);
             o = align_up(o + s, 256);
         }
-        PBQ_CUDA(cudaHostAlloc(&mem, o ? o : 256, cudaHostAllocPortable));
+        bytes = o ? o : 256;
+        mem = PinnedCache::get().take(bytes);
         for (size_t x : off) parts.push_back(static_cast<char*>(mem) + x);
     }
     ~PinnedBlock() {
-        if (mem) cudaFreeHost(mem);
+        if (mem) PinnedCache::get().give(mem, bytes);
     }
     PinnedBlock(const PinnedBlock&) = delete;
     PinnedBlock& operator=(const PinnedBlock&) = delete;

@@ -1400,6 +1400,14 @@ void FFT(const void*, void*, int, int, int) { not_provided("FFT"); }
 void FFT2(const void*, void*, int, int, int, int) { not_provided("FFT2"); }
 void DrawROIs(float*, int, int, const float*, int, int, const int*) { not_provided("DrawROIs"); }
 void Gauss2D_Draw(double*, int, int, float*, int, float) { not_provided("Gauss2D_Draw"); }
+void* PSFCorrelationSpotDetector_Configure(const float*, int, int, const float*, int, int, int, float, int, int) {
+    not_provided("PSFCorrelationSpotDetector_Configure");
+    return nullptr;
+}
+void* SpotExtractionQueue_Create(int, int, void*, void*, void*, int, int, Context*) {
+    not_provided("SpotExtractionQueue_Create");
+    return nullptr;
+}
 // GaussianPSF.cu:216-240: intensity and background of each spot at a known position xy[i]
 // and width, by the LM fit of mu = I * DeltaX DeltaY + bg from (1, 0) with lambda 1e-15 and
 // maxIterations iterations, and their CRLB (sqrt of the |diagonal| of the inverse Fisher

@@ -294,6 +294,28 @@ def spline_background(n, mode, seed=6, R=13, zr=(-0.38, 0.38), A=0.1):
                 constants=img.reshape(n, R * R))
 
 
+def frames(n, h=128, w=160, spots_per_frame=20, seed=8, sigma=1.5, I=(300, 3000), bg=(3.0, 8.0), margin=2):
+    """Camera frames [n, h, w] with Gaussian spots at random positions (at least `margin` px
+    from the border) on a flat background, Poisson noise. Returns dict(frames, truth) with truth
+    rows (frame, x, y, I, bg)."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, h, w), np.float32)
+    truth = []
+    px, py = np.arange(w, dtype=np.float64), np.arange(h, dtype=np.float64)
+    for f in range(n):
+        b = rng.uniform(*bg)
+        x = rng.uniform(margin, w - 1 - margin, spots_per_frame)
+        y = rng.uniform(margin, h - 1 - margin, spots_per_frame)
+        inten = rng.uniform(*I, spots_per_frame)
+        dx = _delta(px, x, np.full(spots_per_frame, sigma))
+        dy = _delta(py, y, np.full(spots_per_frame, sigma))
+        ev = b + np.einsum("s,sy,sx->yx", inten, dy, dx)
+        out[f] = rng.poisson(ev)
+        for k in range(spots_per_frame):
+            truth.append((f, x[k], y[k], inten[k], b))
+    return dict(frames=out, truth=np.array(truth, np.float64))
+
+
 MIXED_SIZES = (7, 9, 11, 16)
 MIXED_SIZE_P = (0.2, 0.3, 0.3, 0.2)
 MIXED_MODELS = ("XYIBg", "XYIBgSigmaXY", "XYZIBg")

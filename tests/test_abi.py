@@ -25,7 +25,11 @@ def test_header_declares_reference_abi():
                  "Gauss2D_CreatePSF_XYZIBg", "CSpline_CreatePSF", "CSpline_Compute", "Context_Create",
                  "Context_Destroy", "Estimator_GetParamLimits", "Estimator_SetLMParams", "EstimQueue_Create",
                  "EstimQueue_Delete", "EstimQueue_Schedule", "EstimQueue_Flush", "EstimQueue_IsIdle",
-                 "EstimQueue_GetResultCount", "EstimQueue_GetQueueLength", "EstimQueue_GetResults"]:
+                 "EstimQueue_GetResultCount", "EstimQueue_GetQueueLength", "EstimQueue_GetResults",
+                 "GLRT_CreatePSF", "Gauss2D_CreatePSF_XYITiltedBg", "Gauss2D_CreatePSF_XYITiltedBgSigmaXY",
+                 "Gauss2D_EstimateIntensityBg", "SpotDetector_Configure", "SpotDetector_ProcessFrame",
+                 "SpotDetector_DestroyFactory", "ExtractROIs", "PSFCorrelationSpotDetector_Configure",
+                 "SpotExtractionQueue_Create"]:
         assert must in names
 
 
@@ -57,3 +61,6 @@ def test_struct_layouts_match_reference_ctypes():
     assert pb.CSplineCalibration.coefs.offset == 24
     assert ctypes.sizeof(pb.LevMarParams) == 12
     assert ctypes.sizeof(pb.EstimatorProperties) == 20
+    from photonpy_b200 import spotdetect
+    assert ctypes.sizeof(spotdetect.SpotDetector) == 32
+    assert spotdetect.SpotDetector.backgroundImagePtr.offset == 24

@@ -142,3 +142,22 @@ def test_oracle_intensity_bg_bit_exact():
     assert np.array_equal(p, g["ibg"])
     crlb, _ = m.crlb(p, None, constants=consts)
     assert np.array_equal(crlb, g["ibg_crlb"])
+
+
+def test_oracle_spot_detection_finds_planted_spots():
+    """The detection restatement (SpotDetector.cu:49-84) finds well-separated bright spots, in
+    row-major order, honours the border rule and the maxSpots cap."""
+    from photonpy_b200 import synth
+    d = synth.frames(1, h=96, w=128, spots_per_frame=12, seed=3, I=(2000, 4000), margin=10)
+    fr = d["frames"][0]
+    found, idx, score, corner, rois = O.detect_spots(fr, 5, 10, 7, 9, 7.0)
+    assert np.all(np.diff(idx) > 0)
+    ys, xs = idx // 128, idx % 128
+    tx, ty = d["truth"][:, 1], d["truth"][:, 2]
+    dist = np.hypot(xs[:, None] - tx[None], ys[:, None] - ty[None]).min(axis=0)
+    assert np.mean(dist < 1.5) > 0.8
+    assert np.all((xs > 4) & (ys > 4) & (xs + 5 < 127) & (ys + 5 < 95))
+    assert np.array_equal(corner, np.stack([ys - 4, xs - 4], 1))
+    assert np.array_equal(rois[0], fr[corner[0, 0]:corner[0, 0] + 9, corner[0, 1]:corner[0, 1] + 9])
+    f2, idx2, _, _, _ = O.detect_spots(fr, 5, 10, 7, 9, 7.0, max_spots=3)
+    assert f2 == found and np.array_equal(idx2, idx[:3])
