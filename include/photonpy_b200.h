@@ -221,10 +221,18 @@ void ExtractROIs(const float* frames, int width, int height, int depth, int roiX
  * found per frame, may exceed maxSpotsPerFrame), d_scores[n][maxSpotsPerFrame] (nullable),
  * d_cornerYX[n][maxSpotsPerFrame][2] and d_rois[n][maxSpotsPerFrame][roisize][roisize] (nullable
  * together); the first min(found, maxSpotsPerFrame) entries of each frame are written.
+ * The factory's device scratch (about one frame batch of floats) is kept between calls and
+ * grown on demand; calls on one factory from different streams are ordered by an event.
  * Returns 0 or -1. */
 int PB200_DetectSpotsDevice(SpotDetectorFactory* sdf, const float* d_frames, const float* d_bg, int nframes,
                             int width, int height, int roisize, int maxSpotsPerFrame, int* d_found, int* d_cornerYX,
                             float* d_scores, float* d_rois, void* stream);
+/* Extension (diagnostic): the spot detector's box filters divide a sum by a pixel count k with
+ * one multiply by the rounded reciprocal and one FMA correction instead of an IEEE division.
+ * This compares the two bit for bit on the current device for every float x and k = 1..maxCount
+ * (maxCount <= 32): mismatches[k-1] = number of differing results (NaN vs NaN is equal),
+ * lastBadBits[k-1] (nullable) = bits of one such x. Returns 0 or -1. */
+int PB200_CheckCountDivision(int maxCount, unsigned long long* mismatches, unsigned* lastBadBits);
 
 /* ---- Loader-time exports bound eagerly by photonpy/cpp/lib.py ------------------------ */
 int CudaGetNumDevices(void);                                                        /* CudaUtils.cu:12 */

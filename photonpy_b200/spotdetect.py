@@ -75,6 +75,35 @@ class SpotDetector(ctypes.Structure):
             check_error("SpotDetector_Configure")
         return SpotDetectorNativeFactory(inst, m._SpotDetector_DestroyFactory)
 
+    def _key(self):
+        return (self.uniformFilter1Size, self.uniformFilter2Size, self.maxFilterSize, self.roisize,
+                float(self.minIntensity), float(self.maxIntensity), self.backgroundImagePtr or 0)
+
+    def _cached_factory(self, methods):
+        """Native factory kept with this detector for repeated device calls (its device scratch
+        then stays allocated); rebuilt when a field changes."""
+        key = self._key()
+        cached = self.__dict__.get("_native")
+        if cached is not None and cached[0] == key:
+            return cached[1]
+        self._release_native()
+        inst = methods._SpotDetector_Configure(self)
+        if not inst:
+            check_error("SpotDetector_Configure")
+        self._native = (key, inst, methods._SpotDetector_DestroyFactory)
+        return inst
+
+    def _release_native(self):
+        cached = self.__dict__.pop("_native", None)
+        if cached is not None:
+            cached[2](cached[1])
+
+    def __del__(self):
+        try:
+            self._release_native()
+        except Exception:
+            pass
+
 
 class SpotDetectionMethods:
     def __init__(self, ctx):
@@ -161,16 +190,16 @@ class SpotDetectionMethods:
         if background is not None:
             bg = torch.as_tensor(background, dtype=torch.float32, device=dev).contiguous()
         s = stream if stream is not None else torch.cuda.current_stream(dev)
-        with spotDetector.CreateNativeFactory(self.ctx) as sdf:
-            rc = self._DetectDevice(sdf.inst, frames.data_ptr(), None if bg is None else bg.data_ptr(), n, w, h,
-                                    int(roisize), K, found.data_ptr(), corner.data_ptr(), scores.data_ptr(),
-                                    rois.data_ptr(), ctypes.c_void_p(s.cuda_stream))
-            if rc != 0:
-                check_error("DetectSpotsDevice")
-            counts = torch.clamp(found, max=K)
-            keep = torch.arange(K, device=dev)[None, :] < counts[:, None].to(torch.int64)
-            frame_idx = torch.arange(n, device=dev)[:, None].expand(n, K)
-            return rois[keep], corner[keep], frame_idx[keep], scores[keep], found
+        inst = spotDetector._cached_factory(self)
+        rc = self._DetectDevice(inst, frames.data_ptr(), None if bg is None else bg.data_ptr(), n, w, h,
+                                int(roisize), K, found.data_ptr(), corner.data_ptr(), scores.data_ptr(),
+                                rois.data_ptr(), ctypes.c_void_p(s.cuda_stream))
+        if rc != 0:
+            check_error("DetectSpotsDevice")
+        counts = torch.clamp(found, max=K)
+        keep = torch.arange(K, device=dev)[None, :] < counts[:, None].to(torch.int64)
+        frame_idx = torch.arange(n, device=dev)[:, None].expand(n, K)
+        return rois[keep], corner[keep], frame_idx[keep], scores[keep], found
 
 
 def localize_frames(frames, spotDetector, estimator, roisize, maxSpotsPerFrame=1000, background=None):

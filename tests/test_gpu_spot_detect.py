@@ -5,8 +5,10 @@ The detection restatement in the oracle is pinned bit for bit against the refere
 detector (oracle/_ref, run on this GPU); the CUDA path is then compared bit for bit with the
 oracle: same spots in the same order, same scores, corners and ROI pixels. Cases: frames whose
 sizes are not multiples of the 32-pixel tile, spots at the borders, a background image, an
-intensity window, the maxSpots cap, several frames per launch. The end-to-end check fits the
-detected ROIs and compares positions with the planted spots.
+intensity window, the maxSpots cap, several frames per launch, filter sizes outside the
+register-strip instantiations (the generic kernel). The end-to-end check fits the detected ROIs
+and compares positions with the planted spots. The exact count division the box filters use is
+compared with IEEE division for every float.
 """
 import numpy as np
 import pytest
@@ -71,6 +73,57 @@ def test_process_frame_equals_oracle(ctx, c):
     assert np.array_equal(corner, ocorner)
     assert np.array_equal(rois, orois)
     assert np.all(spotz == 0)
+
+
+@pytest.mark.parametrize("sizes", [(5, 9, 7), (3, 7, 4), (10, 20, 20), (1, 3, 1), (6, 12, 3)])
+def test_process_frame_filter_sizes(ctx, sizes):
+    """Box/maximum filter sizes set directly: (5, 9) and (3, 7) are not u2 = 2 u1 and (10, 20) is
+    above the instantiations, so these run the generic kernel; (1, 3, 1) makes every pixel a
+    local maximum; (6, 12, 3) is a register-strip kernel with a small maximum filter."""
+    from photonpy_b200 import spotdetect
+    u1, u2, mf = sizes
+    d = synth.frames(1, h=70, w=90, spots_per_frame=12, seed=20 + u1, margin=0)
+    fr = d["frames"][0]
+    sd = spotdetect.SpotDetector(1.5, 7, 2.0)
+    sd.uniformFilter1Size, sd.uniformFilter2Size, sd.maxFilterSize = u1, u2, mf
+    rois, corner, scores, _ = spotdetect.SpotDetectionMethods(ctx).ProcessFrame(fr, sd, 7, 5000)
+    found, idx, oscore, ocorner, orois = O.detect_spots(fr, u1, u2, mf, 7, 2.0, max_spots=5000)
+    assert len(scores) == min(found, 5000) > 0
+    assert np.array_equal(scores, oscore)
+    assert np.array_equal(corner, ocorner)
+    assert np.array_equal(rois, orois)
+
+
+def test_process_frame_nan_and_inf_pixels(ctx):
+    """NaN and infinite pixels: tiles whose detection image holds NaN take the left-to-right
+    maximum fold (where NaN is not skipped like a number); results equal the oracle's."""
+    from photonpy_b200 import spotdetect
+    d = synth.frames(1, h=96, w=100, spots_per_frame=20, seed=31, margin=0)
+    fr = d["frames"][0].copy()
+    fr[10, 10] = np.nan
+    fr[50, 70] = np.inf
+    fr[80, 5] = -np.inf
+    fr[40, 40] = np.nan
+    fr[41, 44] = np.inf
+    sd = spotdetect.SpotDetector(1.5, 9, 7.0)
+    rois, corner, scores, _ = spotdetect.SpotDetectionMethods(ctx).ProcessFrame(fr, sd, 9, 1000)
+    u1, u2, mf = _sizes(1.5)
+    found, idx, oscore, ocorner, orois = O.detect_spots(fr, u1, u2, mf, 9, 7.0, max_spots=1000)
+    assert len(scores) == min(found, 1000) > 0
+    assert np.array_equal(scores, oscore, equal_nan=True)
+    assert np.array_equal(corner, ocorner)
+    assert np.array_equal(rois, orois, equal_nan=True)
+
+
+def test_count_division_exhaustive(ctx):
+    """The box filters' sum / count (rounded reciprocal, one FMA correction) equals IEEE division
+    bit for bit for all 2^32 floats and every count 1..32."""
+    import ctypes
+    lib = ctx.smlm.lib
+    bad = (ctypes.c_ulonglong * 32)()
+    last = (ctypes.c_uint * 32)()
+    assert lib.PB200_CheckCountDivision(32, bad, last) == 0
+    assert list(bad) == [0] * 32, [(k + 1, bad[k], hex(last[k])) for k in range(32) if bad[k]]
 
 
 def test_detect_device_batch_equals_oracle(ctx):
