@@ -81,12 +81,17 @@ __device__ __forceinline__ int div_small(int i, float inv) { return (int)(((floa
 // sign), quotients near the subnormal range (the remainder is no longer exact there), infinities
 // and NaN take the IEEE division. PB200_CheckCountDivision compares the result bit for bit with
 // IEEE division for every float x and every d = 1..32, the counts the box filters divide by.
-__device__ __forceinline__ float pb200_count_div(float x, float d, float r) {
-    const float q = __fmul_rn(x, r);
-    const float aq = fabsf(q);
-    if (!(aq >= 0x1p-100f) || aq > 0x1p+126f) return __fdiv_rn(x, d);
+__device__ __forceinline__ bool count_div_in_range(float q) {
+    const float a = fabsf(q);
+    return a >= 0x1p-100f && a <= 0x1p+126f;  // false for NaN
+}
+__device__ __forceinline__ float count_div_corrected(float x, float q, float d, float r) {
     const float e = __fmaf_rn(-q, d, x);
     return __fmaf_rn(e, r, q);
+}
+__device__ __forceinline__ float pb200_count_div(float x, float d, float r) {
+    const float q = __fmul_rn(x, r);
+    return count_div_in_range(q) ? count_div_corrected(x, q, d, r) : __fdiv_rn(x, d);
 }
 
 // Box filter at global coordinate g of a line of `extent` samples, window [g - win/2, g - win/2 +
@@ -124,6 +129,8 @@ __device__ __forceinline__ void box_strip(const FilterParams& p, const float (&v
                                           float (&o1)[4], float (&o2)[4]) {
     constexpr int off1 = U2 / 2 - U1 / 2;  // the u1 window starts off1 samples into the u2 window
     const bool interior = g0 - U2 / 2 >= 0 && g0 + 3 - U2 / 2 + U2 <= extent;  // u1 windows lie inside
+    float S1[4], S2[4];
+    int C1[4], C2[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         float s1 = 0.0f, s2 = 0.0f;
@@ -139,8 +146,33 @@ __device__ __forceinline__ void box_strip(const FilterParams& p, const float (&v
             c1 = clampi(c1, 1, kMaxWindow);  // outside the line the value is unused
             c2 = clampi(c2, 1, kMaxWindow);
         }
-        o1[j] = pb200_count_div(s1, (float)c1, p.rcp[c1]);
-        o2[j] = pb200_count_div(s2, (float)c2, p.rcp[c2]);
+        S1[j] = s1;
+        S2[j] = s2;
+        C1[j] = c1;
+        C2[j] = c2;
+    }
+    // pb200_count_div for all eight quotients, with one branch to the IEEE division when any of
+    // them is out of the corrected range
+    float q1[4], q2[4];
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        q1[j] = __fmul_rn(S1[j], p.rcp[C1[j]]);
+        q2[j] = __fmul_rn(S2[j], p.rcp[C2[j]]);
+        ok = ok && count_div_in_range(q1[j]) && count_div_in_range(q2[j]);
+    }
+    if (ok) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            o1[j] = count_div_corrected(S1[j], q1[j], (float)C1[j], p.rcp[C1[j]]);
+            o2[j] = count_div_corrected(S2[j], q2[j], (float)C2[j], p.rcp[C2[j]]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            o1[j] = __fdiv_rn(S1[j], (float)C1[j]);
+            o2[j] = __fdiv_rn(S2[j], (float)C2[j]);
+        }
     }
 }
 
@@ -513,20 +545,73 @@ __global__ void count_div_check_kernel(float d, float r, unsigned long long* mis
     if (bad) atomicAdd(mismatches, bad);
 }
 
+// Device buffers of the detector come from a small process-wide cache, so a factory per
+// ProcessFrame call (photonpy's usage) costs no cudaMalloc/cudaFree once warm. A buffer goes back
+// to the cache only when no kernel uses it any more (its owner has synchronised).
+class BufferCache {
+   public:
+    static BufferCache& get() {
+        static BufferCache* c = new BufferCache();  // never destroyed: no CUDA calls at exit
+        return *c;
+    }
+    void* take(size_t n, size_t* got) {
+        int dev = 0;
+        PBS_CUDA(cudaGetDevice(&dev));
+        {
+            std::lock_guard<std::mutex> g(mtx_);
+            for (size_t i = 0; i < blocks_.size(); i++) {
+                Block b = blocks_[i];
+                if (b.dev == dev && b.bytes >= n && b.bytes <= 2 * n + (1 << 20)) {
+                    blocks_.erase(blocks_.begin() + (long)i);
+                    held_ -= b.bytes;
+                    *got = b.bytes;
+                    return b.p;
+                }
+            }
+        }
+        void* p = nullptr;
+        PBS_CUDA(cudaMalloc(&p, n));
+        *got = n;
+        return p;
+    }
+    void give(void* p, size_t n) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return;
+        std::lock_guard<std::mutex> g(mtx_);
+        if (held_ + n > kMaxHeld || blocks_.size() >= 32) {
+            cudaFree(p);
+            return;
+        }
+        blocks_.push_back(Block{p, n, dev});
+        held_ += n;
+    }
+
+   private:
+    struct Block {
+        void* p;
+        size_t bytes;
+        int dev;
+    };
+    static constexpr size_t kMaxHeld = size_t(1) << 30;
+    std::mutex mtx_;
+    std::vector<Block> blocks_;
+    size_t held_ = 0;
+};
+
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
     void ensure(size_t n) {
         if (n <= bytes) return;
-        if (p) cudaFree(p);
+        release();
+        p = BufferCache::get().take(n < 256 ? 256 : n, &bytes);
+    }
+    void release() {
+        if (p) BufferCache::get().give(p, bytes);
         p = nullptr;
         bytes = 0;
-        PBS_CUDA(cudaMalloc(&p, n < 256 ? 256 : n));
-        bytes = n < 256 ? 256 : n;
     }
-    ~DevMem() {
-        if (p) cudaFree(p);
-    }
+    ~DevMem() { release(); }
     template <class T>
     T* as() const { return static_cast<T*>(p); }
 };
