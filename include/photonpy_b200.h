@@ -325,6 +325,10 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
 /* Kernel configuration used for this estimator: lanes per ROI (4, 8, 16, 32; 0 = automatic)
  * and threads per block (64..256). Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
+/* Extension: the host-pointer pipeline of the Estimate/CRLB calls. The ROIs are fitted in chunks of
+ * roisPerChunk (0: automatic), with `slots` chunks (2..4) in flight: while one chunk is fitted
+ * the next ones are copied in and the previous ones copied out. Returns 0 or -1. */
+int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots);
 void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock);
 /* Fit kernel family for the Gaussian models: 0 = column-blocked (default), 1 = generic
  * per-pixel table kernel (the spline model always uses 1). Returns 0 on success. */

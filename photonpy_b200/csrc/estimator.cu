@@ -230,7 +230,10 @@ struct Estimator {
     DevBuf glrtRoi0;
     bool crlbAbs = false;  // CRLB = sqrt(|diag of the inverse|) (the intensity/background fit)
     std::mutex mtx;
-    Slot slots[2];
+    // host-pointer pipeline: ROIs per chunk (0: automatic) and slots (chunks in flight, 2..4)
+    int hostChunk = 0;
+    int hostSlots = 4;
+    Slot slots[4];
 
     Estimator() { PB_CUDA(cudaGetDevice(&device)); }
     ~Estimator() {
@@ -328,8 +331,8 @@ struct Chunking {
     int chunk;
 };
 
-// Host-pointer fit through the two-slot pipeline: H2D(c) + kernel(c) on slot c%2 are issued
-// before D2H(c-1), so copies of one chunk overlap the fit of the other.
+// Host-pointer fit through the slot pipeline: H2D(c) + kernel(c) on slot c % slots are issued
+// before D2H(c - slots + 1), so the copies of one chunk overlap the fits of the others.
 void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, const float* h_initial,
               float* h_params, int* h_iters, float* h_trace, int traceLen, float* h_crlb, float* h_chisq,
               int flags, float* h_glrt = nullptr) {
@@ -342,9 +345,25 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         e->glrtRoi0.ensure(sizeof(float) * npix);
         PB_CUDA(cudaMemcpy(e->glrtRoi0.p, h_smp, sizeof(float) * npix, cudaMemcpyHostToDevice));
     }
+    // Chunks of at most 64 MB of samples (at least 16384 ROIs, an eighth of the call when that is
+    // smaller); the first three are 1/8, 1/4 and 1/2 of that, so the first fit starts early.
     int chunk = n;
-    if (n > 65536) chunk = std::max(32768, (n + 7) / 8);
-    const int nchunks = (n + chunk - 1) / chunk;
+    if (e->hostChunk > 0) {
+        chunk = std::min(n, e->hostChunk);
+    } else if (n > 16384) {
+        const int cmax = (int)std::max<long long>(4096, (64LL << 20) / (4LL * npix));
+        chunk = std::min(cmax, std::max(16384, (n + 7) / 8));
+    }
+    std::vector<std::pair<int, int>> chunks;  // (start, count)
+    for (int start = 0, k = 0; start < n; k++) {
+        int c = chunk;
+        if (k < 3 && n > chunk) c = std::max(1024, chunk >> (3 - k));
+        c = std::min(c, n - start);
+        chunks.push_back({start, c});
+        start += c;
+    }
+    const int nchunks = (int)chunks.size();
+    const int nslots = e->hostSlots;
     FitLaunch fl = e->fit_launch();
     struct Pending {
         int slot, start, count;
@@ -373,8 +392,8 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
                                     cudaMemcpyDeviceToHost, s.stream));
     };
     for (int c = 0; c < nchunks; c++) {
-        const int start = c * chunk, count = std::min(chunk, n - start);
-        Slot& s = e->slot(c & 1);
+        const int start = chunks[c].first, count = chunks[c].second;
+        Slot& s = e->slot(c % nslots);
         if (h_smp) {
             s.smp.ensure(sizeof(float) * (size_t)npix * count);
             PB_CUDA(cudaMemcpyAsync(s.smp.p, h_smp + (size_t)start * npix, sizeof(float) * (size_t)npix * count,
@@ -424,14 +443,14 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         }
         fl(e->desc, a, e->threads, s.stream);
         if (h_crlb) launch_crlb(K, a.fisher, a.crlb, a.chisq, count, s.stream, e->crlbAbs);
-        pend.push_back({c & 1, start, count});
-        if (pend.size() == 2) {
+        pend.push_back({c % nslots, start, count});
+        if ((int)pend.size() == nslots) {
             d2h(pend.front());
             pend.erase(pend.begin());
         }
     }
     for (auto& p : pend) d2h(p);
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < 4; i++)
         if (e->slots[i].stream) PB_CUDA(cudaStreamSynchronize(e->slots[i].stream));
 }
 
@@ -1055,6 +1074,14 @@ int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {
     std::lock_guard<std::mutex> g(e->mtx);
     e->lanes = lanesPerRoi;
     e->threads = threadsPerBlock;
+    return 0;
+}
+
+int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots) {
+    if (!e || roisPerChunk < 0 || slots < 2 || slots > 4) return -1;
+    std::lock_guard<std::mutex> g(e->mtx);
+    e->hostChunk = roisPerChunk;
+    e->hostSlots = slots;
     return 0;
 }
 

@@ -326,6 +326,13 @@ class Estimator:
         if rc != 0:
             raise ValueError("invalid kernel configuration")
 
+    def SetHostPipeline(self, rois_per_chunk=0, slots=4):
+        """Chunking of the host-array calls (Estimate, EstimateWithCRLB, ...): ROIs per chunk
+        (0 = automatic: up to 64 MB of samples, ramped up over the first three chunks) and the
+        number of chunks in flight (2..4), whose copies overlap the fits of the others."""
+        if self._lib.PB200_SetHostPipeline(self.inst, int(rois_per_chunk), int(slots)) != 0:
+            raise ValueError("invalid host pipeline configuration")
+
     def GetKernelConfig(self):
         g, t = ct.c_int(), ct.c_int()
         self._lib.PB200_GetKernelConfig(self.inst, ct.byref(g), ct.byref(t))

@@ -77,6 +77,8 @@ def _bind_common(L):
     L.PB200_SetKernelConfig.restype = ctypes.c_int
     L.PB200_SetKernelVariant.argtypes = [vp, ctypes.c_int]
     L.PB200_SetKernelVariant.restype = ctypes.c_int
+    L.PB200_SetHostPipeline.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.PB200_SetHostPipeline.restype = ctypes.c_int
     L.PB200_GetKernelConfig.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.PB200_ModelInfo.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.PB200_ModelInfo.restype = ctypes.c_int
