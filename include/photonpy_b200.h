@@ -206,8 +206,9 @@ SpotDetectorFactory* SpotDetector_Configure(const SpotDetectorConfig* config);
 void SpotDetector_DestroyFactory(SpotDetectorFactory* factory);
 /* SpotDetector.cu:101-151: detects the spots of one host frame [height][width], returns their
  * number (at most maxSpots) and writes scores[n], spotZ[n] (0), cornerPosYX[n][2] = (y, x) -
- * roisize/2 and rois[n][roisize][roisize] (pixels clamped to the frame). calib must be NULL
- * (camera calibration is not provided). Returns 0 on error. */
+ * roisize/2 and rois[n][roisize][roisize] (pixels clamped to the frame). calib: NULL or a
+ * CameraCalibration*; as in the reference the detector sees the calibrated frame and the ROIs
+ * are cut from the frame as given. Returns 0 on error. */
 int SpotDetector_ProcessFrame(const float* frame, int width, int height, int roisize, int maxSpots, float* spotScores,
                               int* spotZ, int* cornerPosYX, float* rois, SpotDetectorFactory* sdf, void* calib);
 /* SpotDetector.cu:155-178: boxes [roiZ][roiY][roiX] at corners startposZYX[n][3] of a frame stack
@@ -215,6 +216,55 @@ int SpotDetector_ProcessFrame(const float* frame, int width, int height, int roi
  * the stack whatever the corner's z. */
 void ExtractROIs(const float* frames, int width, int height, int depth, int roiX, int roiY, int roiZ,
                  const int* startposZYX, int numspots, float* rois);
+/* ---- Camera calibration, CameraCalibration.cu:9-83 ------------------------------------
+ * Applied to every frame before detection: gain/offset v = max(0, (x - offset) * gain) (NaN kept),
+ * per-pixel gain/offset images the same, sCMOS v = (x - offset[p]) * gain[p]. Owned by ctx
+ * (destroyed with it), as in the reference. */
+typedef struct CameraCalibration CameraCalibration; /* opaque; the reference's ICalibrationProcessor */
+CameraCalibration* GainOffsetCalib_Create(float gain, float offset, Context* ctx);
+CameraCalibration* GainOffsetImageCalib_Create(int width, int height, const float* gain, const float* offset,
+                                               Context* ctx);
+CameraCalibration* sCMOS_Calib_Create(int width, int height, const float* offset, const float* gain,
+                                      const float* variance, Context* ctx);
+
+/* ---- ROI queue, ROIQueue.cpp:8-95 --------------------------------------------------------
+ * Thread-safe FIFO of ROIs [shape z][y][x] with their info. RQ_Pop takes the `count` oldest ROIs
+ * and, as the reference, writes them newest first; it writes nothing when fewer than `count` are
+ * queued. shape is zyx (Int3). */
+typedef struct ROIQueue ROIQueue; /* opaque */
+typedef struct ROIInfo {          /* photonpy/cpp/roi_queue.py ROIInfoDType */
+    int id;                       /* frame (or summed-frame) number */
+    float score;
+    int x, y, z;                  /* ROI corner; z plane of the detector */
+} ROIInfo;
+ROIQueue* RQ_Create(const int* shapeZYX, Context* ctx);
+void RQ_Pop(ROIQueue* q, int count, ROIInfo* rois, float* data);
+int RQ_Length(ROIQueue* q);
+void RQ_Push(ROIQueue* q, int count, const ROIInfo* info, const float* data);
+void RQ_SmpShape(ROIQueue* q, int* shapeZYX);
+void RQ_Delete(ROIQueue* q);
+
+/* ---- Frame processors, ImageProcessor.cpp:12-51 ----------------------------------------- */
+typedef struct ImageProcessor ImageProcessor; /* opaque */
+void ImgProc_Flush(ImageProcessor* q);
+void ImgProc_AddFrameU16(ImageProcessor* q, const uint16_t* data);
+void ImgProc_AddFrameF32(ImageProcessor* q, const float* data);
+int ImgProc_GetQueueLength(ImageProcessor* q);
+int ImgProc_ReadFrame(ImageProcessor* q, float* image, float* processed);
+int ImgProc_NumFinishedFrames(ImageProcessor* q);
+bool ImgProc_IsIdle(ImageProcessor* q);
+void ImgProc_Destroy(ImageProcessor* q);
+/* ImgFilterQueue.cu:117-346: 16-bit frames in (ImgProc_AddFrameU16), calibrated, summed in
+ * groups of sumframes = the ROI queue's z size (as in the reference, the sumframes argument is not
+ * used), spots detected on each summed frame with the factory's configuration (copied, with its
+ * background image, at creation), and ROIs [sumframes][y][x] of the calibrated frames pushed
+ * into roilist with id = summed-frame number, x/y = corner, z = 0, score. Frames are processed
+ * in batches of whatever complete groups are waiting, on the GPU, by one worker thread
+ * (numDetectionThreads is not used). ImgProc_AddFrameF32 is an error, as in the reference. */
+ImageProcessor* SpotExtractionQueue_Create(int width, int height, ROIQueue* roilist, SpotDetectorFactory* sdf,
+                                           CameraCalibration* calib, int numDetectionThreads, int sumframes,
+                                           Context* ctx);
+
 /* Extension: detection and ROI cut-out of nframes device frames [n][height][width] on a stream,
  * for feeding the fitter without host copies. d_bg: device [height][width] or NULL (the
  * configuration's host background image is not used here). Outputs (device): d_found[n] (spots
@@ -249,14 +299,11 @@ void FFT(const void* src, void* dst, int batchsize, int siglen, int forward);
 void FFT2(const void* src, void* dst, int batchsize, int sigw, int sigh, int forward);
 void DrawROIs(float* image, int width, int height, const float* rois, int numrois, int roisize, const int* roiposYX);
 void Gauss2D_Draw(double* image, int imgw, int imgh, float* spotList, int nspots, float addSigma);
-/* Bound by SpotDetectionMethods.__init__ (photonpy/cpp/spotdetect.py:117,172): the PSF-correlation
- * detector (PSFCorrelationSpotDetector.cu:13) and the threaded spot-extraction queue
- * (ImgFilterQueue.cu:346). Both return NULL. */
+/* Bound by SpotDetectionMethods.__init__ (photonpy/cpp/spotdetect.py:117): the PSF-correlation
+ * detector (PSFCorrelationSpotDetector.cu:13). Returns NULL. */
 void* PSFCorrelationSpotDetector_Configure(const float* bgImage, int imageWidth, int imageHeight,
                                            const float* psfstack, int roisize, int depth, int maxFilterSizeXY,
                                            float minPhotons, int bgFilterSize, int debugMode);
-void* SpotExtractionQueue_Create(int width, int height, void* roiQueue, void* spotDetectorFactory, void* calib,
-                                 int numThreads, int sumframes, Context* ctx);
 
 /* ---- Extensions (no reference counterpart) ------------------------------------------ */
 /* Message of the last error on this thread ("" if none); cleared by PB200_ClearError. */

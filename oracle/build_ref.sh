@@ -70,6 +70,10 @@ perl -0pi -e 's/template<typename T>(\s*)PinnedArray\(const DeviceArray<T>& src\
 perl -0pi -e 's/T x = sample\[smpIndex\] \+= readnoiseVG2\[smpIndex\];/T x = sample[smpIndex] + readnoiseVG2[smpIndex];/' Estimators/Estimation.h
 sed -i '/OneOverSqrt2PiSigma3Y = /,/ComputeInitialEstimate/{s/\bimgw\b/Width()/g}' Estimators/Gaussian/GaussianPSFModels.h
 perl -0pi -e 's/\bheight\(\)/Height()/g; s/\bwidth\(\)/Width()/g' Estimators/Gaussian/GaussianPSFModels.h
+# members of a dependent base class named without this-> (the frame-queue templates)
+perl -0pi -e 's/= GetFinishedFrame\(\);/= this->GetFinishedFrame();/; s/\tRecycleOutput\(std::move\(f\)\);/\tthis->RecycleOutput(std::move(f));/; s/auto output = GetNewOutputFrame\(\);/auto output = this->GetNewOutputFrame();/; s/\tAddToFinished\(std::move\(output\)\);/\tthis->AddToFinished(std::move(output));/; s/CopyToHost\(output->h_filtered\.data\(\), stream\)/CopyToHost(output->h_filtered.data(), this->stream)/; s/cudaStreamSynchronize\(stream\);/cudaStreamSynchronize(this->stream);/g' ImgFilterQueueImpl.h
+# a braced size that matches two DeviceImage constructors
+perl -0pi -e 's/original\(\{ imgsize\.x, imgsize\.y\*sumframes \}\)/original(imgsize.x, imgsize.y*sumframes)/' ImgFilterQueue.cu
 # the index-list generator names a predicate that SpotDetector.h defines after including it
 perl -0pi -e 's/#include "SpotIndexListGenerator.h"\n//; s/(struct SpotLocationList)/#include "SpotIndexListGenerator.h"\n\n$1/' SpotDetection/SpotDetector.h
 
@@ -78,7 +82,8 @@ FLAGS=(-x cu -std=c++17 -O3 -Xcompiler -fPIC,-fpermissive,-w,-O3 --expt-extended
        -gencode arch=compute_100a,code=sm_100a -I. -IEstimators -include msvc_compat.h -DNDEBUG)
 SRCS=(Estimators/Estimator.cpp StringUtils.cpp Context.cpp DebugImageCallback.cpp Rendering.cpp CudaUtils.cu
       Estimators/EstimatorImpl.cu Estimators/Gaussian/GaussianPSF.cu Estimators/CSpline/CubicSplinePSF.cu
-      Estimators/EstimationQueue.cpp Estimators/GLRT_PSF.cu SpotDetection/SpotDetector.cu)
+      Estimators/EstimationQueue.cpp Estimators/GLRT_PSF.cu SpotDetection/SpotDetector.cu
+      ImgFilterQueue.cu ROIQueue.cpp CameraCalibration.cu ImageProcessor.cpp)
 OBJS=()
 pids=()
 for s in "${SRCS[@]}"; do

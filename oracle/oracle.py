@@ -223,3 +223,51 @@ def detect_spots(frame, u1, u2, maxfilter, roisize, min_intensity, max_intensity
     lib().pso_cut_rois(_fptr(frame), w, h, idx.ctypes.data_as(ct.POINTER(ct.c_int32)), n, int(roisize),
                        corner.ctypes.data_as(ct.POINTER(ct.c_int32)), _fptr(rois))
     return found, idx[:n], score[:n], corner, rois
+
+
+def camera_calibrate(frames, kind=None, gain=1.0, offset=0.0):
+    """CameraCalibration.cu:19-57 restated in float32 numpy (subtract, then multiply, each
+    rounded). kind: None, "gain_offset" (scalars; negatives to 0), "image" (per-pixel arrays;
+    negatives to 0), "scmos" (per-pixel, no clamp; the intended transform, see the note on
+    photonpy's sCMOS transform in the integration notes)."""
+    x = np.asarray(frames).astype(np.float32)
+    if kind is None:
+        return x
+    g = np.asarray(gain, dtype=np.float32)
+    o = np.asarray(offset, dtype=np.float32)
+    v = (x - o).astype(np.float32) * g
+    v = v.astype(np.float32)
+    if kind in ("gain_offset", "image"):
+        v = np.where(v < 0, np.float32(0), v).astype(np.float32)
+    return v
+
+
+def spot_extraction_queue(frames_u16, u1, u2, maxfilter, det_roisize, min_intensity, max_intensity=np.inf,
+                          background=None, sumframes=1, roi_shape=None, calib=None):
+    """The spot-extraction queue restated (ImgFilterQueue.cu:117-260): 16-bit frames ->
+    calibration -> sums of sumframes frames (left to right) -> spot detection on each sum ->
+    ROI stacks [sumframes][rh][rw] of the calibrated frames (corner = centre - size/2, pixels
+    clamped). Incomplete trailing groups are not processed. Returns (info records as an array of
+    (id, score, x, y, z), rois [n, sumframes, rh, rw]) in frame order, row-major within a frame.
+    calib: None or (kind, gain, offset) for camera_calibrate."""
+    frames = np.asarray(frames_u16)
+    n, h, w = frames.shape
+    rh, rw = roi_shape if roi_shape is not None else (det_roisize, det_roisize)
+    cal = camera_calibrate(frames, *calib) if calib is not None else frames.astype(np.float32)
+    infos, stacks = [], []
+    for g in range(n // sumframes):
+        grp = cal[g * sumframes:(g + 1) * sumframes]
+        s = grp[0].copy()
+        for z in range(1, sumframes):
+            s = (s + grp[z]).astype(np.float32)
+        found, idx, score, _, _ = detect_spots(s, u1, u2, maxfilter, det_roisize, min_intensity, max_intensity,
+                                               background, max_spots=h * w)
+        for i, p in enumerate(idx):
+            cy, cx = int(p) // w - rh // 2, int(p) % w - rw // 2
+            ys = np.clip(np.arange(cy, cy + rh), 0, h - 1)
+            xs = np.clip(np.arange(cx, cx + rw), 0, w - 1)
+            stacks.append(grp[:, ys][:, :, xs])
+            infos.append((g, score[i], cx, cy, 0))
+    info = np.array(infos, dtype=[("id", "<i4"), ("score", "<f4"), ("x", "<i4"), ("y", "<i4"), ("z", "<i4")])
+    rois = np.array(stacks, dtype=np.float32).reshape(len(stacks), sumframes, rh, rw)
+    return info, rois

@@ -339,3 +339,64 @@ def spline_compute(data, border=0):
     out = np.zeros((*(np.array(data.shape) - 3 + 2 * border), 64), np.float32)
     L.CSpline_Compute(_p(shape), _p(data), _p(out), int(border))
     return out
+
+
+ROIInfoDType = np.dtype([("id", "<i4"), ("score", "<f4"), ("x", "<i4"), ("y", "<i4"), ("z", "<i4")])
+
+
+def spot_queue(frames_u16, u1, u2, maxfilter, det_roisize, min_intensity, max_intensity=np.inf, sumframes=1,
+               roisize=None, gain_offset=None, timeout=120.0):
+    """The reference's spot-extraction queue (SpotExtractionQueue_Create, ImgFilterQueue.cu:346;
+    its CUDA detector, so it needs a GPU): pushes the 16-bit frames, waits for the summed frames
+    (bounded), pops every ROI. gain_offset: None or (gain, offset) for GainOffsetCalib_Create.
+    Returns (info, rois [n, sumframes, roisize, roisize]) in the order RQ_Pop gives them."""
+    import time
+    L = lib()
+    vp = ct.c_void_p
+    frames = np.ascontiguousarray(frames_u16, dtype=np.uint16)
+    n, h, w = frames.shape
+    rs = int(roisize or det_roisize)
+    L.RQ_Create.argtypes = [vp, vp]
+    L.RQ_Create.restype = vp
+    L.RQ_Length.argtypes = [vp]
+    L.RQ_Length.restype = ct.c_int
+    L.RQ_Pop.argtypes = [vp, ct.c_int, vp, vp]
+    L.SpotExtractionQueue_Create.argtypes = [ct.c_int, ct.c_int, vp, vp, vp, ct.c_int, ct.c_int, vp]
+    L.SpotExtractionQueue_Create.restype = vp
+    L.ImgProc_AddFrameU16.argtypes = [vp, vp]
+    L.ImgProc_NumFinishedFrames.argtypes = [vp]
+    L.ImgProc_NumFinishedFrames.restype = ct.c_int
+    L.GainOffsetCalib_Create.argtypes = [ct.c_float, ct.c_float, vp]
+    L.GainOffsetCalib_Create.restype = vp
+    L.ImgProc_Destroy.argtypes = [vp]
+    ctx = L.Context_Create()
+    q = None
+    try:
+        shape = np.array([sumframes, rs, rs], np.int32)
+        rq = L.RQ_Create(shape.ctypes.data, ctx)
+        cfg = SpotDetectorConfig(int(u1), int(u2), int(maxfilter), int(det_roisize), float(min_intensity),
+                                 float(max_intensity), None)
+        sdf = L.SpotDetector_Configure(ct.byref(cfg))
+        calib = None
+        if gain_offset is not None:
+            calib = L.GainOffsetCalib_Create(float(gain_offset[0]), float(gain_offset[1]), ctx)
+        q = L.SpotExtractionQueue_Create(w, h, rq, sdf, calib, 2, sumframes, ctx)
+        L.SpotDetector_DestroyFactory(sdf)
+        for f in range(n):
+            L.ImgProc_AddFrameU16(q, frames[f].ctypes.data)
+        t0 = time.time()
+        while L.ImgProc_NumFinishedFrames(q) < n // sumframes:
+            if time.time() - t0 > timeout:
+                raise TimeoutError("reference spot-extraction queue did not finish")
+            time.sleep(0.01)
+        time.sleep(0.05)
+        cnt = L.RQ_Length(rq)
+        info = np.zeros(cnt, ROIInfoDType)
+        rois = np.zeros((cnt, sumframes, rs, rs), np.float32)
+        if cnt:
+            L.RQ_Pop(rq, cnt, info.ctypes.data, rois.ctypes.data)
+        return info, rois
+    finally:
+        if q:
+            L.ImgProc_Destroy(q)  # the queue before the ROI queue it fills
+        L.Context_Destroy(ctx)

@@ -21,9 +21,9 @@ LIB_DIR = os.path.join(PKG, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libphotonpy_b200.so")
 OBJ_DIR = os.path.join(PKG, "_build")
 
-UNITS = ["estimator.cu", "estim_queue.cu", "spot_detect.cu", "probes.cu", "k_xyibg.cu", "k_constsigma.cu", "k_sigma.cu", "k_sigmaxy.cu",
+UNITS = ["estimator.cu", "estim_queue.cu", "spot_detect.cu", "spot_queue.cu", "probes.cu", "k_xyibg.cu", "k_constsigma.cu", "k_sigma.cu", "k_sigmaxy.cu",
          "k_astig.cu", "k_spline.cu", "k_tilted.cu", "k_mixed.cu"]
-HEADERS = ["host_internal.h", "models.cuh", "fit_kernels.cuh", "fit_common.cuh", "gauss_fit.cuh", "launch.cuh", "mixed.cuh", "adjoint.cuh"]
+HEADERS = ["host_internal.h", "spot_internal.h", "models.cuh", "fit_kernels.cuh", "fit_common.cuh", "gauss_fit.cuh", "launch.cuh", "mixed.cuh", "adjoint.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -98,6 +98,13 @@ private:
     size_t held_ = 0;
 };
 
+}  // namespace
+
+void* pb200::pinned_take(size_t bytes) { return PinnedCache::get().take(bytes); }
+void pb200::pinned_give(void* p, size_t bytes) { PinnedCache::get().give(p, bytes); }
+
+namespace {
+
 // One pinned allocation split into consecutive 256-byte aligned arrays of the given sizes.
 struct PinnedBlock {
     void* mem = nullptr;

@@ -186,20 +186,31 @@ struct Estimator;
 struct Context {
     std::mutex mtx;
     std::unordered_set<Estimator*> objects;
-    std::unordered_map<void*, void (*)(void*)> owned;  // queues and other non-estimator objects
+    // queues and other non-estimator objects, in registration order (destroyed newest first:
+    // a frame queue goes before the ROI queue it fills)
+    std::vector<std::pair<void*, void (*)(void*)>> owned;
 };
 
 namespace pb200 {
 void context_attach(Context* ctx, void* obj, void (*destroy)(void*)) {
     if (!ctx) return;
     std::lock_guard<std::mutex> g(ctx->mtx);
-    ctx->owned[obj] = destroy;
+    for (auto& o : ctx->owned)
+        if (o.first == obj) {
+            o.second = destroy;
+            return;
+        }
+    ctx->owned.push_back({obj, destroy});
 }
 
 void context_detach(Context* ctx, void* obj) {
     if (!ctx) return;
     std::lock_guard<std::mutex> g(ctx->mtx);
-    ctx->owned.erase(obj);
+    for (size_t i = 0; i < ctx->owned.size(); i++)
+        if (ctx->owned[i].first == obj) {
+            ctx->owned.erase(ctx->owned.begin() + (long)i);
+            return;
+        }
 }
 
 void set_last_error(const std::string& msg) {
@@ -758,7 +769,7 @@ void Context_Destroy(Context* ctx) {
         std::lock_guard<std::mutex> g(ctx->mtx);
         objs.assign(ctx->objects.begin(), ctx->objects.end());
         ctx->objects.clear();
-        owned.assign(ctx->owned.begin(), ctx->owned.end());
+        owned.assign(ctx->owned.rbegin(), ctx->owned.rend());  // newest first
         ctx->owned.clear();
     }
     for (auto& o : owned) o.second(o.first);  // queues first: they use the estimators
@@ -1429,10 +1440,6 @@ void DrawROIs(float*, int, int, const float*, int, int, const int*) { not_provid
 void Gauss2D_Draw(double*, int, int, float*, int, float) { not_provided("Gauss2D_Draw"); }
 void* PSFCorrelationSpotDetector_Configure(const float*, int, int, const float*, int, int, int, float, int, int) {
     not_provided("PSFCorrelationSpotDetector_Configure");
-    return nullptr;
-}
-void* SpotExtractionQueue_Create(int, int, void*, void*, void*, int, int, Context*) {
-    not_provided("SpotExtractionQueue_Create");
     return nullptr;
 }
 // GaussianPSF.cu:216-240: intensity and background of each spot at a known position xy[i]

@@ -1,5 +1,6 @@
 // Host-side services of estimator.cu shared with the other host translation units.
 #pragma once
+#include <cstddef>
 #include <string>
 
 struct Context;
@@ -11,6 +12,11 @@ namespace pb200 {
 // object is not registered.
 void context_attach(Context* ctx, void* obj, void (*destroy)(void*));
 void context_detach(Context* ctx, void* obj);
+
+// Pinned host blocks from a process-wide cache (blocks of deleted queues are kept for the next
+// one, up to 2 GB). give() takes back exactly what take() handed out.
+void* pinned_take(size_t bytes);
+void pinned_give(void* p, size_t bytes);
 
 // Records `msg` as this thread's last error (PB200_GetLastError) and prints it through the
 // debug-print callback.

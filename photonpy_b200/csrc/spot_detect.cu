@@ -31,6 +31,7 @@
 
 #include "../../include/photonpy_b200.h"
 #include "host_internal.h"
+#include "spot_internal.h"
 
 namespace {
 
@@ -129,8 +130,6 @@ __device__ __forceinline__ void box_strip(const FilterParams& p, const float (&v
                                           float (&o1)[4], float (&o2)[4]) {
     constexpr int off1 = U2 / 2 - U1 / 2;  // the u1 window starts off1 samples into the u2 window
     const bool interior = g0 - U2 / 2 >= 0 && g0 + 3 - U2 / 2 + U2 <= extent;  // u1 windows lie inside
-    float S1[4], S2[4];
-    int C1[4], C2[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         float s1 = 0.0f, s2 = 0.0f;
@@ -146,33 +145,8 @@ __device__ __forceinline__ void box_strip(const FilterParams& p, const float (&v
             c1 = clampi(c1, 1, kMaxWindow);  // outside the line the value is unused
             c2 = clampi(c2, 1, kMaxWindow);
         }
-        S1[j] = s1;
-        S2[j] = s2;
-        C1[j] = c1;
-        C2[j] = c2;
-    }
-    // pb200_count_div for all eight quotients, with one branch to the IEEE division when any of
-    // them is out of the corrected range
-    float q1[4], q2[4];
-    bool ok = true;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        q1[j] = __fmul_rn(S1[j], p.rcp[C1[j]]);
-        q2[j] = __fmul_rn(S2[j], p.rcp[C2[j]]);
-        ok = ok && count_div_in_range(q1[j]) && count_div_in_range(q2[j]);
-    }
-    if (ok) {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            o1[j] = count_div_corrected(S1[j], q1[j], (float)C1[j], p.rcp[C1[j]]);
-            o2[j] = count_div_corrected(S2[j], q2[j], (float)C2[j], p.rcp[C2[j]]);
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            o1[j] = __fdiv_rn(S1[j], (float)C1[j]);
-            o2[j] = __fdiv_rn(S2[j], (float)C2[j]);
-        }
+        o1[j] = pb200_count_div(s1, (float)c1, p.rcp[c1]);
+        o2[j] = pb200_count_div(s2, (float)c2, p.rcp[c2]);
     }
 }
 
@@ -626,7 +600,7 @@ struct DevMem {
 struct SpotDetectorFactory {
     SpotDetectorConfig cfg;
     std::mutex mtx;
-    DevMem frame, bg, found, scoreOut, corner, rois;      // ProcessFrame
+    DevMem frame, calibFrame, bg, found, scoreOut, corner, rois;  // ProcessFrame
     DevMem mask, score, counts, index, scoreTmp;          // scratch of every call
     cudaEvent_t scratchDone = nullptr;
     ~SpotDetectorFactory() {
@@ -673,10 +647,12 @@ const void* filter_kernel_for(int u1, int u2) {
 }
 
 // Runs the four kernels for `n` frames already on the device, on stream s, with the factory's
-// scratch; the caller holds sdf->mtx. Outputs: found[n], scoreOut[n][maxSpots] (optional), and
-// (when rois is set) corner[n][maxSpots][2] + rois[n][maxSpots][roisize][roisize].
+// scratch; the caller holds sdf->mtx. Outputs: found[n], scoreOut[n][maxSpots] (optional),
+// indexOut[n][maxSpots] (optional; pixel indices), and (when rois is set) corner[n][maxSpots][2]
+// + rois[n][maxSpots][roisize][roisize], cut from d_cutFrames (d_frames when null).
 void detect_run(SpotDetectorFactory* sdf, const float* d_frames, const float* d_bg, int n, int w, int h, int roisize,
-                int maxSpots, int* d_found, float* d_scoreOut, int* d_corner, float* d_rois, cudaStream_t s) {
+                int maxSpots, int* d_found, float* d_scoreOut, int* d_corner, float* d_rois, cudaStream_t s,
+                int* d_indexOut = nullptr, const float* d_cutFrames = nullptr) {
     const SpotDetectorConfig& c = sdf->cfg;
     check_config(c);
     if (n > 65535) throw SpotError("spot detection: at most 65535 frames per call");
@@ -686,7 +662,8 @@ void detect_run(SpotDetectorFactory* sdf, const float* d_frames, const float* d_
     const size_t npix = (size_t)w * h;
     // grow the scratch only after the previous call's kernels are done with it
     const size_t need[5] = {sizeof(unsigned) * nw * n, sizeof(float) * npix * n, sizeof(int) * (size_t)nseg * n,
-                            sizeof(int) * (size_t)maxSpots * n, d_scoreOut ? 0 : sizeof(float) * (size_t)maxSpots * n};
+                            d_indexOut ? 0 : sizeof(int) * (size_t)maxSpots * n,
+                            d_scoreOut ? 0 : sizeof(float) * (size_t)maxSpots * n};
     DevMem* bufs[5] = {&sdf->mask, &sdf->score, &sdf->counts, &sdf->index, &sdf->scoreTmp};
     bool grow = false;
     for (int i = 0; i < 5; i++) grow |= need[i] > bufs[i]->bytes;
@@ -697,6 +674,7 @@ void detect_run(SpotDetectorFactory* sdf, const float* d_frames, const float* d_
     }
     PBS_CUDA(cudaStreamWaitEvent(s, sdf->scratchDone, 0));
     float* scoreOut = d_scoreOut ? d_scoreOut : sdf->scoreTmp.as<float>();
+    int* index = d_indexOut ? d_indexOut : sdf->index.as<int>();
 
     FilterParams p{};
     p.frames = d_frames;
@@ -742,18 +720,31 @@ void detect_run(SpotDetectorFactory* sdf, const float* d_frames, const float* d_
     detect_count_kernel<<<dim3(nseg, n), kSegThreads, 0, s>>>(p.mask, nw, nseg, sdf->counts.as<int>());
     PBS_CUDA(cudaGetLastError());
     detect_emit_kernel<<<dim3(nseg, n), kSegThreads, 0, s>>>(p.mask, p.score, w, ntx, nw, nseg,
-                                                             sdf->counts.as<int>(), maxSpots, d_found,
-                                                             sdf->index.as<int>(), scoreOut);
+                                                             sdf->counts.as<int>(), maxSpots, d_found, index,
+                                                             scoreOut);
     PBS_CUDA(cudaGetLastError());
     if (d_rois) {
         const long long tasks = (long long)n * maxSpots;
         const int blocks = (int)std::min<long long>((tasks + 7) / 8, 1 << 30);
-        cut_rois_kernel<<<blocks, 256, 0, s>>>(d_frames, w, h, roisize, maxSpots, n, d_found, sdf->index.as<int>(),
-                                               d_corner, d_rois);
+        cut_rois_kernel<<<blocks, 256, 0, s>>>(d_cutFrames ? d_cutFrames : d_frames, w, h, roisize, maxSpots, n,
+                                               d_found, index, d_corner, d_rois);
         PBS_CUDA(cudaGetLastError());
     }
     PBS_CUDA(cudaEventRecord(sdf->scratchDone, s));
 }
+
+}  // namespace
+
+const SpotDetectorConfig* pb200::spot_factory_config(const SpotDetectorFactory* sdf) { return &sdf->cfg; }
+
+void pb200::spot_detect_indices(SpotDetectorFactory* sdf, const float* d_frames, const float* d_bg, int n, int w,
+                                int h, int maxSpots, int* d_found, int* d_index, float* d_score, cudaStream_t s) {
+    std::lock_guard<std::mutex> g(sdf->mtx);
+    detect_run(sdf, d_frames, d_bg, n, w, h, sdf->cfg.roisize, maxSpots, d_found, d_score, nullptr, nullptr, s,
+               d_index);
+}
+
+namespace {
 
 template <class F, class R>
 R spot_guarded(F&& f, R fallback) {
@@ -788,7 +779,6 @@ int SpotDetector_ProcessFrame(const float* frame, int width, int height, int roi
         [&]() -> int {
             if (!frame || !sdf || width <= 0 || height <= 0 || maxSpots < 0 || roisize < 1)
                 throw SpotError("SpotDetector_ProcessFrame: bad arguments");
-            if (calib) throw SpotError("SpotDetector_ProcessFrame: camera calibration is not provided by photonpy_b200");
             std::lock_guard<std::mutex> g(sdf->mtx);
             const size_t npix = (size_t)width * height;
             const int cap = std::max(maxSpots, 1);
@@ -804,10 +794,20 @@ int SpotDetector_ProcessFrame(const float* frame, int width, int height, int roi
                 PBS_CUDA(cudaMemcpy(sdf->bg.p, sdf->cfg.backgroundImage, sizeof(float) * npix, cudaMemcpyHostToDevice));
                 d_bg = sdf->bg.as<float>();
             }
+            // with a camera calibration the detector sees the calibrated frame, while the ROIs are
+            // cut from the frame as given (SpotDetector.cu:104-106, 141)
+            const float* d_det = sdf->frame.as<float>();
+            if (calib) {
+                sdf->calibFrame.ensure(sizeof(float) * npix);
+                pb200::camera_calib_apply_f32(static_cast<const CameraCalibration*>(calib), sdf->frame.as<float>(),
+                                              sdf->calibFrame.as<float>(), width, height, 1, 0);
+                d_det = sdf->calibFrame.as<float>();
+            }
             // the reference cuts ROIs of the ProcessFrame call's own roisize, but tests the border
             // with the configuration's
-            detect_run(sdf, sdf->frame.as<float>(), d_bg, 1, width, height, roisize, cap, sdf->found.as<int>(),
-                       sdf->scoreOut.as<float>(), sdf->corner.as<int>(), sdf->rois.as<float>(), 0);
+            detect_run(sdf, d_det, d_bg, 1, width, height, roisize, cap, sdf->found.as<int>(),
+                       sdf->scoreOut.as<float>(), sdf->corner.as<int>(), sdf->rois.as<float>(), 0, nullptr,
+                       sdf->frame.as<float>());
             int found = 0;
             PBS_CUDA(cudaMemcpy(&found, sdf->found.p, sizeof(int), cudaMemcpyDeviceToHost));
             const int n = std::min(found, maxSpots);

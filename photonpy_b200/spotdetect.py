@@ -7,8 +7,9 @@ of frames already on the GPU (torch tensors) and returns ROIs on the GPU, ready 
 ``Estimator.EstimateDevice``. ``localize_frames`` chains the two: frames in, localizations out,
 with nothing but the frames crossing PCIe.
 
-Not provided: the PSF-correlation detector and the threaded spot-extraction queue
-(``CreateQueue``), which need photonpy's camera-calibration and image-queue machinery.
+``CreateQueue`` builds photonpy's spot-extraction queue (16-bit frames in, ROIs of summed
+frames out through a ``ROIQueue``), run in GPU batches. Not provided: the PSF-correlation
+detector.
 """
 from __future__ import annotations
 
@@ -131,6 +132,10 @@ class SpotDetectionMethods:
             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
             ctl.ndpointer(np.int32, flags="aligned, c_contiguous"), ctypes.c_int32,
             ctl.ndpointer(np.float32, flags="aligned, c_contiguous")]
+        self._SpotExtractionQueue_Create = lib.SpotExtractionQueue_Create
+        self._SpotExtractionQueue_Create.argtypes = [ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32,
+                                                     ctypes.c_int32, vp]
+        self._SpotExtractionQueue_Create.restype = vp
         self._DetectDevice = lib.PB200_DetectSpotsDevice
         self._DetectDevice.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, vp, vp, vp, vp, vp]
@@ -149,11 +154,28 @@ class SpotDetectionMethods:
         check_error("ExtractROIs")
         return rois
 
+    def CreateQueue(self, imgshape, roishape, spotDetectorType, calib=None, sumframes=1, numThreads=3, ctx=None):
+        """photonpy/cpp/spotdetect.py:178-203: a spot-detection queue. Returns (input_queue,
+        output_queue): an ImageProcessor taking 16-bit frames and the ROIQueue of
+        [sumframes, *roishape] ROIs it fills."""
+        from .image_proc import ImageProcessor
+        from .roi_queue import ROIQueue
+        if ctx is None:
+            ctx = self.ctx
+        rq = ROIQueue([sumframes, *roishape], ctx)
+        with spotDetectorType.CreateNativeFactory(self.ctx) as sdf:
+            inst = self._SpotExtractionQueue_Create(imgshape[1], imgshape[0], rq.inst, sdf.inst,
+                                                    calib.inst if calib else None, numThreads, sumframes,
+                                                    ctx.inst if ctx else None)
+        if not inst:
+            check_error("SpotExtractionQueue_Create")
+        return ImageProcessor(imgshape, inst, self.ctx), rq
+
     def ProcessFrame(self, image, spotDetector, roisize, maxSpotsPerFrame, calib=None):
-        """photonpy/cpp/spotdetect.py:224-245: returns (rois, cornerYX, scores, spotz)."""
+        """photonpy/cpp/spotdetect.py:224-245: returns (rois, cornerYX, scores, spotz). With a
+        camera calibration the detector sees the calibrated frame; the ROIs hold the frame as
+        given."""
         assert len(image.shape) == 2
-        if calib is not None:
-            raise NotImplementedError("camera calibration is not provided by photonpy_b200")
         h, w = image.shape
         image = np.ascontiguousarray(image, dtype=np.float32)
         scores = np.zeros(maxSpotsPerFrame, dtype=np.float32)
@@ -162,7 +184,7 @@ class SpotDetectionMethods:
         spotz = np.zeros(maxSpotsPerFrame, dtype=np.int32)
         with spotDetector.CreateNativeFactory(self.ctx) as sdf:
             numspots = self._SpotDetector_ProcessFrame(image, w, h, roisize, maxSpotsPerFrame, scores, spotz, cornerYX,
-                                                       rois, sdf.inst, None)
+                                                       rois, sdf.inst, calib.inst if calib else None)
         check_error("SpotDetector_ProcessFrame")
         return rois[:numspots], cornerYX[:numspots], scores[:numspots], spotz[:numspots]
 
