@@ -309,9 +309,10 @@ void* PSFCorrelationSpotDetector_Configure(const float* bgImage, int imageWidth,
 /* Message of the last error on this thread ("" if none); cleared by PB200_ClearError. */
 const char* PB200_GetLastError(void);
 void PB200_ClearError(void);
-/* Fused localization: LM fit + Fisher/CRLB + chi-square in one launch (what photonpy's
- * EstimationQueue runs as Estimate followed by ChiSquareAndCRLB, EstimationQueue.cpp:285-289).
- * Host pointers; large batches are pipelined in chunks over two CUDA streams. */
+/* Localization in one call: LM fit, Fisher/CRLB + chi-square at the fitted parameters (what
+ * photonpy's EstimationQueue runs as Estimate followed by ChiSquareAndCRLB,
+ * EstimationQueue.cpp:285-289), as three launches per chunk (LM, Fisher pass, FP64 inverse) on
+ * one stream. Host pointers; large batches are pipelined in chunks over four CUDA streams. */
 void PB200_EstimateCRLB(Estimator* e, int numspots, const float* sample, const float* constants,
                         const float* initial, float* params, int* iterations, float* crlb, float* chisq);
 /* Device-pointer variants on a caller stream (cudaStream_t as void*; NULL = legacy default).
