@@ -183,9 +183,15 @@ __device__ __forceinline__ void map_virtual(const float (&av)[NV], float (&acc)[
     }
 }
 
+// Which passes a kernel instance contains: both (the mixed-batch kernel), the LM fit only, or
+// the Fisher/CRLB (+ GLRT) pass only. The standalone launches use the single-pass instances:
+// without the other pass's code and registers they run faster (the host issues the LM launch,
+// then the Fisher launch at the fitted parameters).
+enum FitPass { PASS_BOTH = 0, PASS_LM = 1, PASS_FISHER = 2 };
+
 // Fit the ROIs roi, roi + roiStep, ... < roiEnd of one (model, ROI size) with one group of G
 // lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_floats floats).
-template <class M, int G, int CPL>
+template <class M, int G, int CPL, int PASS = PASS_BOTH>
 __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArgs& a, int roi, const int roiEnd,
                                                 const int roiStep, float* spix, const int lane, const unsigned mask) {
     constexpr int K = M::K;
@@ -200,7 +206,9 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
     float4* ytab = reinterpret_cast<float4*>(aux);
     float* fisherScratch = (npix4 >= 4 * K * K) ? spix : aux;
     const int c0 = lane * CPL;
-    const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
+    constexpr bool kLM = PASS != PASS_FISHER, kFisher = PASS != PASS_LM;
+    const bool fisherOnly = PASS == PASS_FISHER || (PASS == PASS_BOTH && (a.flags & FIT_CRLB_ONLY) != 0);
+    const bool wantFisher = kFisher && (a.crlb || a.glrt);
     const bool haveSmp = a.smp != nullptr;
     const bool glrt = a.glrt != nullptr;  // needs samples (checked by the host)
     const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
@@ -255,7 +263,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
             it = 0;
             rescuedAny = false;
             if (fisherOnly) mode = MODE_FISHER;
-            else if (a.maxIter <= 0) mode = (a.crlb || a.glrt) ? MODE_FISHER : MODE_SKIP;
+            else if (a.maxIter <= 0) mode = wantFisher ? MODE_FISHER : MODE_SKIP;
             else mode = MODE_LM;
         }
         // The groups of a warp leave together: a group without ROIs idles until its warp-mates
@@ -288,7 +296,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
             float av[NV];
 #pragma unroll
             for (int q = 0; q < NV; q++) av[q] = 0.0f;
-            const bool lm = (mode == MODE_LM);
+            const bool lm = kLM && (!kFisher || mode == MODE_LM);
             if (c0 < R) {
                 for (int y = 0; y < R; y++) {
                     const float4 Y = ytab[y];
@@ -376,7 +384,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                     }
                 }
                 if (!done) continue;
-                if (a.crlb || a.glrt) {
+                if (wantFisher) {
                     mode = MODE_FISHER;
                     continue;
                 }
@@ -423,13 +431,13 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
 
 
 // Standalone launch: every group of the grid strides over the whole batch.
-template <class M, int G, int CPL>
+template <class M, int G, int CPL, int PASS>
 __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const FitArgs a) {
     extern __shared__ __align__(16) float sm[];
     const int lane = threadIdx.x & (G - 1);
     const int gib = threadIdx.x / G;
     const int gpb = blockDim.x / G;
-    gauss_fit_range<M, G, CPL>(d, a, blockIdx.x * gpb + gib, a.n, gridDim.x * gpb, sm + gib * a.smemStride, lane,
+    gauss_fit_range<M, G, CPL, PASS>(d, a, blockIdx.x * gpb + gib, a.n, gridDim.x * gpb, sm + gib * a.smemStride, lane,
                                group_mask<G>());
 }
 

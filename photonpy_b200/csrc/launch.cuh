@@ -71,11 +71,34 @@ void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t
     launch_groups(fit_kernel<M, G>, G, threads, group_smem_floats<M>(d.roisize), a.n, d, a, s);
 }
 
+// LM launch, then (when CRLB or GLRT values are requested) the Fisher launch at the fitted
+// parameters, each with its single-pass kernel instance.
 template <class M, int G, int CPL>
 void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
     if (a.n <= 0) return;
-    launch_groups(gauss_fit_kernel<M, G, CPL>, G, threads, gauss_group_floats<M::K>(d.roisize), a.n,
-                  d, a, s);
+    const int stride = gauss_group_floats<M::K>(d.roisize);
+    if (a.flags & FIT_CRLB_ONLY) {
+        launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, a, s);
+        return;
+    }
+    FitArgs lm = a;
+    lm.crlb = nullptr;
+    lm.fisher = nullptr;
+    lm.glrt = nullptr;
+    lm.glrtMeanRoi = nullptr;
+    lm.chisq = nullptr;
+    launch_groups(gauss_fit_kernel<M, G, CPL, PASS_LM>, G, threads, stride, a.n, d, lm, s);
+    if (a.crlb || a.glrt) {
+        FitArgs fi = a;
+        fi.flags |= FIT_CRLB_ONLY;
+        fi.initial = a.params;
+        fi.params = nullptr;
+        fi.iterations = nullptr;
+        fi.trace = nullptr;
+        fi.traceLen = 0;
+        fi.diag = nullptr;
+        launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, fi, s);
+    }
 }
 
 template <class M, int G>
