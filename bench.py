@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sigmaxy", choices=["sigmaxy", "xyibg", "astig", "spline", "mixed", "frames"])
-    ap.add_argument("--tile", type=int, default=8, help="mixed workload: ROIs per tile")
+    ap.add_argument("--tile", type=int, default=1, help="mixed workload: ROIs a group takes per claim")
     ap.add_argument("--n", type=int, default=None, help="ROIs per GPU (default: the workload's size)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")

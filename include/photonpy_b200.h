@@ -342,13 +342,16 @@ int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, c
                             float* d_nll, float* d_dparams, float* d_dcalib, void* stream);
 /* Mixed batches (no reference counterpart; photonpy runs one estimator, i.e. one model and
  * ROI size, per call). A plan binds nbuckets (estimator, count, device buffers) groups; one
- * run fits all of them in a single persistent launch in which warps claim tiles of tileRois
- * ROIs of one bucket from a counter, followed by the FP64 CRLB kernels. Buckets must be
- * Gaussian models with ROI size <= 16. d_constants/d_iterations/d_crlb/d_chisq arrays (and
- * their entries) may be NULL. The plan owns its scratch (task table, tile counter, Fisher
- * rows). threadsPerBlock selects the kernel's register budget: 128 (3 blocks per SM),
- * 256 (2 blocks per SM), 129 (128 threads, 4 blocks per SM). PB200_MixedPlanCapture records one run into a CUDA graph on `stream` (non-default);
- * later PB200_MixedPlanRun calls replay it. Runs of one plan must not overlap. */
+ * run fits all of them with two persistent launches (the LM pass over every bucket, then the
+ * Fisher/CRLB pass at the fitted parameters) and the FP64 CRLB kernels. In each launch a warp
+ * walks the buckets in order and its ROI groups take tileRois consecutive ROIs of the current
+ * bucket per claim from the bucket's counter. Buckets must be Gaussian models with ROI size
+ * <= 16. d_constants/d_iterations/d_crlb/d_chisq arrays (and their entries) may be NULL. The
+ * plan owns its scratch (task tables, ROI counters, Fisher rows). threadsPerBlock selects the
+ * kernel's register budget: 128 (3 blocks per SM), 256 (2 blocks per SM), 129 (128 threads,
+ * 4 blocks per SM). PB200_MixedPlanCapture records one run into a CUDA graph on `stream`
+ * (non-default); later PB200_MixedPlanRun calls replay it. Runs of one plan must not overlap.
+ * PB200_MixedPlanInfo's totalTiles is the number of claims, sum of ceil(count / tileRois). */
 MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int* counts, const float* const* d_samples,
                                  const float* const* d_constants, float* const* d_params, int* const* d_iterations,
                                  float* const* d_crlb, float* const* d_chisq, int tileRois, int threadsPerBlock);

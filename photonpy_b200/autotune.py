@@ -3,7 +3,7 @@
 For one estimator (model, ROI size, LM settings) it times the fused fit + CRLB over the
 candidate kernel configurations — kernel family (column-blocked / generic table), lanes per
 ROI (4, 8, 16, 32) and threads per block — on a batch of device-resident ROIs and keeps the
-fastest. For a MixedBatch it tunes the tile size (ROIs per warp claim) and the kernel's
+fastest. For a MixedBatch it tunes the claim size (ROIs a group takes per claim) and the kernel's
 register budget. Results are cached per GPU model in a JSON file
 (``$PB200_AUTOTUNE_CACHE`` or ``~/.cache/photonpy_b200/autotune.json``) so later runs apply
 them without timing.
@@ -150,7 +150,7 @@ def tune_estimator(est, samples=None, constants=None, n=65536, reps=3, use_cache
     return dict(config=(v, g, t), ms=ms, timings={str(k): ms_ for k, ms_ in timings.items()}, cached=False)
 
 
-def tune_mixed(buckets, tiles=(8, 16, 32, 64), budgets=(256, 129, 128), reps=3):
+def tune_mixed(buckets, tiles=(1, 2, 4, 8), budgets=(256, 129, 128), reps=3):
     """Time MixedBatch tile sizes and register budgets for these buckets; returns
     dict(tile=..., threads=..., ms=..., timings={...}) (the caller builds its MixedBatch with them)."""
     import torch

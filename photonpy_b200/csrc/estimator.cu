@@ -343,35 +343,14 @@ struct Chunking {
 };
 
 // The LM fit, then, when CRLB or GLRT values are requested, the Fisher pass at the fitted
-// parameters as a launch of its own (FIT_CRLB_ONLY, parameters from the fit's output). The fit
-// kernel could run the Fisher pass itself as a ROI's last trip, but then the groups of a warp
-// that are still iterating wait for it and the LM kernel carries its registers: for 1M SigmaXY
-// ROIs of 16x16 the fused kernel took 31.9 ms, the LM-only launch 26.3 ms and the Fisher launch
-// 1.0 ms (same results bit for bit). The Fisher launch reads the samples once more from HBM.
-void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) {
-    FitLaunch fl = e->fit_launch();
-    const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
-    if (fisherOnly || !(a.crlb || a.glrt)) {
-        fl(e->desc, a, e->threads, s);
-        return;
-    }
-    FitArgs lm = a;
-    lm.crlb = nullptr;
-    lm.fisher = nullptr;
-    lm.glrt = nullptr;
-    lm.glrtMeanRoi = nullptr;
-    lm.chisq = nullptr;
-    fl(e->desc, lm, e->threads, s);
-    FitArgs fi = a;
-    fi.flags |= FIT_CRLB_ONLY;
-    fi.initial = a.params;
-    fi.params = nullptr;
-    fi.iterations = nullptr;
-    fi.trace = nullptr;
-    fi.traceLen = 0;
-    fi.diag = nullptr;
-    fl(e->desc, fi, e->threads, s);
-}
+// parameters as a launch of its own (the model launchers in launch.cuh split a request into an
+// LM launch and a FIT_CRLB_ONLY launch, each with a kernel instance compiled for that pass).
+// The fit kernel could run the Fisher pass itself as a ROI's last trip, but then the groups of a
+// warp that are still iterating wait for it and the LM code carries its registers: for 1M
+// SigmaXY ROIs of 16x16 that fused form took 31.9 ms, the split 27.3 ms, and the single-pass
+// instances 24.4 ms, with the same results bit for bit. The Fisher launch reads the samples once
+// more from HBM.
+void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) { e->fit_launch()(e->desc, a, e->threads, s); }
 
 // Host-pointer fit through the slot pipeline: H2D(c) + kernel(c) on slot c % slots are issued
 // before D2H(c - slots + 1), so the copies of one chunk overlap the fits of the others.
@@ -1190,7 +1169,8 @@ struct MixedPlan {
     int ntasks = 0, totalTiles = 0, tileRois = 32, variant = 0, strideFloats = 0;
     std::vector<MixedTask> tasks;
     std::vector<int> K;
-    DevBuf dTasks, dCounter, dFisher;
+    DevBuf dTasks, dTasksFisher, dCounter, dFisher;  // dCounter: per-bucket ROI counters of the two passes
+    bool anyFisher = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
     ~MixedPlan() {
@@ -1200,10 +1180,15 @@ struct MixedPlan {
 };
 
 namespace {
+// The LM pass over every bucket, then the Fisher pass at the fitted parameters (buckets without
+// a CRLB request have no ROIs in it), then the FP64 CRLB of each bucket.
 void mixed_enqueue(MixedPlan* p, cudaStream_t s) {
-    PB_CUDA(cudaMemsetAsync(p->dCounter.p, 0, sizeof(int), s));
+    PB_CUDA(cudaMemsetAsync(p->dCounter.p, 0, 2 * sizeof(int) * p->ntasks, s));
     launch_mixed(p->dTasks.as<MixedTask>(), p->ntasks, p->totalTiles, p->tileRois, p->dCounter.as<int>(),
-                 p->strideFloats, p->variant, s);
+                 p->strideFloats, p->variant, false, s);
+    if (p->anyFisher)
+        launch_mixed(p->dTasksFisher.as<MixedTask>(), p->ntasks, p->totalTiles, p->tileRois,
+                     p->dCounter.as<int>() + p->ntasks, p->strideFloats, p->variant, true, s);
     for (int b = 0; b < p->ntasks; b++) {
         const FitArgs& a = p->tasks[b].a;
         if (a.crlb) launch_crlb(p->K[b], a.fisher, a.crlb, a.chisq, a.n, s);
@@ -1263,7 +1248,6 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                         a.fisher = p->dFisher.as<float>() + off;
                         off += (size_t)fisher_row_floats(e->K) * counts[b];
                     }
-                    t.tileBegin = p->totalTiles;
                     const int cpl = (e->desc.roisize + G - 1) / G;
                     t.handler = e->desc.model * 4 + cpl - 1;
                     p->totalTiles += (counts[b] + tileRois - 1) / tileRois;
@@ -1276,11 +1260,22 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     p->K.push_back(e->K);
                 }
                 p->ntasks = (int)p->tasks.size();
+                std::vector<MixedTask> lmTasks(p->tasks), fiTasks(p->tasks);
+                for (int b = 0; b < p->ntasks; b++) {
+                    lmTasks[b].a = lm_pass_args(p->tasks[b].a);
+                    fiTasks[b].a = fisher_pass_args(p->tasks[b].a);
+                    if (!p->tasks[b].a.crlb) fiTasks[b].a.n = 0;  // its tiles end at once
+                    else p->anyFisher = true;
+                }
                 p->dTasks.ensure(sizeof(MixedTask) * std::max(1, p->ntasks));
-                if (p->ntasks)
-                    PB_CUDA(cudaMemcpy(p->dTasks.p, p->tasks.data(), sizeof(MixedTask) * p->ntasks,
+                p->dTasksFisher.ensure(sizeof(MixedTask) * std::max(1, p->ntasks));
+                if (p->ntasks) {
+                    PB_CUDA(cudaMemcpy(p->dTasks.p, lmTasks.data(), sizeof(MixedTask) * p->ntasks,
                                        cudaMemcpyHostToDevice));
-                p->dCounter.ensure(sizeof(int));
+                    PB_CUDA(cudaMemcpy(p->dTasksFisher.p, fiTasks.data(), sizeof(MixedTask) * p->ntasks,
+                                       cudaMemcpyHostToDevice));
+                }
+                p->dCounter.ensure(2 * sizeof(int) * std::max(1, p->ntasks));
             } catch (...) {
                 delete p;
                 throw;
@@ -1298,8 +1293,11 @@ int PB200_MixedPlanRun(MixedPlan* p, void* stream) {
             const cudaStream_t s = (cudaStream_t)stream;
             if (p->graphExec) {
                 PB_CUDA(cudaGraphLaunch(p->graphExec, s));
-                for (int b = 0; b <= p->ntasks; b++)  // the graph holds the fit kernel and one CRLB kernel per bucket
-                    if (b == p->ntasks || p->tasks[b].a.crlb) count_launch();
+                // the graph holds the LM and Fisher passes and one CRLB kernel per bucket
+                count_launch();
+                if (p->anyFisher) count_launch();
+                for (int b = 0; b < p->ntasks; b++)
+                    if (p->tasks[b].a.crlb) count_launch();
             } else {
                 mixed_enqueue(p, s);
             }

@@ -19,6 +19,12 @@ enum FitFlags : int {
     FIT_CRLB_ONLY = 1,  // skip LM: params come from `initial`, compute Fisher/CRLB/chi^2 only
 };
 
+// Which passes a kernel instance contains: both (the mixed-batch kernel), the LM fit only, or
+// the Fisher/CRLB (+ GLRT) pass only. The standalone launches use the single-pass instances:
+// without the other pass's code and registers they run faster (the host issues the LM launch,
+// then the Fisher launch at the fitted parameters).
+enum FitPass { PASS_BOTH = 0, PASS_LM = 1, PASS_FISHER = 2 };
+
 struct FitArgs {
     const float* smp;      // [n][npix] (may be null with FIT_CRLB_ONLY: no chi-square)
     const float* consts;   // [n][numconst] or null

@@ -54,7 +54,7 @@ __host__ __device__ constexpr int group_smem_floats(int R) {
     return round_up(round_up(R * R, 4) + group_scratch_floats<M>(R), 32) + 8;
 }
 
-template <class M, int G>
+template <class M, int G, int PASS>
 __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitArgs a) {
     constexpr int K = M::K;
     constexpr int NA = K * (K + 1) / 2;
@@ -74,7 +74,9 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
     const int gstride = gridDim.x * gpb;
     const int dx = G % R, dy = G / R;
     const int x0 = lane % R, y0 = lane / R;
-    const bool fisherOnly = (a.flags & FIT_CRLB_ONLY) != 0;
+    constexpr bool kLM = PASS != PASS_FISHER, kFisher = PASS != PASS_LM;
+    const bool fisherOnly = PASS == PASS_FISHER || (PASS == PASS_BOTH && (a.flags & FIT_CRLB_ONLY) != 0);
+    const bool wantFisher = kFisher && (a.crlb || a.glrt);
     const bool haveSmp = a.smp != nullptr;
     const bool glrt = a.glrt != nullptr;  // needs samples (checked by the host)
     const bool vec4 = ((npix & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.smp) & 15) == 0);
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
             it = 0;
             rescuedAny = false;
             if (fisherOnly) mode = MODE_FISHER;
-            else if (a.maxIter <= 0) mode = (a.crlb || a.glrt) ? MODE_FISHER : MODE_SKIP;  // start value, iterations = 1
+            else if (a.maxIter <= 0) mode = wantFisher ? MODE_FISHER : MODE_SKIP;  // start value, iterations = 1
             else mode = MODE_LM;
         }
         // The groups of a warp leave together (an idle group waits for its warp-mates), so every
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
             float acc[NACC];
 #pragma unroll
             for (int q = 0; q < NACC; q++) acc[q] = 0.0f;
-            const bool lm = (mode == MODE_LM);
+            const bool lm = kLM && (!kFisher || mode == MODE_LM);
             int x = x0, y = y0;
             for (int p = lane; p < npix; p += G) {
                 float mu, J[K];
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                     }
                 }
                 if (!done) continue;
-                if (a.crlb || a.glrt) {
+                if (wantFisher) {
                     mode = MODE_FISHER;
                     continue;
                 }

@@ -183,17 +183,24 @@ __device__ __forceinline__ void map_virtual(const float (&av)[NV], float (&acc)[
     }
 }
 
-// Which passes a kernel instance contains: both (the mixed-batch kernel), the LM fit only, or
-// the Fisher/CRLB (+ GLRT) pass only. The standalone launches use the single-pass instances:
-// without the other pass's code and registers they run faster (the host issues the LM launch,
-// then the Fisher launch at the fitted parameters).
-enum FitPass { PASS_BOTH = 0, PASS_LM = 1, PASS_FISHER = 2 };
-
 // Fit the ROIs roi, roi + roiStep, ... < roiEnd of one (model, ROI size) with one group of G
-// lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_floats floats).
+// lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_floats floats). With
+// `claim` set, the group instead takes its ROIs, the first included, from that counter, roiStep
+// consecutive ROIs per atomicAdd of the group's first lane, so groups refill from a shared pool
+// until it runs out.
 template <class M, int G, int CPL, int PASS = PASS_BOTH>
 __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArgs& a, int roi, const int roiEnd,
-                                                const int roiStep, float* spix, const int lane, const unsigned mask) {
+                                                const int roiStep, float* spix, const int lane, const unsigned mask,
+                                                int* claim = nullptr) {
+    int claimEnd = 0;
+    auto claim_next = [&]() -> int {
+        int r = 0;
+        if (lane == 0) r = atomicAdd(claim, roiStep);
+        r = __shfl_sync(mask, r, 0, G);
+        claimEnd = r + roiStep;
+        return r;
+    };
+    if (claim) roi = claim_next();
     constexpr int K = M::K;
     constexpr int NA = K * (K + 1) / 2;
     constexpr int NACC = NA + K + 1;
@@ -424,7 +431,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
             if (a.iterations) a.iterations[roi] = it + 1;
             if (a.diag) a.diag[roi] = rescuedAny ? 1 : 0;
         }
-        roi += roiStep;
+        roi = claim ? (roi + 1 < claimEnd ? roi + 1 : claim_next()) : roi + roiStep;
         mode = MODE_LOAD;
     }
 }

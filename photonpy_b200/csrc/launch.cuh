@@ -65,10 +65,40 @@ inline void launch_groups(KernelT kern, int G, int threads, int strideFloats, in
     count_launch();
 }
 
+// Arguments of the LM launch (no Fisher outputs) and of the Fisher launch at the fitted
+// parameters (FIT_CRLB_ONLY, parameters read from the LM launch's output).
+inline FitArgs lm_pass_args(const FitArgs& a) {
+    FitArgs lm = a;
+    lm.crlb = nullptr;
+    lm.fisher = nullptr;
+    lm.glrt = nullptr;
+    lm.glrtMeanRoi = nullptr;
+    lm.chisq = nullptr;
+    return lm;
+}
+inline FitArgs fisher_pass_args(const FitArgs& a) {
+    FitArgs fi = a;
+    fi.flags |= FIT_CRLB_ONLY;
+    fi.initial = a.params;
+    fi.params = nullptr;
+    fi.iterations = nullptr;
+    fi.trace = nullptr;
+    fi.traceLen = 0;
+    fi.diag = nullptr;
+    return fi;
+}
+
+// Split into single-pass launches as in launch_fit_gauss.
 template <class M, int G>
 void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
     if (a.n <= 0) return;
-    launch_groups(fit_kernel<M, G>, G, threads, group_smem_floats<M>(d.roisize), a.n, d, a, s);
+    const int stride = group_smem_floats<M>(d.roisize);
+    if (a.flags & FIT_CRLB_ONLY) {
+        launch_groups(fit_kernel<M, G, PASS_FISHER>, G, threads, stride, a.n, d, a, s);
+        return;
+    }
+    launch_groups(fit_kernel<M, G, PASS_LM>, G, threads, stride, a.n, d, lm_pass_args(a), s);
+    if (a.crlb || a.glrt) launch_groups(fit_kernel<M, G, PASS_FISHER>, G, threads, stride, a.n, d, fisher_pass_args(a), s);
 }
 
 // LM launch, then (when CRLB or GLRT values are requested) the Fisher launch at the fitted
@@ -81,24 +111,9 @@ void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s
         launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, a, s);
         return;
     }
-    FitArgs lm = a;
-    lm.crlb = nullptr;
-    lm.fisher = nullptr;
-    lm.glrt = nullptr;
-    lm.glrtMeanRoi = nullptr;
-    lm.chisq = nullptr;
-    launch_groups(gauss_fit_kernel<M, G, CPL, PASS_LM>, G, threads, stride, a.n, d, lm, s);
-    if (a.crlb || a.glrt) {
-        FitArgs fi = a;
-        fi.flags |= FIT_CRLB_ONLY;
-        fi.initial = a.params;
-        fi.params = nullptr;
-        fi.iterations = nullptr;
-        fi.trace = nullptr;
-        fi.traceLen = 0;
-        fi.diag = nullptr;
-        launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, fi, s);
-    }
+    launch_groups(gauss_fit_kernel<M, G, CPL, PASS_LM>, G, threads, stride, a.n, d, lm_pass_args(a), s);
+    if (a.crlb || a.glrt)
+        launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, fisher_pass_args(a), s);
 }
 
 template <class M, int G>
@@ -211,8 +226,8 @@ inline int fisher_row_floats(int K) { return K * (K + 1) / 2 + 1; }
 // Mixed-model persistent kernel (k_mixed.cu).
 struct MixedTask;
 int mixed_lanes();
-void launch_mixed(const MixedTask* d_tasks, int ntasks, int totalTiles, int tileRois, int* d_counter,
-                  int strideFloats, int variant, cudaStream_t s);
+void launch_mixed(const MixedTask* d_tasks, int ntasks, int totalClaims, int chunk, int* d_counters,
+                  int strideFloats, int variant, bool fisherPass, cudaStream_t s);
 
 // Per-model entry points (k_*.cu). `variant` 0 = column-blocked Gaussian kernel,
 // 1 = generic table kernel (the only one for the spline).

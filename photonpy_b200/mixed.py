@@ -2,8 +2,9 @@
 
 photonpy fits one estimator — one model and one ROI size — per call (its EstimationQueue
 holds one estimator per queue, EstimationQueue.h:27-108). A ``MixedBatch`` binds several
-estimators with their device-resident ROIs; one ``run()`` fits all of them (LM + Fisher/CRLB)
-in a single persistent kernel whose warps claim tiles of ROIs from a counter, and
+estimators with their device-resident ROIs; one ``run()`` fits all of them with two persistent
+launches (the LM pass, then the Fisher/CRLB pass) in which ROI groups claim ``tile_rois``
+consecutive ROIs at a time from per-bucket counters, and
 ``capture()`` records that run into a CUDA graph for replay. ``run_plain()`` is the
 one-launch-per-bucket form of the same work, for comparison.
 """
@@ -38,7 +39,7 @@ def _ptr_array(tensors):
 class MixedBatch:
     """buckets: list of (Estimator, samples [n, R, R] float32 CUDA tensor[, constants tensor])."""
 
-    def __init__(self, buckets, tile_rois=8, threads=256, with_crlb=True):
+    def __init__(self, buckets, tile_rois=1, threads=256, with_crlb=True):
         import torch
         self._L = _bind(load_library())
         self.buckets = []
