@@ -231,7 +231,7 @@ struct Estimator {
     std::vector<ParamLimit> limits;
     LMParams lm{30, 1e-15f, 0.0f};  // C++ default of the reference (Estimator.cpp:24)
     Context* ctx = nullptr;
-    DevBuf coefs;
+    DevBuf coefs, coefsQ;  // spline coefficients: reference layout and the q-major copy
     int lanes = 0, threads = 256;
     int variant = 0;  // 0: column-blocked Gaussian kernel, 1: generic table kernel
     int device = 0;
@@ -652,6 +652,24 @@ __global__ void spline_evaluate_kernel(const float* __restrict__ coefs, int s0, 
     }
 }
 
+// The q-major copy of the spline coefficients (ModelDesc::coefsQ).
+__global__ void coefs_qmajor_kernel(const float4* __restrict__ src, float4* __restrict__ dst, size_t nvox) {
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nvox * 16; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = t / 16, q = t % 16;
+        dst[q * nvox + v] = src[t];
+    }
+}
+
+void build_coefs_qmajor(Estimator* e) {
+    const size_t nvox = (size_t)e->desc.spline_shape[0] * e->desc.spline_shape[1] * e->desc.spline_shape[2];
+    e->coefsQ.ensure(sizeof(float) * 64 * nvox);
+    const int grid = (int)std::min<size_t>((nvox * 16 + 255) / 256, 65535);
+    coefs_qmajor_kernel<<<grid, 256>>>(e->coefs.as<float4>(), e->coefsQ.as<float4>(), nvox);
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaDeviceSynchronize());
+    e->desc.coefsQ = e->coefsQ.as<float4>();
+}
+
 Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const float* h_coefs, int mode, Context* ctx,
                        const float* d_coefs_src) {
     // modes CSPLINE_FLATBG 0, CSPLINE_TILTEDBG 1, CSPLINE_BGIMAGE 2 (CubicSplinePSF.cu:76-101)
@@ -679,6 +697,7 @@ Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const floa
             PB_CUDA(cudaMemcpy(e->coefs.p, src, sizeof(float) * ncoef, cudaMemcpyHostToDevice));
         }
         e->desc.coefs = e->coefs.as<float>();
+        build_coefs_qmajor(e);
         e->K = model_num_params(e->desc.model);
         e->numconst = mode == 2 ? roisize * roisize : 0;  // the background image of each spot
         e->format = mode == 1 ? "x,y,z,I,bg,bgx,bgy" : "x,y,z,I,bg";
@@ -933,6 +952,7 @@ Estimator* GLRT_CreatePSF(Estimator* model, Context* ctx) {
                 e->coefs.ensure(sizeof(float) * ncoef);
                 PB_CUDA(cudaMemcpy(e->coefs.p, model->coefs.p, sizeof(float) * ncoef, cudaMemcpyDeviceToDevice));
                 e->desc.coefs = e->coefs.as<float>();
+                build_coefs_qmajor(e);
             }
         } catch (...) {
             delete e;
@@ -1145,7 +1165,10 @@ int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, c
                     }
                 }
             }
-            if (d_coefs && d.model == MODEL_CSPLINE) d.coefs = d_coefs;
+            if (d_coefs && d.model == MODEL_CSPLINE) {
+                d.coefs = d_coefs;
+                d.coefsQ = nullptr;  // the caller's coefficients in the reference layout
+            }
             AdjointArgs a{};
             a.smp = d_sample;
             a.params = d_params;

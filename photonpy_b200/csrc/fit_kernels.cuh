@@ -41,6 +41,12 @@ __host__ __device__ constexpr bool model_has_pixel_consts() {
     return pixel_consts_trait<M>::value;
 }
 
+// Models that evaluate several pixels per call (M::kPixelBlock, M::pixel_block<PB>).
+template <class M, class = void>
+struct pixel_block_trait : std::integral_constant<int, 1> {};
+template <class M>
+struct pixel_block_trait<M, std::void_t<decltype(M::kPixelBlock)>> : std::integral_constant<int, M::kPixelBlock> {};
+
 // Shared-memory scratch a group needs besides its pixels: the model table, or the FP64
 // Fisher/LM work area (2*K*K doubles + K doubles), whichever is larger.
 template <class M>
@@ -155,11 +161,8 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
 #pragma unroll
             for (int q = 0; q < NACC; q++) acc[q] = 0.0f;
             const bool lm = kLM && (!kFisher || mode == MODE_LM);
-            int x = x0, y = y0;
-            for (int p = lane; p < npix; p += G) {
-                float mu, J[K];
-                m.pixel(d, tab, x, y, mu, J);
-                const float s = haveSmp ? spix[p] : 0.0f;
+            // one pixel's terms; a lane visits its pixels lane, lane + G, ... in this order
+            auto accumulate = [&](float mu, const float (&J)[K], float s) {
                 float w;
                 if (lm) {
                     // ComputeLevMarAlphaBeta (Estimation.h:109-128)
@@ -187,9 +190,35 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
 #pragma unroll
                     for (int j = i; j < K; j++) acc[q++] += wi * J[j];
                 }
-                x += dx;
-                y += dy;
-                if (x >= R) { x -= R; y++; }
+            };
+            constexpr int PB = pixel_block_trait<M>::value;
+            if constexpr (PB > 1) {
+                for (int p0 = lane; p0 < npix; p0 += G * PB) {
+                    int xs[PB], ys[PB];
+#pragma unroll
+                    for (int t = 0; t < PB; t++) {
+                        const int p = p0 + G * t;
+                        ys[t] = p / R;
+                        xs[t] = p - ys[t] * R;
+                    }
+                    float mus[PB], Js[PB][K];
+                    m.template pixel_block<PB>(d, tab, xs, ys, mus, Js);
+#pragma unroll
+                    for (int t = 0; t < PB; t++) {
+                        const int p = p0 + G * t;
+                        if (p < npix) accumulate(mus[t], Js[t], haveSmp ? spix[p] : 0.0f);
+                    }
+                }
+            } else {
+                int x = x0, y = y0;
+                for (int p = lane; p < npix; p += G) {
+                    float mu, J[K];
+                    m.pixel(d, tab, x, y, mu, J);
+                    accumulate(mu, J, haveSmp ? spix[p] : 0.0f);
+                    x += dx;
+                    y += dy;
+                    if (x >= R) { x -= R; y++; }
+                }
             }
 #pragma unroll
             for (int q = 0; q < NACC; q++) acc[q] = group_sum<G>(acc[q], mask);

@@ -57,6 +57,10 @@ struct ModelDesc {
     int spline_shape[3];  // Nz, Ny, Nx of the coefficient grid
     float spline_zmin, spline_zmax;
     const float* coefs;   // device, [Nz][Ny][Nx][64]
+    // device, the same coefficients q-major: float4 q (coefficients 4q..4q+3) of voxel v at
+    // coefsQ[q * Nz*Ny*Nx + v], so that lanes reading neighbouring voxels read neighbouring
+    // addresses (the fit kernels' copy; null when the caller supplies coefs directly)
+    const float4* coefsQ;
 };
 
 __host__ __device__ constexpr int model_num_params(int m) {
@@ -549,6 +553,7 @@ struct SplineModelT {
     static constexpr int K = (MODE == 1) ? 7 : 5;
     static constexpr int kId = (MODE == 0) ? MODEL_CSPLINE : (MODE == 1 ? MODEL_CSPLINE_TILTED : MODEL_CSPLINE_BGIMAGE);
     static constexpr bool kPixelConsts = (MODE == 2);
+    static constexpr int kPixelBlock = 4;  // pixels per pixel_block() call
     static __host__ __device__ constexpr int table_floats(int) { return 256; }
 
     float tx, ty, tI, tbg, du;
@@ -651,6 +656,65 @@ struct SplineModelT {
         } else {
             mu = ADD(MUL(tI, psf), tbg);
             J[4] = 1.0f;
+        }
+    }
+
+    // pixel() for PB pixels at once: each 16-byte read of the shared power-basis tables serves
+    // all PB pixels (the tables, not the coefficients, are the bulk of the shared-memory
+    // traffic). Every pixel's sums are formed in the same order as in pixel(). Pixels with
+    // y >= roisize (past the ROI) get defined, unused values.
+    template <int PB>
+    __device__ __forceinline__ void pixel_block(const ModelDesc& d, const float* tab, const int (&x)[PB],
+                                                const int (&y)[PB], float (&mu)[PB], float (&J)[PB][K]) const {
+        const float4* cp[PB];
+        float psf[PB], ddx[PB], ddy[PB], ddz[PB];
+        const size_t nvox = (size_t)d.spline_shape[0] * Ny * Nx;
+        const bool qmajor = d.coefsQ != nullptr;
+        const size_t qstride = qmajor ? nvox : 1;
+#pragma unroll
+        for (int t = 0; t < PB; t++) {
+            const int j = max(0, min((int)SUB((float)y[t], ty), Ny - 1));
+            const int i = max(0, min((int)SUB((float)x[t], tx), Nx - 1));
+            const size_t v = (size_t)k * Nx * Ny + (size_t)j * Nx + i;
+            cp[t] = qmajor ? d.coefsQ + v : reinterpret_cast<const float4*>(d.coefs) + 16 * v;
+            psf[t] = ddx[t] = ddy[t] = ddz[t] = 0.0f;
+        }
+        const float4* f4 = reinterpret_cast<const float4*>(tab);
+#pragma unroll 2
+        for (int q = 0; q < 16; q++) {
+            const float4 a = f4[q], b = f4[16 + q], e = f4[32 + q], g = f4[48 + q];
+#pragma unroll
+            for (int t = 0; t < PB; t++) {
+                const float4 c = __ldg(cp[t] + q * qstride);
+                psf[t] = ADD(ADD(ADD(ADD(psf[t], MUL(a.x, c.x)), MUL(a.y, c.y)), MUL(a.z, c.z)), MUL(a.w, c.w));
+                ddx[t] = ADD(ADD(ADD(ADD(ddx[t], MUL(b.x, c.x)), MUL(b.y, c.y)), MUL(b.z, c.z)), MUL(b.w, c.w));
+                ddy[t] = ADD(ADD(ADD(ADD(ddy[t], MUL(e.x, c.x)), MUL(e.y, c.y)), MUL(e.z, c.z)), MUL(e.w, c.w));
+                ddz[t] = ADD(ADD(ADD(ADD(ddz[t], MUL(g.x, c.x)), MUL(g.y, c.y)), MUL(g.z, c.z)), MUL(g.w, c.w));
+            }
+        }
+        const float zs = DIV(tI, du);
+#pragma unroll
+        for (int t = 0; t < PB; t++) {
+            float p = psf[t];
+            if (p < 0.0f) p = 0.0f;
+            J[t][0] = MUL(ddx[t], -tI);
+            J[t][1] = MUL(ddy[t], -tI);
+            J[t][2] = MUL(ddz[t], zs);
+            J[t][3] = p;
+            if (MODE == 1) {
+                const float px = SUB((float)x[t], halfw), py = SUB((float)y[t], halfw);
+                mu[t] = ADD(ADD(ADD(MUL(tI, p), tbg), MUL(bgx, px)), MUL(bgy, py));
+                J[t][4] = 1.0f;
+                J[t][5 % K] = px;
+                J[t][6 % K] = py;
+            } else if (MODE == 2) {
+                const float bg = y[t] < d.roisize ? __ldg(img + y[t] * d.roisize + x[t]) : 0.0f;
+                mu[t] = ADD(MUL(tI, p), MUL(tbg, bg));
+                J[t][4] = bg;
+            } else {
+                mu[t] = ADD(MUL(tI, p), tbg);
+                J[t][4] = 1.0f;
+            }
         }
     }
 
