@@ -254,11 +254,21 @@ def fp32_peak(pb, torch):
     return best
 
 
+HBM_FALLBACK_GBS = 6650.0  # an earlier copy-bandwidth measurement on this pool's B200s
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         return {}
+
+
+def hbm_peak(peaks):
+    """(GB/s, source): the measured copy bandwidth, else the fallback figure."""
+    if peaks.get("hbm_gbs"):
+        return float(peaks["hbm_gbs"]), "of measured (MEASURED_PEAKS.json hbm_gbs)"
+    return HBM_FALLBACK_GBS, "of fallback (no MEASURED_PEAKS.json)"
 
 
 def traffic_from_profile(workload):
@@ -513,7 +523,7 @@ def run_frames(args):
                            what="photonpy's own spot-extraction queue (its CUDA detector, 2 detection threads) "
                                 "built for sm_100a, host 16-bit frames in, ROIs out; no fit")
     peaks = measured_peaks()
-    hbm = peaks.get("hbm_gbs")
+    hbm, hbm_src = hbm_peak(peaks)
     frame_bytes = 4.0 * n * H * W
     achieved = frame_bytes / (ms_det * 1e-3) / 1e9
     line = dict(
@@ -527,8 +537,8 @@ def run_frames(args):
         detection=dict(ms_per_step=ms_det, value=n / (ms_det * 1e-3), unit="frames/s"),
         roofline=dict(bound="hbm", achieved=achieved, peak=hbm, unit="GB/s",
                       frac=achieved / hbm if hbm else None, traffic=None,
-                      note="detection (4 kernels) over the frame bytes read; the filter kernel is bound by "
-                           "instruction issue, not by HBM (profiles/spot_detect_512x512x200.md)"),
+                      note="detection (4 kernels) over the frame bytes read, " + hbm_src + "; the filter kernel "
+                           "is bound by instruction issue, not by HBM (profiles/spot_detect_512x512x200.md)"),
         e2e=e2e, queue_api=queue, cpu_baseline=cpu, reference_gpu_queue=ref_gpu, gpu_launches=int(launches),
         clocks=clk.summary())
     print(json.dumps(line), flush=True)
@@ -684,9 +694,9 @@ def main():
                           frac=achieved_tflops / peak_fp32 if peak_fp32 else None, traffic=traffic,
                           peak_source="FP32 FMA probe measured in this run (PB200_Fp32ProbeLaunch)",
                           flops_per_step=flops, kernel_ms=ms),
-            roofline_hbm=dict(bound="hbm", achieved=hbm_gbs, peak=peaks.get("hbm_gbs"), unit="GB/s",
-                              frac=(hbm_gbs / peaks["hbm_gbs"]) if peaks.get("hbm_gbs") else None,
-                              note="algorithmic ROI-stream bytes (of measured MEASURED_PEAKS.json hbm_gbs)"),
+            roofline_hbm=dict(bound="hbm", achieved=hbm_gbs, peak=hbm_peak(peaks)[0], unit="GB/s",
+                              frac=hbm_gbs / hbm_peak(peaks)[0],
+                              note="algorithmic ROI-stream bytes, " + hbm_peak(peaks)[1]),
             e2e=e2e, cpu_baseline=cpu, gpu_launches=int(launches), clocks=clk.summary(),
         )
         print(json.dumps(line), flush=True)
