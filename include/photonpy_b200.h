@@ -264,6 +264,22 @@ void ImgProc_Destroy(ImageProcessor* q);
 ImageProcessor* SpotExtractionQueue_Create(int width, int height, ROIQueue* roilist, SpotDetectorFactory* sdf,
                                            CameraCalibration* calib, int numDetectionThreads, int sumframes,
                                            Context* ctx);
+/* ImageProcessor.cpp:61-233: extraction of predefined ROIs from a stream of 16-bit frames
+ * (ImgProc_AddFrameU16, calibrated as above). ROI i takes the roisize x roisize box at
+ * (x, y) = cornerpos of numframes frames from startframe (frames numbered from 0 in push order;
+ * box coordinates clamped to the frame, where the reference reads outside it); its record is
+ * available once its last frame is processed, records in order of last frame, then start
+ * frame, then request order. ROIExtractor_GetResults hands out up to numrois records oldest
+ * first; slot i of framedata [numrois][roiframes][roisize][roisize] gets min(numframes,
+ * roiframes) boxes. NumFinishedFrames counts processed frames (the reference returns 0). */
+typedef struct ExtractionROI { /* photonpy/cpp/image_proc.py ROIExtractor.ROIType */
+    int cornerpos[2];          /* x, y */
+    int startframe, numframes;
+} ExtractionROI;
+ImageProcessor* ROIExtractor_Create(int imgWidth, int imgHeight, const ExtractionROI* rois, int numrois, int roiframes,
+                                    int roisize, CameraCalibration* calib, Context* ctx);
+int ROIExtractor_GetResultCount(ImageProcessor* re);
+int ROIExtractor_GetResults(ImageProcessor* re, int numrois, ExtractionROI* rois, float* framedata);
 
 /* Extension: detection and ROI cut-out of nframes device frames [n][height][width] on a stream,
  * for feeding the fitter without host copies. d_bg: device [height][width] or NULL (the

@@ -271,3 +271,36 @@ def spot_extraction_queue(frames_u16, u1, u2, maxfilter, det_roisize, min_intens
     info = np.array(infos, dtype=[("id", "<i4"), ("score", "<f4"), ("x", "<i4"), ("y", "<i4"), ("z", "<i4")])
     rois = np.array(stacks, dtype=np.float32).reshape(len(stacks), sumframes, rh, rw)
     return info, rois
+
+
+ROI_TYPE = np.dtype([("cornerpos", "<i4", 2), ("startframe", "<i4"), ("numframes", "<i4")])
+
+
+def extract_rois(frames_u16, rois, roiframes, roisize, calib=None):
+    """The ROI extractor restated (ImageProcessor.cpp:61-233): ROI i collects the roisize x
+    roisize box at (x, y) = cornerpos of frames startframe .. startframe + numframes - 1 of the
+    calibrated movie; records complete at their last frame (the start frame when numframes <= 0)
+    and come out by last frame, then start frame, then request order. Boxes are clamped to the
+    frame (the reference reads outside it). Returns (records, boxes [n, roiframes, roisize,
+    roisize]) for the records complete within the movie; unwritten boxes are zero."""
+    frames = np.asarray(frames_u16)
+    n, h, w = frames.shape
+    cal = camera_calibrate(frames, *calib) if calib is not None else frames.astype(np.float32)
+    rois = np.asarray(rois, dtype=ROI_TYPE)
+    last = rois["startframe"] + np.maximum(rois["numframes"], 1) - 1
+    order = sorted(range(len(rois)), key=lambda i: (last[i], rois["startframe"][i], i))
+    out_r, out_b = [], []
+    for i in order:
+        if last[i] >= n:
+            continue
+        r = rois[i]
+        b = np.zeros((roiframes, roisize, roisize), np.float32)
+        x0, y0 = int(r["cornerpos"][0]), int(r["cornerpos"][1])
+        ys = np.clip(np.arange(y0, y0 + roisize), 0, h - 1)
+        xs = np.clip(np.arange(x0, x0 + roisize), 0, w - 1)
+        for f in range(min(max(int(r["numframes"]), 0), roiframes)):
+            b[f] = cal[int(r["startframe"]) + f][ys][:, xs]
+        out_r.append(r)
+        out_b.append(b)
+    return np.array(out_r, dtype=ROI_TYPE), np.array(out_b, np.float32).reshape(len(out_b), roiframes, roisize,
+                                                                                roisize)

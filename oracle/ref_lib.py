@@ -400,3 +400,58 @@ def spot_queue(frames_u16, u1, u2, maxfilter, det_roisize, min_intensity, max_in
         if q:
             L.ImgProc_Destroy(q)  # the queue before the ROI queue it fills
         L.Context_Destroy(ctx)
+
+
+ROI_TYPE = np.dtype([("cornerpos", "<i4", 2), ("startframe", "<i4"), ("numframes", "<i4")])
+
+
+def roi_extractor(frames_u16, rois, roiframes, roisize, gain_offset=None, timeout=120.0):
+    """The reference's ROI extractor (ROIExtractor_Create, ImageProcessor.cpp:221; needs a GPU):
+    pushes the 16-bit frames, waits (bounded) until it is idle, and takes every record in the
+    order ROIExtractor_GetResults gives them. ROIs must lie inside the frame (the reference
+    reads outside it otherwise)."""
+    import time
+    L = lib()
+    vp = ct.c_void_p
+    frames = np.ascontiguousarray(frames_u16, dtype=np.uint16)
+    n, h, w = frames.shape
+    rois = np.ascontiguousarray(rois, dtype=ROI_TYPE)
+    L.ROIExtractor_Create.argtypes = [ct.c_int, ct.c_int, vp, ct.c_int, ct.c_int, ct.c_int, vp, vp]
+    L.ROIExtractor_Create.restype = vp
+    L.ROIExtractor_GetResultCount.argtypes = [vp]
+    L.ROIExtractor_GetResultCount.restype = ct.c_int
+    L.ROIExtractor_GetResults.argtypes = [vp, ct.c_int, vp, vp]
+    L.ROIExtractor_GetResults.restype = ct.c_int
+    L.ImgProc_AddFrameU16.argtypes = [vp, vp]
+    L.ImgProc_IsIdle.argtypes = [vp]
+    L.ImgProc_IsIdle.restype = ct.c_bool
+    L.ImgProc_Destroy.argtypes = [vp]
+    L.GainOffsetCalib_Create.argtypes = [ct.c_float, ct.c_float, vp]
+    L.GainOffsetCalib_Create.restype = vp
+    ctx = L.Context_Create()
+    q = None
+    try:
+        calib = None
+        if gain_offset is not None:
+            calib = L.GainOffsetCalib_Create(float(gain_offset[0]), float(gain_offset[1]), ctx)
+        q = L.ROIExtractor_Create(w, h, rois.ctypes.data, len(rois), int(roiframes), int(roisize), calib, ctx)
+        for f in range(n):
+            L.ImgProc_AddFrameU16(q, frames[f].ctypes.data)
+        t0 = time.time()
+        time.sleep(0.05)
+        while not L.ImgProc_IsIdle(q):
+            if time.time() - t0 > timeout:
+                raise TimeoutError("reference ROI extractor did not finish")
+            time.sleep(0.01)
+        time.sleep(0.05)
+        cnt = L.ROIExtractor_GetResultCount(q)
+        out_r = np.zeros(cnt, ROI_TYPE)
+        out_b = np.zeros((cnt, roiframes, roisize, roisize), np.float32)
+        if cnt:
+            got = L.ROIExtractor_GetResults(q, cnt, out_r.ctypes.data, out_b.ctypes.data)
+            out_r, out_b = out_r[:got], out_b[:got]
+        return out_r, out_b
+    finally:
+        if q:
+            L.ImgProc_Destroy(q)
+        L.Context_Destroy(ctx)

@@ -291,48 +291,31 @@ __global__ void cut_stacks_kernel(const float* __restrict__ frames, int w, int h
     }
 }
 
-class SpotExtractionQueue : public ImageProcessor {
+// Pinned ring of raw 16-bit frames and the worker thread that takes every complete unit of
+// `group` frames waiting (up to 64 MB of raw pixels) and hands them to process(), the
+// derived queue's GPU batch. Units are numbered from 0 in push order.
+class FrameRing : public ImageProcessor {
    public:
-    SpotExtractionQueue(int w, int h, ROIQueue* out, const SpotDetectorConfig& cfg, CameraCalibration* calib)
-        : w_(w), h_(h), npix_((size_t)w * h), out_(out), calib_(calib) {
-        sf_ = out->shape[0];
-        rh_ = out->shape[1];
-        rw_ = out->shape[2];
-        if (sf_ < 1 || rh_ < 1 || rw_ < 1) throw FrameQueueError("SpotExtractionQueue: bad ROI queue shape");
-        if (w < 1 || h < 1 || npix_ >= (1u << 31)) throw FrameQueueError("SpotExtractionQueue: bad frame size");
+    FrameRing(int w, int h, int group, const char* name)
+        : w_(w), h_(h), npix_((size_t)w * h), group_(group), name_(name) {
+        if (w < 1 || h < 1 || npix_ >= (1u << 31)) throw FrameQueueError(std::string(name) + ": bad frame size");
+        if (group < 1) throw FrameQueueError(std::string(name) + ": bad group size");
         PBF_CUDA(cudaGetDevice(&dev_));
-        SpotDetectorConfig c = cfg;
-        if (cfg.backgroundImage) {  // copied now: the caller's array need not outlive the queue
-            dBg_.ensure(sizeof(float) * npix_);
-            PBF_CUDA(cudaMemcpy(dBg_.p, cfg.backgroundImage, sizeof(float) * npix_, cudaMemcpyHostToDevice));
-        }
-        c.backgroundImage = nullptr;
-        det_ = SpotDetector_Configure(&c);
-        if (!det_) throw FrameQueueError("SpotExtractionQueue: detector configuration failed");
-        // batches of up to 64 MB of raw frames, whole groups; the ring holds two batches
         const size_t frameBytes = sizeof(uint16_t) * npix_;
         int bmax = (int)std::min<size_t>(4096, std::max<size_t>(1, (size_t(64) << 20) / frameBytes));
-        bmax = std::max(sf_, bmax / sf_ * sf_);
-        bmax = std::min(bmax, 65535 / sf_ * sf_);  // kernel grid limit on groups and frames
-        maxGroups_ = bmax / sf_;
-        cap_ = 2 * bmax;
+        bmax = std::max(group_, bmax / group_ * group_);
+        bmax = std::min(bmax, 65535 / group_ * group_);  // kernel grid limit on frames per launch
+        maxUnits_ = bmax / group_;
+        cap_ = 2 * bmax;  // the ring holds two batches
         ringBytes_ = frameBytes * cap_;
         ring_ = static_cast<uint16_t*>(pb200::pinned_take(ringBytes_));
         PBF_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        worker_ = std::thread([this]() { run(); });
     }
 
-    ~SpotExtractionQueue() override {
-        {
-            std::lock_guard<std::mutex> lk(mtx_);
-            stop_ = true;
-        }
-        cvWork_.notify_all();
-        cvSpace_.notify_all();
-        if (worker_.joinable()) worker_.join();
+    ~FrameRing() override {
+        stop_worker();
         if (stream_) cudaStreamDestroy(stream_);
         if (ring_) pb200::pinned_give(ring_, ringBytes_);
-        if (det_) SpotDetector_DestroyFactory(det_);
     }
 
     void AddFrameU16(const uint16_t* data) override {
@@ -347,7 +330,7 @@ class SpotExtractionQueue : public ImageProcessor {
     }
 
     void AddFrameF32(const float*) override {
-        throw FrameQueueError("SpotExtractionQueue: float frames are not accepted (16-bit frames only)");
+        throw FrameQueueError(name_ + ": float frames are not accepted (16-bit frames only)");
     }
 
     int GetQueueLength() override {
@@ -362,40 +345,101 @@ class SpotExtractionQueue : public ImageProcessor {
 
     bool IsIdle() override {
         std::lock_guard<std::mutex> lk(mtx_);
-        return !busy_ && count_ / sf_ == 0;
+        return !busy_ && count_ / group_ == 0;
     }
+
+   protected:
+    // Starts the worker; the derived constructor calls it last.
+    void start_worker() {
+        worker_ = std::thread([this]() { run(); });
+    }
+    // Stops the worker after its current batch; the derived destructor calls it first, so that
+    // process() never runs on a half-destroyed object.
+    void stop_worker() {
+        {
+            std::lock_guard<std::mutex> lk(mtx_);
+            stop_ = true;
+        }
+        cvWork_.notify_all();
+        cvSpace_.notify_all();
+        if (worker_.joinable()) worker_.join();
+    }
+    // Raw frames of units [unitBase, unitBase + units) at ring_ + first * npix_ (contiguous).
+    virtual void process(int first, int units, int unitBase) = 0;
+
+    int w_, h_;
+    size_t npix_;
+    int group_;
+    std::string name_;
+    int dev_ = 0;
+    cudaStream_t stream_ = nullptr;
+    uint16_t* ring_ = nullptr;  // [head_, head_ + count_) waiting, modulo cap_
 
    private:
     void run() {
         cudaSetDevice(dev_);
         while (true) {
-            int first, groups, idBase;
+            int first, units, unitBase;
             {
                 std::unique_lock<std::mutex> lk(mtx_);
-                cvWork_.wait(lk, [&]() { return stop_ || count_ / sf_ > 0; });
+                cvWork_.wait(lk, [&]() { return stop_ || count_ / group_ > 0; });
                 if (stop_) return;
                 first = head_;
-                groups = std::min({count_ / sf_, maxGroups_, (cap_ - head_) / sf_});
-                idBase = finished_;
+                units = std::min({count_ / group_, maxUnits_, (cap_ - head_) / group_});
+                unitBase = finished_;
                 busy_ = true;
             }
             try {
-                process(first, groups, idBase);
+                process(first, units, unitBase);
             } catch (const std::exception& e) {
-                pb200::set_last_error(std::string("SpotExtractionQueue: ") + e.what() + " (frames dropped)");
+                pb200::set_last_error(name_ + ": " + e.what() + " (frames dropped)");
                 cudaStreamSynchronize(stream_);
             }
             {
                 std::lock_guard<std::mutex> lk(mtx_);
-                head_ = (head_ + groups * sf_) % cap_;
-                count_ -= groups * sf_;
-                finished_ += groups;
+                head_ = (head_ + units * group_) % cap_;
+                count_ -= units * group_;
+                finished_ += units;
                 busy_ = false;
             }
             cvSpace_.notify_all();
         }
     }
 
+    size_t ringBytes_ = 0;
+    int cap_ = 0, head_ = 0, count_ = 0, maxUnits_ = 1;
+    int finished_ = 0;
+    bool busy_ = false, stop_ = false;
+    std::mutex mtx_;
+    std::condition_variable cvWork_, cvSpace_;
+    std::thread worker_;
+};
+
+class SpotExtractionQueue : public FrameRing {
+   public:
+    SpotExtractionQueue(int w, int h, ROIQueue* out, const SpotDetectorConfig& cfg, CameraCalibration* calib)
+        : FrameRing(w, h, out->shape[0], "SpotExtractionQueue"), out_(out), calib_(calib) {
+        sf_ = out->shape[0];
+        rh_ = out->shape[1];
+        rw_ = out->shape[2];
+        if (rh_ < 1 || rw_ < 1) throw FrameQueueError("SpotExtractionQueue: bad ROI queue shape");
+        SpotDetectorConfig c = cfg;
+        if (cfg.backgroundImage) {  // copied now: the caller's array need not outlive the queue
+            dBg_.ensure(sizeof(float) * npix_);
+            PBF_CUDA(cudaMemcpy(dBg_.p, cfg.backgroundImage, sizeof(float) * npix_, cudaMemcpyHostToDevice));
+        }
+        c.backgroundImage = nullptr;
+        det_ = SpotDetector_Configure(&c);
+        if (!det_) throw FrameQueueError("SpotExtractionQueue: detector configuration failed");
+        start_worker();
+    }
+
+    ~SpotExtractionQueue() override {
+        stop_worker();
+        if (det_) SpotDetector_DestroyFactory(det_);
+    }
+
+   private:
     void process(int first, int groups, int idBase) {
         const int nf = groups * sf_;
         const size_t npix = npix_;
@@ -475,27 +519,166 @@ class SpotExtractionQueue : public ImageProcessor {
         out_->push((int)total, info_.data(), hRois_.as<float>());
     }
 
-    int w_, h_;
-    size_t npix_;
     int sf_ = 1, rh_ = 1, rw_ = 1;
     ROIQueue* out_;
     CameraCalibration* calib_;
     SpotDetectorFactory* det_ = nullptr;
-    int dev_ = 0;
-    cudaStream_t stream_ = nullptr;
-    // pinned ring of raw frames: [head_, head_ + count_) waiting, modulo cap_
-    uint16_t* ring_ = nullptr;
-    size_t ringBytes_ = 0;
-    int cap_ = 0, head_ = 0, count_ = 0, maxGroups_ = 1;
-    int finished_ = 0;
-    bool busy_ = false, stop_ = false;
-    std::mutex mtx_;
-    std::condition_variable cvWork_, cvSpace_;
-    std::thread worker_;
     int C_ = 256;  // spot slots per summed frame in the detector outputs
     DBuf dBg_, dRaw_, dOrig_, dSum_, dFound_, dIndex_, dScore_, dOffsets_, dCorner_, dScoreOut_, dRois_;
     HBuf hFound_, hCorner_, hScore_, hRois_;
     std::vector<ROIInfo> info_;
+};
+
+// Gathers the ROI pixels of a batch: task t copies the roisize x roisize box at corner
+// (x, y) = (task.x, task.y) of frame task.z of the batch (coordinates clamped to the frame)
+// into out[t]. One warp per task.
+__global__ void gather_boxes_kernel(const float* __restrict__ frames, int w, int h, int roisize,
+                                    const int4* __restrict__ tasks, int ntasks, float* __restrict__ out) {
+    const long long t = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (t >= ntasks) return;
+    const int lane = threadIdx.x & 31;
+    const int4 k = tasks[t];
+    const float* src = frames + (size_t)k.z * w * h;
+    float* dst = out + (size_t)t * roisize * roisize;
+    for (int q = lane; q < roisize * roisize; q += 32) {
+        const int fy = min(max(k.y + q / roisize, 0), h - 1), fx = min(max(k.x + q % roisize, 0), w - 1);
+        dst[q] = __ldg(src + (size_t)fy * w + fx);
+    }
+}
+
+// The ROI extractor (ImageProcessor.cpp:61-233): 16-bit frames in (calibrated like the spot
+// queue's), and for each requested ROI the boxes of its numframes frames from startframe on,
+// collected into one record that becomes available once its last frame has been processed.
+// Records come out in the order the reference hands them out: by last frame, then by start
+// frame, then in request order. As a difference, box coordinates are clamped to the frame
+// (the reference reads outside the frame for boxes that cross its border).
+class ROIExtractorQueue : public FrameRing {
+   public:
+    ROIExtractorQueue(int w, int h, const ExtractionROI* rois, int n, int roiframes, int roisize,
+                      CameraCalibration* calib)
+        : FrameRing(w, h, 1, "ROIExtractor"), roiframes_(roiframes), rs_(roisize), calib_(calib) {
+        if (n < 0 || (n > 0 && !rois) || roisize < 1 || roiframes < 0)
+            throw FrameQueueError("ROIExtractor_Create: bad arguments");
+        spots_.resize(n);
+        int last = -1;
+        for (int i = 0; i < n; i++) {
+            if (rois[i].startframe < 0) throw FrameQueueError("ROIExtractor_Create: negative startframe");
+            spots_[i].roi = rois[i];
+            spots_[i].data.assign((size_t)std::max(0, rois[i].numframes) * rs_ * rs_, 0.0f);
+            last = std::max(last, rois[i].startframe);
+        }
+        // activation order: by start frame, then request order (a stable sort)
+        order_.resize(n);
+        for (int i = 0; i < n; i++) order_[i] = i;
+        std::stable_sort(order_.begin(), order_.end(),
+                         [&](int a, int b) { return rois[a].startframe < rois[b].startframe; });
+        start_worker();
+    }
+
+    ~ROIExtractorQueue() override { stop_worker(); }
+
+    int result_count() {
+        std::lock_guard<std::mutex> lk(resMtx_);
+        return (int)results_.size();
+    }
+
+    // ROIExtractor::GetResults (ImageProcessor.cpp:105-126): up to n records, oldest first; slot
+    // i of framedata holds roiframes boxes, of which min(numframes, roiframes) are written.
+    int results(int n, ExtractionROI* rois, float* framedata) {
+        std::vector<int> take;
+        {
+            std::lock_guard<std::mutex> lk(resMtx_);
+            while ((int)take.size() < n && !results_.empty()) {
+                take.push_back(results_.front());
+                results_.pop_front();
+            }
+        }
+        const size_t box = (size_t)rs_ * rs_;
+        for (size_t i = 0; i < take.size(); i++) {
+            Spot& sp = spots_[take[i]];
+            if (rois) rois[i] = sp.roi;
+            if (framedata) {
+                const int nf = std::min(std::max(0, sp.roi.numframes), roiframes_);
+                std::memcpy(framedata + (size_t)roiframes_ * box * i, sp.data.data(), sizeof(float) * box * nf);
+            }
+            std::vector<float>().swap(sp.data);  // handed out
+        }
+        return (int)take.size();
+    }
+
+   private:
+    struct Spot {
+        ExtractionROI roi;
+        std::vector<float> data;  // [numframes][roisize][roisize]
+    };
+
+    void process(int first, int units, int frameBase) override {
+        const int nf = units;
+        const size_t npix = npix_;
+        dRaw_.ensure(sizeof(uint16_t) * npix * nf);
+        dFrames_.ensure(sizeof(float) * npix * nf);
+        PBF_CUDA(cudaMemcpyAsync(dRaw_.p, ring_ + (size_t)first * npix, sizeof(uint16_t) * npix * nf,
+                                 cudaMemcpyHostToDevice, stream_));
+        pb200::camera_calib_apply_u16(calib_, dRaw_.as<uint16_t>(), dFrames_.as<float>(), w_, h_, nf, stream_);
+        // boxes wanted from these frames, in activation order
+        const int f0 = frameBase, f1 = frameBase + nf;
+        const int n = (int)order_.size();
+        while (live_ < n && last_frame(spots_[order_[live_]].roi) < f0) live_++;  // done before this batch
+        tasks_.clear();
+        dest_.clear();
+        for (int o = live_; o < n; o++) {
+            const int i = order_[o];
+            const ExtractionROI& r = spots_[i].roi;
+            if (r.startframe >= f1) break;  // order_ is sorted by start frame
+            const int lo = std::max(r.startframe, f0), hi = std::min(r.startframe + r.numframes, f1);
+            for (int f = lo; f < hi; f++) {
+                tasks_.push_back(make_int4(r.cornerpos[0], r.cornerpos[1], f - f0, 0));
+                dest_.push_back({i, f - r.startframe});
+            }
+        }
+        const int T = (int)tasks_.size();
+        const size_t box = (size_t)rs_ * rs_;
+        if (T > 0) {
+            dTasks_.ensure(sizeof(int4) * T);
+            dBoxes_.ensure(sizeof(float) * box * T);
+            hBoxes_.ensure(sizeof(float) * box * T);
+            PBF_CUDA(cudaMemcpyAsync(dTasks_.p, tasks_.data(), sizeof(int4) * T, cudaMemcpyHostToDevice, stream_));
+            gather_boxes_kernel<<<(T + 7) / 8, 256, 0, stream_>>>(dFrames_.as<float>(), w_, h_, rs_,
+                                                                 dTasks_.as<int4>(), T, dBoxes_.as<float>());
+            PBF_CUDA(cudaGetLastError());
+            PBF_CUDA(cudaMemcpyAsync(hBoxes_.p, dBoxes_.p, sizeof(float) * box * T, cudaMemcpyDeviceToHost,
+                                     stream_));
+        }
+        PBF_CUDA(cudaStreamSynchronize(stream_));  // also keeps the ring slots until the copy is done
+        const float* hb = hBoxes_.as<float>();
+        for (int t = 0; t < T; t++)
+            std::memcpy(spots_[dest_[t].first].data.data() + box * dest_[t].second, hb + box * t,
+                        sizeof(float) * box);
+        // records complete at frame startframe + max(numframes, 1) - 1: hand them out frame by
+        // frame, each frame's in activation order
+        std::lock_guard<std::mutex> lk(resMtx_);
+        for (int f = f0; f < f1; f++)
+            for (int o = live_; o < n; o++) {
+                const int i = order_[o];
+                const ExtractionROI& r = spots_[i].roi;
+                if (r.startframe > f) break;
+                if (last_frame(r) == f) results_.push_back(i);
+            }
+    }
+
+    static int last_frame(const ExtractionROI& r) { return r.startframe + std::max(r.numframes, 1) - 1; }
+
+    int roiframes_, rs_;
+    CameraCalibration* calib_;
+    std::vector<Spot> spots_;
+    std::vector<int> order_;
+    int live_ = 0;  // order_[0, live_) are complete
+    std::vector<int4> tasks_;
+    std::vector<std::pair<int, int>> dest_;  // (spot, frame within the spot) of each task
+    std::mutex resMtx_;
+    std::deque<int> results_;
+    DBuf dRaw_, dFrames_, dTasks_, dBoxes_;
+    HBuf hBoxes_;
 };
 
 void destroy_calib(void* p) { delete static_cast<CameraCalibration*>(p); }
@@ -654,6 +837,33 @@ ImageProcessor* SpotExtractionQueue_Create(int width, int height, ROIQueue* roil
             return q;
         },
         (ImageProcessor*)nullptr);
+}
+
+ImageProcessor* ROIExtractor_Create(int imgWidth, int imgHeight, const ExtractionROI* rois, int numrois, int roiframes,
+                                    int roisize, CameraCalibration* calib, Context* ctx) {
+    return fq_guarded(
+        [&]() -> ImageProcessor* {
+            auto* q = new ROIExtractorQueue(imgWidth, imgHeight, rois, numrois, roiframes, roisize, calib);
+            q->ctx = ctx;
+            pb200::context_attach(ctx, q, destroy_imgproc);
+            return q;
+        },
+        (ImageProcessor*)nullptr);
+}
+
+int ROIExtractor_GetResultCount(ImageProcessor* re) {
+    auto* q = dynamic_cast<ROIExtractorQueue*>(re);
+    return q ? q->result_count() : 0;
+}
+
+int ROIExtractor_GetResults(ImageProcessor* re, int numrois, ExtractionROI* rois, float* framedata) {
+    return fq_guarded(
+        [&]() -> int {
+            auto* q = dynamic_cast<ROIExtractorQueue*>(re);
+            if (!q) throw FrameQueueError("ROIExtractor_GetResults: not a ROI extractor");
+            return q->results(numrois, rois, framedata);
+        },
+        0);
 }
 
 }  // extern "C"

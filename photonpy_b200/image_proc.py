@@ -74,6 +74,44 @@ class ImageProcessor:
             self.inst = None
 
 
+class ROIExtractor(ImageProcessor):
+    """photonpy/cpp/image_proc.py ROIExtractor: boxes of predefined ROIs cut from a stream of
+    16-bit frames. rois: ROIType records (cornerpos = (x, y), startframe, numframes)."""
+
+    ROIType = np.dtype([("cornerpos", "<i4", 2), ("startframe", "<i4"), ("numframes", "<i4")])
+
+    def __init__(self, imgshape, rois, roiframes, roisize, calib, ctx: Context):
+        lib = ctx.lib
+        create = lib.ROIExtractor_Create
+        create.argtypes = [ct.c_int32, ct.c_int32, ctl.ndpointer(ROIExtractor.ROIType, flags="aligned, c_contiguous"),
+                           ct.c_int32, ct.c_int32, ct.c_int32, ct.c_void_p, ct.c_void_p]
+        create.restype = ct.c_void_p
+        self._GetResultCount = lib.ROIExtractor_GetResultCount
+        self._GetResultCount.argtypes = [ct.c_void_p]
+        self._GetResultCount.restype = ct.c_int32
+        self._GetResults = lib.ROIExtractor_GetResults
+        self._GetResults.argtypes = [ct.c_void_p, ct.c_int32,
+                                     ctl.ndpointer(ROIExtractor.ROIType, flags="aligned, c_contiguous"),
+                                     ctl.ndpointer(np.float32, flags="aligned, c_contiguous")]
+        self._GetResults.restype = ct.c_int32
+        rois = np.ascontiguousarray(rois, dtype=ROIExtractor.ROIType)
+        inst = create(imgshape[1], imgshape[0], rois, len(rois), roiframes, roisize,
+                      calib.inst if calib else None, ctx.inst)
+        check_instance(inst, "ROIExtractor_Create")
+        self.roiframes = roiframes
+        self.roisize = roisize
+        super().__init__(imgshape, inst, ctx)
+
+    def GetResultCount(self):
+        return self._GetResultCount(self.inst)
+
+    def GetResults(self, numrois):
+        rois = np.zeros(numrois, dtype=ROIExtractor.ROIType)
+        framedata = np.zeros((numrois, self.roiframes, self.roisize, self.roisize), dtype=np.float32)
+        count = self._GetResults(self.inst, numrois, rois, framedata)
+        return rois[:count], framedata[:count]
+
+
 def check_instance(inst, what):
     if not inst:
         check_error(what)

@@ -5,7 +5,8 @@ photonpy/smlm/process_movie.py.
 to a file in photonpy's format: repeated pairs of ``numpy.save`` arrays, the ``ROIInfoDType``
 records of a batch and its pixels [n, (sumframes,) roisize, roisize] (process_movie.py:30-60).
 ``load_rois_iterator`` / ``load_rois`` read such a file back (process_movie.py:67-95) and
-``localize_rois`` fits the ROIs through an ``EstimQueue`` (process_movie.py:134-202).
+``localize_rois`` fits the ROIs through an ``EstimQueue`` (process_movie.py:134-202), and
+``extract_rois_iterator`` cuts predefined ROIs out of a movie (process_movie.py:96-131).
 ``create_calib_obj`` takes scalars or arrays (photonpy also reads TIFF calibration movies, which
 needs tifffile; pass the arrays instead).
 """
@@ -84,6 +85,38 @@ def load_rois(rois_fn, maxrois=None):
         rois_info.append(ri)
         pixels.append(px)
     return np.concatenate(rois_info), np.concatenate(pixels)
+
+
+def extract_rois_iterator(movie, roipos, roiframe, calib, roisize, ctx: Context, minBatchSize):
+    """Boxes of predefined ROIs from a movie (an iterable of 16-bit frames): roipos [n, 2] ROI
+    corners, given to the extractor as its cornerpos (x, y) records, roiframe [n] the frame of
+    each. Yields (rois, frames) batches of at least minBatchSize records (the last one may be
+    smaller). photonpy's version of this function calls a PushFrame method its frame processor
+    does not have; here the frames go in through PushFrameU16."""
+    from .image_proc import ROIExtractor
+    roilist = np.zeros(len(roipos), dtype=ROIExtractor.ROIType)
+    roilist["cornerpos"] = roipos
+    roilist["startframe"] = roiframe
+    roilist["numframes"] = 1
+    with Context(ctx.smlm) as ex_ctx:
+        q = None
+        for i, img in enumerate(movie):
+            if i == 0:
+                q = ROIExtractor(img.shape, roilist, 1, roisize, calib, ex_ctx)
+            q.PushFrameU16(img)
+            resultcount = q.GetResultCount()
+            if resultcount > minBatchSize:
+                yield q.GetResults(resultcount)
+        if q is None:
+            return
+        while not q.IsIdle():
+            time.sleep(0.005)
+            resultcount = q.GetResultCount()
+            if resultcount > minBatchSize:
+                yield q.GetResults(resultcount)
+        resultcount = q.GetResultCount()
+        if resultcount > 0:
+            yield q.GetResults(resultcount)
 
 
 def localize_rois(rois_data_source, psf, initial_estim=None, constants=None, prog_cb=None, total=None):
