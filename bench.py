@@ -546,6 +546,28 @@ def run_frames(args):
     ctx.Destroy()
 
 
+def reference_gpu_plain(d, m=50_000):
+    """photonpy's own plain GPU form (its one-thread-per-ROI CUDA kernels built for sm_100a)
+    through its host API, Estimate + ChiSquareAndCRLB, on the first m ROIs of the batch; host
+    copies included, as photonpy always has them."""
+    from oracle import ref_lib
+    if not ref_lib.available() or d["kind"] not in ("XYIBg", "XYIBgSigmaXY", "XYZIBg"):
+        return None
+    sub = d["samples"][:m]
+    est = ref_gpu_estimator(d)
+    try:
+        p, _, _ = est.estimate(sub[:1000], trace_len=0)  # warm-up
+        t0 = time.perf_counter()
+        p, _, _ = est.estimate(sub, trace_len=0)
+        est.crlb_chisq(p, sub)
+        dt = time.perf_counter() - t0
+    finally:
+        est.close()
+    return dict(value=len(sub) / dt, unit=UNIT, sample=f"first {len(sub)} ROIs of the batch",
+                what="photonpy's own one-thread-per-ROI CUDA kernels built for sm_100a, through its host API "
+                     "(Estimate + ChiSquareAndCRLB, host copies included)")
+
+
 def ref_gpu_estimator(d):
     from oracle import ref_lib
     k = d["kind"]
@@ -672,9 +694,10 @@ def main():
         # results through the host path equal the device path
         assert np.array_equal(h_par.numpy(), out["params"].cpu().numpy())
 
-    cpu = None
+    cpu = ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(d, args.cpu_seconds)
+        ref_gpu = reference_gpu_plain(d)
 
     if rank == 0:
         tr = traffic_from_profile(args.workload)
@@ -697,7 +720,8 @@ def main():
             roofline_hbm=dict(bound="hbm", achieved=hbm_gbs, peak=hbm_peak(peaks)[0], unit="GB/s",
                               frac=hbm_gbs / hbm_peak(peaks)[0],
                               note="algorithmic ROI-stream bytes, " + hbm_peak(peaks)[1]),
-            e2e=e2e, cpu_baseline=cpu, gpu_launches=int(launches), clocks=clk.summary(),
+            e2e=e2e, cpu_baseline=cpu, reference_gpu_plain=ref_gpu, gpu_launches=int(launches),
+            clocks=clk.summary(),
         )
         print(json.dumps(line), flush=True)
     est.Destroy()
