@@ -157,7 +157,7 @@ Estimator* GLRT_CreatePSF(Estimator* model, Context* ctx);                     /
 int PB200_SetGLRTReferenceMean(Estimator* e, int on);
 
 /* ---- Estimation queue, Estimators/EstimationQueue.h:21-25, 112-126 --------------------
- * Streams ROIs from host memory through the fused fit + CRLB + chi-square kernels: spots are
+ * Streams ROIs from host memory through the fit + CRLB + chi-square kernels: spots are
  * packed into pinned batches of batchSize; a worker thread launches waiting batches on
  * numStreams CUDA streams (numStreams < 0: 3), several full batches per launch when they
  * are waiting; results are collected per batch. GetResults returns only whole batches,
@@ -375,7 +375,7 @@ int PB200_MixedPlanRun(MixedPlan* plan, void* stream);
 int PB200_MixedPlanCapture(MixedPlan* plan, void* stream);
 int PB200_MixedPlanInfo(MixedPlan* plan, int* ntasks, int* totalTiles, int* strideFloats);
 void PB200_MixedPlanDestroy(MixedPlan* plan);
-/* No counterpart in the reference. Fused fit + CRLB + chi-square like PB200_EstimateDevice,
+/* No counterpart in the reference. Fit + CRLB + chi-square in one call like PB200_EstimateDevice,
  * for callers that must not allocate device memory during a fit (real-time acquisition loops
  * with all device memory reserved in advance, hosts whose memory must come from their own
  * pools): it calls no cudaMalloc/cudaFree or other allocating routine. Its only scratch, the
