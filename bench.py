@@ -53,7 +53,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sigmaxy", choices=["sigmaxy", "xyibg", "astig", "spline", "mixed", "frames"])
-    ap.add_argument("--tile", type=int, default=1, help="mixed workload: ROIs a group takes per claim")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="mixed workload: ROIs a group takes per claim (0: the autotuner picks it and the "
+                         "register budget)")
     ap.add_argument("--n", type=int, default=None, help="ROIs per GPU (default: the workload's size)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -323,8 +325,9 @@ def mixed_estimator(pb, ctx, g):
 
 
 def run_mixed(args):
-    """Mixed workload: one persistent graph-replayed launch (fused) vs one launch per
-    (model, ROI size) bucket (plain), device-resident inputs; CPU and reference-GPU baselines."""
+    """Mixed workload: persistent graph-replayed launches (fused) vs one launch per (model, ROI
+    size) bucket (plain), device-resident inputs; claim size and register budget picked by the
+    autotuner unless --tile is given; CPU and reference-GPU baselines."""
     import torch
     import photonpy_b200 as pb
     from photonpy_b200 import roofline, synth
@@ -336,7 +339,13 @@ def run_mixed(args):
     ctx = pb.Context()
     ests = [mixed_estimator(pb, ctx, g) for g in groups]
     xs = [torch.from_numpy(g["samples"]).cuda() for g in groups]
-    mb = MixedBatch(list(zip(ests, xs)), tile_rois=args.tile, threads=args.threads)
+    tuned = None
+    tile, threads = args.tile, args.threads
+    if tile <= 0:
+        from photonpy_b200.autotune import tune_mixed
+        tuned = tune_mixed(list(zip(ests, xs)))
+        tile, threads = tuned["tile"], tuned["threads"]
+    mb = MixedBatch(list(zip(ests, xs)), tile_rois=tile, threads=threads)
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
         mb.run(s)
@@ -393,7 +402,8 @@ def run_mixed(args):
         metric=METRIC, value=n / (ms_fused * 1e-3), unit=UNIT, n_gpus=1, steps=args.steps, warmup=max(args.warmup, 3),
         ms_per_step=ms_fused, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
         data="synthetic (seeded Poisson ROIs, photonpy_b200.synth)",
-        config=dict(workload=w["desc"], rois=n, buckets=len(groups), tile_rois=args.tile, lanes_per_roi=4,
+        config=dict(workload=w["desc"], rois=n, buckets=len(groups), tile_rois=tile, threads_per_block=threads,
+                    autotuned=(tuned["timings"] if tuned else None), lanes_per_roi=4,
                     graph_replay=True, lm_iterations=MAX_IT, lm_lambda=LAMBDA,
                     l2="inputs of %.2f GB per step exceed the 126 MB L2" % (sum(x.numel() for x in xs) * 4 / 1e9)),
         plain_gpu=dict(value=n / (ms_plain * 1e-3), ms_per_step=ms_plain, launches_per_step=2 * len(groups),
