@@ -1209,9 +1209,18 @@ void mixed_enqueue(MixedPlan* p, cudaStream_t s) {
     PB_CUDA(cudaMemsetAsync(p->dCounter.p, 0, 2 * sizeof(int) * p->ntasks, s));
     launch_mixed(p->dTasks.as<MixedTask>(), p->ntasks, p->totalTiles, p->tileRois, p->dCounter.as<int>(),
                  p->strideFloats, p->variant, false, s);
-    if (p->anyFisher)
-        launch_mixed(p->dTasksFisher.as<MixedTask>(), p->ntasks, p->totalTiles, p->tileRois,
+    // A Fisher pass is one trip per ROI, so with one ROI per claim the claims themselves
+    // (atomics on a few counters) took a tenth of the LM pass's time on 4M ROIs. Its groups take
+    // about eight claims each instead (claims of 1..32 ROIs; 128 resident groups per SM).
+    if (p->anyFisher) {
+        long long fisherRois = 0;
+        for (const MixedTask& t : p->tasks)
+            if (t.a.crlb) fisherRois += t.a.n;
+        const long long perClaim = fisherRois / (8LL * 128 * num_sms());
+        const int chunk = (int)std::min<long long>(32, std::max<long long>(p->tileRois, perClaim));
+        launch_mixed(p->dTasksFisher.as<MixedTask>(), p->ntasks, p->totalTiles, chunk,
                      p->dCounter.as<int>() + p->ntasks, p->strideFloats, p->variant, true, s);
+    }
     for (int b = 0; b < p->ntasks; b++) {
         const FitArgs& a = p->tasks[b].a;
         if (a.crlb) launch_crlb(p->K[b], a.fisher, a.crlb, a.chisq, a.n, s);
