@@ -563,8 +563,7 @@ class ROIExtractorQueue : public FrameRing {
         int last = -1;
         for (int i = 0; i < n; i++) {
             if (rois[i].startframe < 0) throw FrameQueueError("ROIExtractor_Create: negative startframe");
-            spots_[i].roi = rois[i];
-            spots_[i].data.assign((size_t)std::max(0, rois[i].numframes) * rs_ * rs_, 0.0f);
+            spots_[i].roi = rois[i];  // its pixel buffer is allocated when its first box arrives
             last = std::max(last, rois[i].startframe);
         }
         // activation order: by start frame, then request order (a stable sort)
@@ -597,7 +596,7 @@ class ROIExtractorQueue : public FrameRing {
         for (size_t i = 0; i < take.size(); i++) {
             Spot& sp = spots_[take[i]];
             if (rois) rois[i] = sp.roi;
-            if (framedata) {
+            if (framedata && !sp.data.empty()) {
                 const int nf = std::min(std::max(0, sp.roi.numframes), roiframes_);
                 std::memcpy(framedata + (size_t)roiframes_ * box * i, sp.data.data(), sizeof(float) * box * nf);
             }
@@ -651,9 +650,11 @@ class ROIExtractorQueue : public FrameRing {
         }
         PBF_CUDA(cudaStreamSynchronize(stream_));  // also keeps the ring slots until the copy is done
         const float* hb = hBoxes_.as<float>();
-        for (int t = 0; t < T; t++)
-            std::memcpy(spots_[dest_[t].first].data.data() + box * dest_[t].second, hb + box * t,
-                        sizeof(float) * box);
+        for (int t = 0; t < T; t++) {
+            Spot& sp = spots_[dest_[t].first];
+            if (sp.data.empty()) sp.data.assign((size_t)sp.roi.numframes * box, 0.0f);
+            std::memcpy(sp.data.data() + box * dest_[t].second, hb + box * t, sizeof(float) * box);
+        }
         // records complete at frame startframe + max(numframes, 1) - 1: hand them out frame by
         // frame, each frame's in activation order
         std::lock_guard<std::mutex> lk(resMtx_);
