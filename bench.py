@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per ROI (0 = library default)")
-    ap.add_argument("--threads", type=int, default=256, help="threads per block")
+    ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library default)")
     ap.add_argument("--variant", type=int, default=None, help="Gaussian kernel family (0 column-blocked, 1 generic)")
     return ap.parse_args()
 
@@ -340,7 +340,7 @@ def run_mixed(args):
     ests = [mixed_estimator(pb, ctx, g) for g in groups]
     xs = [torch.from_numpy(g["samples"]).cuda() for g in groups]
     tuned = None
-    tile, threads = args.tile, args.threads
+    tile, threads = args.tile, args.threads or 256
     if tile <= 0:
         from photonpy_b200.autotune import tune_mixed
         tuned = tune_mixed(list(zip(ests, xs)))
@@ -369,7 +369,12 @@ def run_mixed(args):
             n0 = pb.launch_count()
             ms_fused = timed(lambda: mb.run(s), args.steps)
             launches = pb.launch_count() - n0
+        n0 = pb.launch_count()
+        mb.run_plain(s)
+        plain_launches = pb.launch_count() - n0
         ms_plain = timed(lambda: mb.run_plain(s), args.steps)
+        ms_plain_default = timed(lambda: mb.run_plain(s, lanes=None), args.steps)
+        mb.run(s)  # results of the fused path for the flop count below
     flops = 0.0
     for g, r in zip(groups, mb.results()):
         flops += roofline.localization_flops(g["kind"], g["R"], r["iterations"].cpu().numpy(), MAX_IT)
@@ -406,8 +411,12 @@ def run_mixed(args):
                     autotuned=(tuned["timings"] if tuned else None), lanes_per_roi=4,
                     graph_replay=True, lm_iterations=MAX_IT, lm_lambda=LAMBDA,
                     l2="inputs of %.2f GB per step exceed the 126 MB L2" % (sum(x.numel() for x in xs) * 4 / 1e9)),
-        plain_gpu=dict(value=n / (ms_plain * 1e-3), ms_per_step=ms_plain, launches_per_step=2 * len(groups),
-                       what="one fit launch + one CRLB launch per (model, ROI size) bucket, same kernels"),
+        plain_gpu=dict(value=n / (ms_plain * 1e-3), ms_per_step=ms_plain, launches_per_step=plain_launches,
+                       what="the LM, Fisher and CRLB launches of every (model, ROI size) bucket, same "
+                            "kernels and lanes per ROI"),
+        plain_gpu_default_config=dict(value=n / (ms_plain_default * 1e-3), ms_per_step=ms_plain_default,
+                                      what="the same per-bucket launches with each estimator's default "
+                                           "kernel configuration (2 lanes per ROI for the 7 and 9 px buckets)"),
         fused_over_plain=ms_plain / ms_fused,
         roofline=dict(bound="fp32", achieved=flops / (ms_fused * 1e-3) / 1e12, peak=peak, unit="TFLOP/s",
                       frac=flops / (ms_fused * 1e-3) / 1e12 / peak if peak else None, traffic=None,

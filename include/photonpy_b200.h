@@ -389,13 +389,16 @@ void PB200_MixedPlanDestroy(MixedPlan* plan);
 int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
                               const float* d_initial, float* d_params, int* d_iterations, float* d_crlb,
                               float* d_chisq, void* stream);
-/* Kernel configuration used for this estimator: lanes per ROI (4, 8, 16, 32; 0 = automatic)
- * and threads per block (64..256). Returns 0 on success. */
+/* Kernel configuration used for this estimator: lanes per ROI (2, 4, 8, 16, 32; 0 = automatic;
+ * 2 for the column-blocked Gaussian kernel with ROIs up to 10 pixels wide, otherwise the next
+ * supported count is used) and threads per block (64..256, a multiple of 32; 0 = automatic).
+ * Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
 /* Extension: the host-pointer pipeline of the Estimate/CRLB calls. The ROIs are fitted in chunks of
  * roisPerChunk (0: automatic), with `slots` chunks (2..4) in flight: while one chunk is fitted
  * the next ones are copied in and the previous ones copied out. Returns 0 or -1. */
 int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots);
+/* Lanes per ROI and threads per block the fit kernel of this estimator launches with. */
 void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock);
 /* Fit kernel family for the Gaussian models: 0 = column-blocked (default), 1 = generic
  * per-pixel table kernel (the spline model always uses 1). Returns 0 on success. */

@@ -50,8 +50,8 @@ def candidates(model: int, roisize: int):
     out = []
     variants = (1,) if model == 5 else (0, 1)
     for v in variants:
-        for g in (4, 8, 16, 32):
-            if v == 0 and math.ceil(roisize / g) > (2 if g == 32 else 4):
+        for g in ((2, 4, 8, 16, 32) if v == 0 else (4, 8, 16, 32)):
+            if v == 0 and math.ceil(roisize / g) > (2 if g == 32 else (5 if g == 2 else 4)):
                 continue
             if g > roisize * roisize:
                 continue

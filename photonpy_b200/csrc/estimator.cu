@@ -169,8 +169,13 @@ namespace {
 
 // Lanes per ROI when no tuned value is set: enough ROIs per warp to amortise the redundant
 // K x K solve for small ROIs, enough lanes to keep per-lane pixel loops short for large ones.
+// Flat-background Gaussians of 7..10 pixels: 2 lanes per ROI with 4 or 5 columns each (16 ROIs
+// per warp in the column-blocked kernel).
+bool gauss_two_lanes(int model, int R) { return model <= MODEL_XYZIBG && R >= 7 && R <= 10; }
+
 int default_lanes(int model, int R) {
     if (model_is_spline(model)) return R * R <= 100 ? 8 : 16;
+    if (gauss_two_lanes(model, R)) return 2;
     if (R <= 16) return 4;
     if (R <= 32) return 8;
     return 16;
@@ -232,7 +237,7 @@ struct Estimator {
     LMParams lm{30, 1e-15f, 0.0f};  // C++ default of the reference (Estimator.cpp:24)
     Context* ctx = nullptr;
     DevBuf coefs, coefsQ;  // spline coefficients: reference layout and the q-major copy
-    int lanes = 0, threads = 256;
+    int lanes = 0, threads = 0;  // 0: automatic
     int variant = 0;  // 0: column-blocked Gaussian kernel, 1: generic table kernel
     int device = 0;
     // Likelihood-ratio test estimator (GLRT_CreatePSF): diagnostics = {ll_on, ll_off, mean} per spot.
@@ -252,16 +257,35 @@ struct Estimator {
             if (s.stream) cudaStreamDestroy(s.stream);
     }
     int lanes_for() const { return lanes ? lanes : default_lanes(desc.model, desc.roisize); }
-    // Fit launcher for this estimator's model, ROI size and kernel configuration.
-    FitLaunch fit_launch() const {
-        int G = lanes_for();
+    // Lanes per ROI and columns per lane of the fit kernel this configuration launches (cpl 0:
+    // the generic table kernel, which starts at 4 lanes).
+    void fit_shape(int& G, int& cpl) const {
+        G = lanes_for();
+        cpl = 0;
         const int R = desc.roisize;
         if (desc.model <= MODEL_XYZIBG && variant == 0) {  // column-blocked kernel: flat-background Gaussians
-            while (G < 32 && (R + G - 1) / G > 4) G *= 2;
-            const int cpl = (R + G - 1) / G;
-            if (cpl <= (G == 32 ? 2 : 4)) return fit_launcher_for(desc.model, G, cpl, 0);
+            while (G < 32 && (R + G - 1) / G > gauss_max_cpl(G)) G *= 2;
+            const int c = (R + G - 1) / G;
+            if (c <= gauss_max_cpl(G)) {
+                cpl = c;
+                return;
+            }
         }
-        return fit_launcher_for(desc.model, G, 0, 1);
+        if (G < 4) G = 4;
+    }
+    // Threads per block: 128 for the 2-lane column-blocked kernel (measured faster than 64..256
+    // on 10x10 ROIs), 256 for the others.
+    int threads_for() const {
+        if (threads) return threads;
+        int G, cpl;
+        fit_shape(G, cpl);
+        return (cpl && G == 2) ? 128 : 256;
+    }
+    // Fit launcher for this estimator's model, ROI size and kernel configuration.
+    FitLaunch fit_launch() const {
+        int G, cpl;
+        fit_shape(G, cpl);
+        return fit_launcher_for(desc.model, G, cpl, cpl ? 0 : 1);
     }
     int npix() const { return desc.roisize * desc.roisize; }
     Slot& slot(int i) {
@@ -350,7 +374,7 @@ struct Chunking {
 // SigmaXY ROIs of 16x16 that fused form took 31.9 ms, the split 27.3 ms, and the single-pass
 // instances 24.4 ms, with the same results bit for bit. The Fisher launch reads the samples once
 // more from HBM.
-void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) { e->fit_launch()(e->desc, a, e->threads, s); }
+void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) { e->fit_launch()(e->desc, a, e->threads_for(), s); }
 
 // Host-pointer fit through the slot pipeline: H2D(c) + kernel(c) on slot c % slots are issued
 // before D2H(c - slots + 1), so the copies of one chunk overlap the fits of the others.
@@ -1109,8 +1133,10 @@ void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_par
 
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {
     if (!e) return -1;
-    if (lanesPerRoi != 0 && lanesPerRoi != 4 && lanesPerRoi != 8 && lanesPerRoi != 16 && lanesPerRoi != 32) return -1;
-    if (threadsPerBlock < 64 || threadsPerBlock > 256 || (threadsPerBlock & 31)) return -1;
+    if (lanesPerRoi != 0 && lanesPerRoi != 2 && lanesPerRoi != 4 && lanesPerRoi != 8 && lanesPerRoi != 16 &&
+        lanesPerRoi != 32)
+        return -1;
+    if (threadsPerBlock != 0 && (threadsPerBlock < 64 || threadsPerBlock > 256 || (threadsPerBlock & 31))) return -1;
     std::lock_guard<std::mutex> g(e->mtx);
     e->lanes = lanesPerRoi;
     e->threads = threadsPerBlock;
@@ -1134,8 +1160,11 @@ int PB200_SetKernelVariant(Estimator* e, int variant) {
 
 void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock) {
     if (!e) return;
-    if (lanesPerRoi) *lanesPerRoi = e->lanes_for();
-    if (threadsPerBlock) *threadsPerBlock = e->threads;
+    if (lanesPerRoi) {
+        int cpl;
+        e->fit_shape(*lanesPerRoi, cpl);
+    }
+    if (threadsPerBlock) *threadsPerBlock = e->threads_for();
 }
 
 int PB200_ModelInfo(Estimator* e, int* roisize) {

@@ -4,7 +4,7 @@
 namespace pb200 {
 
 FitLaunch fit_launcher_sigma(int G, int CPL, int variant) {
-    if (1 && variant == 0) return gauss_fit_table<GaussModel<MODEL_XYIBG_SIGMA>>(G, CPL);
+    if (variant == 0) return gauss_fit_table<GaussModel<MODEL_XYIBG_SIGMA>>(G, CPL);
     return generic_fit_table<GaussModel<MODEL_XYIBG_SIGMA>>(G);
 }
 

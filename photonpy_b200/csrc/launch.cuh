@@ -156,7 +156,11 @@ void launch_adjoint(const ModelDesc& d, AdjointArgs a, cudaStream_t s) {
     count_launch();
 }
 
-// Gaussian models: column-blocked kernel with CPL = ceil(R / G) (1..4).
+// Columns per lane the column-blocked kernel is built for: up to 5 with 2 lanes per ROI (ROIs
+// up to 10 pixels wide, 16 per warp), 4 with 4..16 lanes, 2 with 32.
+inline int gauss_max_cpl(int G) { return G == 32 ? 2 : (G == 2 ? 5 : 4); }
+
+// Gaussian models: column-blocked kernel with CPL = ceil(R / G) (1..gauss_max_cpl(G)).
 template <class M>
 FitLaunch gauss_fit_table(int G, int CPL) {
 #define PB_CASE(g)                                    \
@@ -168,6 +172,14 @@ FitLaunch gauss_fit_table(int G, int CPL) {
         default: return launch_fit_gauss<M, g, 4>;    \
         }
     switch (G) {
+    case 2:
+        switch (CPL) {
+        case 1: return launch_fit_gauss<M, 2, 1>;
+        case 2: return launch_fit_gauss<M, 2, 2>;
+        case 3: return launch_fit_gauss<M, 2, 3>;
+        case 4: return launch_fit_gauss<M, 2, 4>;
+        default: return launch_fit_gauss<M, 2, 5>;
+        }
         PB_CASE(4)
         PB_CASE(8)
         PB_CASE(16)
@@ -180,6 +192,7 @@ FitLaunch gauss_fit_table(int G, int CPL) {
 template <class M>
 FitLaunch generic_fit_table(int G) {
     switch (G) {
+    case 2:  // the per-pixel table kernel starts at 4 lanes per ROI
     case 4: return launch_fit_generic<M, 4>;
     case 8: return launch_fit_generic<M, 8>;
     case 16: return launch_fit_generic<M, 16>;

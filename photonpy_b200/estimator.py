@@ -317,14 +317,22 @@ class Estimator:
         check_error("ExpectedValueDevice")
         return (deriv, ev) if derivatives else ev
 
-    def SetKernelConfig(self, lanes_per_roi=0, threads_per_block=256, variant=None):
-        """Lanes per ROI (4, 8, 16, 32; 0 = automatic), threads per block and, for the Gaussian
-        models, the kernel family (0 = column-blocked, 1 = generic per-pixel table)."""
+    def SetKernelConfig(self, lanes_per_roi=0, threads_per_block=0, variant=None):
+        """Lanes per ROI (2, 4, 8, 16, 32; 0 = automatic), threads per block (64..256; 0 =
+        automatic) and, for the Gaussian models, the kernel family (0 = column-blocked, 1 =
+        generic per-pixel table)."""
         rc = self._lib.PB200_SetKernelConfig(self.inst, int(lanes_per_roi), int(threads_per_block))
         if rc == 0 and variant is not None:
             rc = self._lib.PB200_SetKernelVariant(self.inst, int(variant))
         if rc != 0:
             raise ValueError("invalid kernel configuration")
+        prev = self.kernel_config_setting()
+        self._kernel_setting = (int(lanes_per_roi), int(threads_per_block), prev[2] if variant is None else int(variant))
+
+    def kernel_config_setting(self):
+        """(lanes_per_roi, threads_per_block, variant) as last given to SetKernelConfig (0 =
+        automatic), for restoring a configuration; GetKernelConfig gives the values in use."""
+        return getattr(self, "_kernel_setting", (0, 0, 0))
 
     def SetHostPipeline(self, rois_per_chunk=0, slots=4):
         """Chunking of the host-array calls (Estimate, EstimateWithCRLB, ...): ROIs per chunk

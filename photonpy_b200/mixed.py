@@ -98,12 +98,22 @@ class MixedBatch:
         self.captured = True
         return self
 
-    def run_plain(self, stream=None):
-        """The same work as one launch (plus its CRLB kernel) per bucket."""
+    def run_plain(self, stream=None, lanes=4):
+        """The same work as single-model launches, bucket by bucket (LM, Fisher and CRLB
+        launches each). With lanes=4, the mixed kernel's lanes per ROI, the results are
+        bit-identical to run(); lanes=None keeps each estimator's own kernel configuration
+        (2 lanes per ROI for 7..10 pixel Gaussians by default, whose pixel sums then run in
+        another order)."""
         for b in self.buckets:
-            o = b["out"]
-            b["est"].EstimateDevice(b["samples"], constants=b["constants"], with_crlb=self.with_crlb, stream=stream,
-                                    out=o)
+            est, o = b["est"], b["out"]
+            saved = est.kernel_config_setting()
+            if lanes is not None:
+                est.SetKernelConfig(lanes, 0, variant=0)
+            try:
+                est.EstimateDevice(b["samples"], constants=b["constants"], with_crlb=self.with_crlb, stream=stream,
+                                   out=o)
+            finally:
+                est.SetKernelConfig(*saved)
         return self
 
     def results(self):

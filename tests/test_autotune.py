@@ -12,6 +12,8 @@ def test_candidates_respect_columns_per_lane():
     assert all(not (v == 0 and math.ceil(16 / g) > (2 if g == 32 else 4)) for v, g, t in c)
     assert all(v == 1 for v, _, _ in autotune.candidates(5, 13))  # spline: generic kernel only
     assert (0, 4, 128) not in autotune.candidates(0, 20)  # 20 px needs 5 columns per lane at 4 lanes
+    assert (0, 2, 256) in autotune.candidates(0, 10)  # 2 lanes x 5 columns
+    assert (0, 2, 256) not in autotune.candidates(0, 11)
 
 
 def test_choose_best_skips_failed_candidates():

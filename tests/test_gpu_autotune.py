@@ -31,6 +31,26 @@ def test_tune_estimator_applies_a_candidate(ctx, tmp_path):
     assert r2["cached"]
 
 
+def test_default_kernel_config(ctx):
+    """Automatic lanes and threads: 2 lanes x 128 threads for flat-background Gaussians up to
+    10 px wide, 4 x 256 up to 16 px; an explicit setting replaces them and 0 restores them."""
+    import photonpy_b200 as pb
+    gm = pb.GaussianPSFMethods(ctx)
+    small = gm.CreatePSF_XYIBg(10, 1.5, True)
+    assert small.GetKernelConfig() == (2, 128)
+    small.SetKernelConfig(8, 192)
+    assert small.GetKernelConfig() == (8, 192)
+    small.SetKernelConfig(0, 0)
+    assert small.GetKernelConfig() == (2, 128)
+    small.SetKernelConfig(0, 0, variant=1)  # generic table kernel: 2 lanes run as 4
+    assert small.GetKernelConfig() == (4, 256)
+    small.SetKernelConfig(2, 0, variant=0)
+    assert small.GetKernelConfig() == (2, 128)
+    assert gm.CreatePSF_XYIBgSigmaXY(16, [1.5, 1.5], True).GetKernelConfig() == (4, 256)
+    with pytest.raises(ValueError):
+        small.SetKernelConfig(3, 0)
+
+
 def test_tune_mixed_picks_a_candidate(ctx):
     import torch
     from photonpy_b200.autotune import tune_mixed

@@ -41,6 +41,32 @@ def test_mixed_launch_equals_plain_launches(ctx, tile):
     mb.close()
 
 
+def test_mixed_launch_close_to_default_config_launches(ctx):
+    """With each estimator's own configuration (2 lanes per ROI for the 7 and 9 px buckets)
+    the per-bucket launches sum pixels in another order: the fits agree to within float
+    rounding on the ROIs both sides converge on, and the estimators' settings are restored."""
+    import torch
+    from photonpy_b200.mixed import MixedBatch
+    buckets = _buckets(ctx, n=3000, seed=7)
+    before = [b[0].GetKernelConfig() for b in buckets]
+    assert any(c[0] == 2 for c in before)
+    mb = MixedBatch(buckets, tile_rois=1).run()
+    torch.cuda.synchronize()
+    fused = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
+    mb.run_plain(lanes=None)
+    torch.cuda.synchronize()
+    assert [b[0].GetKernelConfig() for b in buckets] == before
+    mb.run_plain()
+    assert [b[0].GetKernelConfig() for b in buckets] == before
+    mb.run_plain(lanes=None)
+    torch.cuda.synchronize()
+    for f, p in zip(fused, mb.results()):
+        conv = ((f["iterations"] < 50) & (p["iterations"] < 50)).cpu().numpy()
+        dp = (f["params"] - p["params"]).abs().cpu().numpy()[:, :2]
+        assert np.mean(np.all(dp[conv] < 1e-3, axis=1)) > 0.97
+    mb.close()
+
+
 def test_mixed_graph_replay(ctx):
     import torch
     from photonpy_b200.mixed import MixedBatch

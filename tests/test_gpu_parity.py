@@ -114,7 +114,7 @@ def test_fused_estimate_crlb_equals_separate_calls(name, ctx):
 
 
 @pytest.mark.parametrize("name", ["xyibg_r10", "sigmaxy_r16", "astig_r12", "constsigma_r9"])
-@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+@pytest.mark.parametrize("lanes", [2, 4, 8, 16, 32])
 def test_kernel_variants_agree(name, lanes, ctx):
     """The column-blocked kernel and the generic per-pixel table kernel, at every lanes-per-ROI
     setting, give the same fits (same arithmetic, different summation order)."""
