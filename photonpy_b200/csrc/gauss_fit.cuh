@@ -22,14 +22,21 @@
 namespace pb200 {
 
 // Shared-memory floats of one group: pixels, then max(y-terms, FP64 re-solve scratch,
-// Fisher scratch when the pixel area cannot hold it). Stride = 16 mod 32 so that the
-// 16-byte row loads of two neighbouring groups fall in complementary bank quads.
+// Fisher scratch when the pixel area cannot hold it) (base), and a stride of 16 mod 32 so
+// that the 16-byte row loads of two neighbouring 4-lane groups fall in complementary bank
+// quads (the mixed kernel's layout; the single-model launches pick their stride with
+// gauss_group_stride).
 template <int K>
-__host__ __device__ constexpr int gauss_group_floats(int R) {
+__host__ __device__ constexpr int gauss_group_base_floats(int R) {
     return round_up(round_up(R * R, 4) + cmax(cmax(4 * R, rescue_floats(K)),
                                               (round_up(R * R, 4) >= 4 * K * K) ? 0 : 4 * K * K),
-                    32) + 16;
+                    4);
 }
+template <int K>
+__host__ __device__ constexpr int gauss_group_floats(int R) {
+    return round_up(gauss_group_base_floats<K>(R), 32) + 16;
+}
+
 
 // ---------------------------------------------------------------------------------------
 // Separable accumulation of the Poisson Hessian and gradient.

@@ -4,6 +4,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -101,12 +104,68 @@ void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t
     if (a.crlb || a.glrt) launch_groups(fit_kernel<M, G, PASS_FISHER>, G, threads, stride, a.n, d, fisher_pass_args(a), s);
 }
 
+// Worst shared-memory bank conflict (threads per bank) of one warp of the column-blocked
+// kernel's pixel pass with group stride S: the sample reads (lane l of group g reads row y at
+// g*S + R*y + CPL*l + q, one float per column, or one float4 per row when CPL == 4 and R % 4
+// == 0, served 8 threads at a time), plus the y-term float4 read (one address per group,
+// broadcast to its lanes).
+inline int gauss_stride_conflicts(int S, int npix4, int R, int G, int CPL) {
+    const bool vec = CPL == 4 && (R & 3) == 0;
+    int worst = 1;
+    for (int y = 0; y < R; y++) {
+        for (int q = 0; q < (vec ? 1 : CPL); q++) {
+            for (int ph = 0; ph < (vec ? 4 : 1); ph++) {
+                int count[32] = {0};
+                const int t0 = vec ? ph * 8 : 0, t1 = vec ? t0 + 8 : 32;
+                for (int t = t0; t < t1; t++) {
+                    const int g = t / G, l = t % G, c = CPL * l + q;
+                    if (c >= R) continue;
+                    const int addr = g * S + R * y + c;
+                    for (int w = 0; w < (vec ? 4 : 1); w++) worst = std::max(worst, ++count[(addr + w) & 31]);
+                }
+            }
+        }
+    }
+    int ytab = 1;
+    for (int ph = 0; ph < 4; ph++) {
+        int count[32] = {0};
+        for (int g = ph * 8 / G; g <= (ph * 8 + 7) / G; g++)
+            for (int w = 0; w < 4; w++) ytab = std::max(ytab, ++count[(g * S + npix4 + w) & 31]);
+    }
+    return worst + ytab;
+}
+
+// Group stride of the single-model column-blocked launches: of base, base + 4, ..., base + 28
+// floats (base = gauss_group_base_floats), the smallest with the fewest bank conflicts in the
+// pixel pass. With the 16-mod-32 stride every second group of a warp read the same banks: 8-way
+// conflicts on the sample reads of 2-lane groups, 4-way with 4 lanes of 3 columns.
+template <int K>
+int gauss_group_stride(int R, int G, int CPL) {
+    static std::mutex mtx;
+    static std::map<long long, int> cache;
+    const long long key = ((long long)R << 16) | (G << 8) | CPL;
+    std::lock_guard<std::mutex> lock(mtx);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    const int base = gauss_group_base_floats<K>(R), npix4 = round_up(R * R, 4);
+    int best = base, bestCost = 1 << 30;
+    for (int S = base; S < base + 32; S += 4) {
+        const int c = gauss_stride_conflicts(S, npix4, R, G, CPL);
+        if (c < bestCost) {
+            bestCost = c;
+            best = S;
+        }
+    }
+    cache[key] = best;
+    return best;
+}
+
 // LM launch, then (when CRLB or GLRT values are requested) the Fisher launch at the fitted
 // parameters, each with its single-pass kernel instance.
 template <class M, int G, int CPL>
 void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
     if (a.n <= 0) return;
-    const int stride = gauss_group_floats<M::K>(d.roisize);
+    const int stride = gauss_group_stride<M::K>(d.roisize, G, CPL);
     if (a.flags & FIT_CRLB_ONLY) {
         launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, a, s);
         return;
