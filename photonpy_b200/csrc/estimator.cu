@@ -1313,14 +1313,31 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     t.handler = e->desc.model * 4 + cpl - 1;
                     p->totalTiles += (counts[b] + tileRois - 1) / tileRois;
                     switch (e->K) {
-                    case 4: p->strideFloats = std::max(p->strideFloats, gauss_group_floats<4>(e->desc.roisize)); break;
-                    case 5: p->strideFloats = std::max(p->strideFloats, gauss_group_floats<5>(e->desc.roisize)); break;
-                    default: p->strideFloats = std::max(p->strideFloats, gauss_group_floats<6>(e->desc.roisize)); break;
+                    case 4: p->strideFloats = std::max(p->strideFloats, gauss_group_base_floats<4>(e->desc.roisize)); break;
+                    case 5: p->strideFloats = std::max(p->strideFloats, gauss_group_base_floats<5>(e->desc.roisize)); break;
+                    default: p->strideFloats = std::max(p->strideFloats, gauss_group_base_floats<6>(e->desc.roisize)); break;
                     }
                     p->tasks.push_back(t);
                     p->K.push_back(e->K);
                 }
                 p->ntasks = (int)p->tasks.size();
+                {
+                    // group stride: of the largest bucket's floats + 0, 4, ..., 28, the one with the
+                    // fewest modelled bank conflicts over the buckets, weighted by their ROI counts
+                    const int base = p->strideFloats;
+                    long long bestCost = -1;
+                    for (int S = base; S < base + 32; S += 4) {
+                        long long cost = 0;
+                        for (const MixedTask& t : p->tasks) {
+                            const int R = t.d.roisize;
+                            cost += (long long)t.a.n * gauss_stride_conflicts(S, round_up(R * R, 4), R, G, (R + G - 1) / G);
+                        }
+                        if (bestCost < 0 || cost < bestCost) {
+                            bestCost = cost;
+                            p->strideFloats = S;
+                        }
+                    }
+                }
                 std::vector<MixedTask> lmTasks(p->tasks), fiTasks(p->tasks);
                 for (int b = 0; b < p->ntasks; b++) {
                     lmTasks[b].a = lm_pass_args(p->tasks[b].a);

@@ -22,19 +22,13 @@
 namespace pb200 {
 
 // Shared-memory floats of one group: pixels, then max(y-terms, FP64 re-solve scratch,
-// Fisher scratch when the pixel area cannot hold it) (base), and a stride of 16 mod 32 so
-// that the 16-byte row loads of two neighbouring 4-lane groups fall in complementary bank
-// quads (the mixed kernel's layout; the single-model launches pick their stride with
-// gauss_group_stride).
+// Fisher scratch when the pixel area cannot hold it). The launches space the groups by a
+// stride of at least this many floats chosen against bank conflicts (gauss_group_stride).
 template <int K>
 __host__ __device__ constexpr int gauss_group_base_floats(int R) {
     return round_up(round_up(R * R, 4) + cmax(cmax(4 * R, rescue_floats(K)),
                                               (round_up(R * R, 4) >= 4 * K * K) ? 0 : 4 * K * K),
                     4);
-}
-template <int K>
-__host__ __device__ constexpr int gauss_group_floats(int R) {
-    return round_up(gauss_group_base_floats<K>(R), 32) + 16;
 }
 
 
@@ -191,7 +185,7 @@ __device__ __forceinline__ void map_virtual(const float (&av)[NV], float (&acc)[
 }
 
 // Fit the ROIs roi, roi + roiStep, ... < roiEnd of one (model, ROI size) with one group of G
-// lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_floats floats). With
+// lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_base_floats floats). With
 // `claim` set, the group instead takes its ROIs, the first included, from that counter, roiStep
 // consecutive ROIs per atomicAdd of the group's first lane, so groups refill from a shared pool
 // until it runs out.
