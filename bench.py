@@ -366,9 +366,10 @@ def run_mixed(args):
 
     with torch.cuda.stream(s):
         with ClockSampler(0) as clk:
-            n0 = pb.launch_count()
             ms_fused = timed(lambda: mb.run(s), args.steps)
-            launches = pb.launch_count() - n0
+            n0 = pb.launch_count()
+            mb.run(s)  # launches of one step, counted outside the timed loop (which has warm-up runs)
+            launches = (pb.launch_count() - n0) * args.steps
         n0 = pb.launch_count()
         mb.run_plain(s)
         plain_launches = pb.launch_count() - n0
