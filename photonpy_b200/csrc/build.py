@@ -1,9 +1,11 @@
 """Build libphotonpy_b200.so (sm_100a) in-tree with nvcc.
 
-    python -m photonpy_b200.csrc.build [--verbose]
+    python -m photonpy_b200.csrc.build [--verbose] [--define NAME=VALUE ...] [--out PATH]
 
 Output: photonpy_b200/lib/libphotonpy_b200.so. The library statically links the CUDA
 runtime so that it does not depend on which libcudart other modules of the process load.
+--define passes compile-time switches (for example PB200_LM_IEEE_CHOL=1, see fit_common.cuh)
+and --out writes such a build elsewhere; PHOTONPY_B200_LIBRARY makes the package load it.
 """
 from __future__ import annotations
 
@@ -46,18 +48,21 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, defines=(), out: str | None = None) -> str:
+    lib_path = os.path.abspath(out) if out else LIB_PATH
+    obj_dir = OBJ_DIR if not out else os.path.join(os.path.dirname(lib_path), "_obj")
+    if not force and not out and not defines and up_to_date():
         return LIB_PATH
-    os.makedirs(LIB_DIR, exist_ok=True)
-    os.makedirs(OBJ_DIR, exist_ok=True)
+    os.makedirs(os.path.dirname(lib_path), exist_ok=True)
+    os.makedirs(obj_dir, exist_ok=True)
     common = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-O3", "-I", os.path.join(ROOT, "include")]
+    common += ["-D" + d for d in defines]
     if verbose:
         common += ["-Xptxas", "-v"]
 
     def compile_unit(u):
         src = os.path.join(HERE, u)
-        obj = os.path.join(OBJ_DIR, os.path.splitext(u)[0] + ".o")
+        obj = os.path.join(obj_dir, os.path.splitext(u)[0] + ".o")
         cmd = [nvcc(), *common, "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
@@ -69,18 +74,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if verbose:
         for _, log in results:
             sys.stderr.write(log)
-    tmp = LIB_PATH + f".tmp{os.getpid()}"
+    tmp = lib_path + f".tmp{os.getpid()}"
     cmd = [nvcc(), "-shared", *ARCH, "-o", tmp, *[o for o, _ in results], "-cudart", "static", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--define", action="append", default=[], help="NAME=VALUE compile-time switch")
+    ap.add_argument("--out", default=None, help="library path (default: the package's lib/)")
     args = ap.parse_args()
-    print(build(force=args.force, verbose=args.verbose))
+    print(build(force=args.force, verbose=args.verbose, defines=args.define, out=args.out))

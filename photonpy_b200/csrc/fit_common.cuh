@@ -6,12 +6,25 @@
 //  * damping lambda > 0: a_kk += lambda * sum_j a_jk^2 (scale invariant); lambda < 0: a_kk -= lambda;
 //  * the Cholesky factorization fails (LM stops) only on an exactly-zero pivot;
 //  * Fisher inverse by LUP with partial pivoting and tolerance 1e-9 (failure -> +Inf CRLB).
-// By design: pivots are applied through rsqrt products instead of IEEE divides; a pivot that
-// lost more than six decimal digits (v <= 1e-6 * a_kk, including v < 0) is re-solved in FP64;
-// the Fisher matrix is inverted in FP64 instead of FP32.
+// By design: a pivot that lost more than six decimal digits (v <= 1e-6 * a_kk, including
+// v < 0) is re-solved in FP64; the Fisher matrix is inverted in FP64 instead of FP32.
+//
+// Arithmetic of the LM step, chosen at compile time:
+//   PB200_LM_IEEE_RCP  1: the per-pixel weight uses the IEEE reciprocal 1/mu, as
+//                         Estimation.h:116-117 does; 0: the approximate reciprocal (1 ulp).
+//   PB200_LM_IEEE_CHOL 1: the damped Cholesky solve takes square roots and divides with the
+//                         reference's operation order and no contraction (SolveMatrix.h:107-163,
+//                         Estimation.h:213-223); 0: pivots applied through rsqrt products.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#ifndef PB200_LM_IEEE_RCP
+#define PB200_LM_IEEE_RCP 0
+#endif
+#ifndef PB200_LM_IEEE_CHOL
+#define PB200_LM_IEEE_CHOL 0
+#endif
 
 namespace pb200 {
 
@@ -92,12 +105,87 @@ __device__ __forceinline__ float rcp_fast(float x) {
     return r;
 }
 
+// 1/mu of the per-pixel LM weight (x >= 1e-6).
+__device__ __forceinline__ float lm_rcp(float x) {
+#if PB200_LM_IEEE_RCP
+    return __frcp_rn(x);
+#else
+    return rcp_fast(x);
+#endif
+}
+
+// Damped LM step with the reference's arithmetic: damping (Estimation.h:213-223), Cholesky
+// (SolveMatrix.h:107-125) and the two triangular solves (SolveMatrix.h:145-163), each sum
+// formed left to right with separately rounded products, square roots and quotients IEEE
+// rounded. Same return codes as lm_solve below.
+template <int K, int NACC>
+__device__ __forceinline__ int lm_solve_ieee(const float (&acc)[NACC], float lambda, float (&step)[K], float (&dk)[K]) {
+    constexpr int NA = K * (K + 1) / 2;
+    float A[K][K];
+    {
+        int q = 0;
+#pragma unroll
+        for (int i = 0; i < K; i++)
+#pragma unroll
+            for (int j = i; j < K; j++) {
+                A[i][j] = acc[q];
+                A[j][i] = acc[q];
+                q++;
+            }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        float s = 0.0f;
+#pragma unroll
+        for (int j = 0; j < K; j++) s = __fadd_rn(s, __fmul_rn(A[j][k], A[j][k]));
+        dk[k] = (lambda < 0.0f) ? __fsub_rn(A[k][k], lambda) : __fadd_rn(A[k][k], __fmul_rn(s, lambda));
+    }
+    float L[K][K];
+    int status = 1;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int p = 0; p < k; ++p) sum = __fadd_rn(sum, __fmul_rn(L[k][p], L[k][p]));
+        const float v = __fsub_rn(dk[k], sum);
+        if (v == 0.0f) status = 0;
+        else if (!(v > 1e-6f * dk[k]) && status == 1) status = 2;  // also catches v < 0 and NaN
+        L[k][k] = __fsqrt_rn(v);
+#pragma unroll
+        for (int i = k + 1; i < K; ++i) {
+            float s2 = 0.0f;
+#pragma unroll
+            for (int p = 0; p < k; ++p) s2 = __fadd_rn(s2, __fmul_rn(L[i][p], L[k][p]));
+            L[i][k] = __fdiv_rn(__fsub_rn(A[i][k], s2), L[k][k]);
+        }
+    }
+    float y[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = 0; k < i; ++k) sum = __fadd_rn(sum, __fmul_rn(L[i][k], y[k]));
+        y[i] = __fdiv_rn(__fsub_rn(acc[NA + i], sum), L[i][i]);
+    }
+#pragma unroll
+    for (int i = K - 1; i >= 0; --i) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int k = i + 1; k < K; ++k) sum = __fadd_rn(sum, __fmul_rn(L[k][i], step[k]));
+        step[i] = __fdiv_rn(__fsub_rn(y[i], sum), L[i][i]);
+    }
+    return status;
+}
+
 // Damped LM step in registers. acc = [alpha upper packed (NA) | beta (K) | extra].
 // Returns 1 on success, 0 on an exactly-zero pivot (reference failure), 2 when a pivot is
 // weak and the step must be re-solved in FP64. (Two-dimensional arrays and running packed
 // indices keep every access compile-time after unrolling, so nothing lands in local memory.)
 template <int K, int NACC>
 __device__ __forceinline__ int lm_solve(const float (&acc)[NACC], float lambda, float (&step)[K], float (&dk)[K]) {
+#if PB200_LM_IEEE_CHOL
+    return lm_solve_ieee<K, NACC>(acc, lambda, step, dk);
+#endif
     constexpr int NA = K * (K + 1) / 2;
     float A[K][K];
     {

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256) fit_kernel(const ModelDesc d, const FitAr
                     // ComputeLevMarAlphaBeta (Estimation.h:109-128)
                     const float sv = s < 1e-6f ? 1e-6f : s;
                     const float muc = mu > 1e-6f ? mu : 1e-6f;
-                    const float invmu = rcp_nr(muc);
+                    const float invmu = PB200_LM_IEEE_RCP ? __frcp_rn(muc) : rcp_nr(muc);
                     const float t = __fmul_rn(sv, invmu);
                     w = __fmul_rn(t, invmu);
                     const float bf = __fsub_rn(1.0f, t);

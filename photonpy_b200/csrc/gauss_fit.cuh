@@ -337,7 +337,7 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                             // ComputeLevMarAlphaBeta (Estimation.h:109-128); a NaN sample counts as 1e-6
                             const float sval = fmaxf(s, 1e-6f);
                             const float muc = fmaxf(mu, 1e-6f);
-                            const float invmu = rcp_fast(muc);
+                            const float invmu = lm_rcp(muc);
                             const float t = __fmul_rn(sval, invmu);
                             w = __fmul_rn(t, invmu);
                             row_add_b<V>(U, __fsub_rn(1.0f, t), X[q]);

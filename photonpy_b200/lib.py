@@ -49,7 +49,9 @@ _callbacks = []
 
 
 def library_path() -> str:
-    return LIB_PATH
+    """The library the package loads: PHOTONPY_B200_LIBRARY when set (another build of the same
+    sources, e.g. with different compile-time switches), else the in-tree build."""
+    return os.environ.get("PHOTONPY_B200_LIBRARY") or LIB_PATH
 
 
 def load_library() -> ctypes.CDLL:
@@ -57,10 +59,12 @@ def load_library() -> ctypes.CDLL:
     global _cdll
     with _load_lock:
         if _cdll is None:
-            from .csrc import build as _build
-            if not _build.up_to_date():
-                _build.build()
-            _cdll = ctypes.CDLL(LIB_PATH)
+            path = library_path()
+            if path == LIB_PATH:
+                from .csrc import build as _build
+                if not _build.up_to_date():
+                    _build.build()
+            _cdll = ctypes.CDLL(path)
             _bind_common(_cdll)
     return _cdll
 
@@ -126,7 +130,7 @@ class SMLM:
             raise RuntimeError("The SMLM library can only be used with 64-bit python.")
         self.debugMode = debugMode
         self.lib = load_library()
-        self.lib_path = LIB_PATH
+        self.lib_path = library_path()
         smlmlib = self.lib
         self.numDevices = smlmlib.CudaGetNumDevices()
         self._CudaSetDevice = smlmlib.CudaSetDevice

@@ -100,3 +100,43 @@ def parity_stats(name, ref_params, ref_its, params, its, maxit=50):
         frac_capped_ref=float(np.mean(~conv_ref)),
         max_dpos_converged=float(dpos[both].max()) if both.any() else 0.0,
     )
+
+
+def ref_estimator(name, g, cuda):
+    """The reference's own estimator (oracle/_ref build) for a golden set; cuda selects its GPU
+    kernels, else its CPU path (the one the golden vectors come from)."""
+    from oracle import ref_lib
+    R = int(g["roisize"])
+    if name.startswith("xyibg"):
+        return ref_lib.RefEstimator("XYIBg", R, cuda=cuda, sigma=tuple(g["sigma"]))
+    if name.startswith("constsigma"):
+        return ref_lib.RefEstimator("XYIBgConstSigma", R, cuda=cuda)
+    if name.startswith("sigma_"):
+        return ref_lib.RefEstimator("XYIBgSigma", R, cuda=cuda, sigma=tuple(g["sigma"]))
+    if name.startswith("sigmaxy"):
+        return ref_lib.RefEstimator("XYIBgSigmaXY", R, cuda=cuda, sigma=tuple(g["sigma"]))
+    if name.startswith("astig"):
+        return ref_lib.RefEstimator("XYZIBg", R, cuda=cuda, astig=(g["astig_x"][:4], g["astig_y"][:4]),
+                                    zrange=tuple(g["zrange"]))
+    if name.startswith("spline"):
+        mode = 1 if "tilted" in name else (2 if "bgimage" in name else 0)
+        coefs = ref_lib.spline_compute(g["zstack"], border=1)
+        return ref_lib.RefEstimator("CSpline", R, cuda=cuda, coefs=coefs, spline_zrange=tuple(g["spline_zrange"]),
+                                    spline_mode=mode)
+    if name.startswith("tiltedbg"):
+        return ref_lib.RefEstimator("XYITiltedBg", R, cuda=cuda)
+    if name.startswith("tiltedsxy"):
+        return ref_lib.RefEstimator("XYITiltedBgSigmaXY", R, cuda=cuda, sigma=tuple(g["sigma"]))
+    raise KeyError(name)
+
+
+def ref_fit(est, samples, constants=None, chunk=20000):
+    """(params, iterations) of a reference estimator, in chunks (its CPU path starts one thread
+    per spot)."""
+    ps, its = [], []
+    for s in range(0, len(samples), chunk):
+        c = None if constants is None else constants[s:s + chunk]
+        p, it, _ = est.estimate(samples[s:s + chunk], constants=c, trace_len=0)
+        ps.append(p)
+        its.append(it)
+    return np.concatenate(ps), np.concatenate(its)
