@@ -78,6 +78,10 @@ WORKLOADS = {
 }
 
 
+# seed of each workload's batch (rank r of the GPU arm draws with seed + 1000 r)
+BASE_SEED = {"sigmaxy": 2, "xyibg": 1, "astig": 3, "spline": 4}
+
+
 def make_data(workload, n, seed, device=None):
     from photonpy_b200 import synth
     synth.use_torch(device, seed)
@@ -145,40 +149,83 @@ def oracle_model(d):
     raise ValueError(k)
 
 
-def cpu_localize(d, samples):
+def cpu_localize(d, samples, keep=False):
     """photonpy's CPU estimator (reference build) — or the oracle port when it is absent —
     on `samples`: Estimate + ChiSquareAndCRLB, in chunks of 20k spots (the reference starts one
-    thread per spot). Returns (seconds, kind)."""
+    thread per spot). Returns (seconds, kind), plus (params, iterations, crlb) with keep."""
     from oracle import ref_lib
+    out = ([], [], [])
     t0 = time.perf_counter()
     if ref_lib.available():
         est = ref_estimator(d)
         for s in range(0, len(samples), 20000):
             chunk = samples[s:s + 20000]
-            p, _, _ = est.estimate(chunk, trace_len=0)
-            est.crlb_chisq(p, chunk)
+            p, it, _ = est.estimate(chunk, trace_len=0)
+            crlb, _ = est.crlb_chisq(p, chunk)
+            if keep:
+                for lst, v in zip(out, (p, it, crlb)):
+                    lst.append(v)
         est.close()
         kind = "reference"
     else:
         m = oracle_model(d)
         for s in range(0, len(samples), 20000):
             chunk = samples[s:s + 20000]
-            p, _ = m.fit(chunk)
-            m.crlb(p, chunk)
+            p, it = m.fit(chunk)
+            crlb, _ = m.crlb(p, chunk)
+            if keep:
+                for lst, v in zip(out, (p, it, crlb)):
+                    lst.append(v)
         kind = "port"
-    return time.perf_counter() - t0, kind
+    dt = time.perf_counter() - t0
+    if keep:
+        return dt, kind, tuple(np.concatenate(v) for v in out)
+    return dt, kind
 
 
 def cpu_baseline(d, budget_s):
+    """The CPU estimator timed on the first ROIs of the batch (about budget_s of work); also
+    returns its results on those ROIs (params, iterations, crlb) for the parity check."""
     samples = d["samples"]
     n0 = min(len(samples), 2000)
     t, kind = cpu_localize(d, samples[:n0])
     rate = n0 / max(t, 1e-6)
     n = int(min(len(samples), max(n0, rate * budget_s)))
-    t, kind = cpu_localize(d, samples[:n])
+    t, kind, res = cpu_localize(d, samples[:n], keep=True)
     return dict(value=n / t, unit=UNIT, cores=os.cpu_count(), kind=kind,
                 sample=f"first {n} ROIs of the same batch ({d['kind']} {d['R']}x{d['R']}), "
-                       f"Estimate + ChiSquareAndCRLB, {t:.1f} s")
+                       f"Estimate + ChiSquareAndCRLB, {t:.1f} s"), res
+
+
+POS_TOL = {"XYIBg": (1e-3, 1e-3), "XYIBgSigmaXY": (1e-3, 1e-3), "XYZIBg": (1e-3, 1e-3, 1.0),
+           "CSpline": (1e-3, 1e-3, 1e-3)}
+
+
+def parity_summary(kind, ref, ours, maxit=MAX_IT):
+    """Agreement of the GPU results with the CPU estimator's on the same ROIs, stratified by
+    converged (both iteration counts <= maxit) and capped (the reference hit the cap): fractions
+    of spots with positions within 1e-3 px (z: 1 nm astig, 1e-3 um spline), I and bg within 1e-4
+    relative, CRLB within 1e-4 relative, iteration counts equal, converged flags equal."""
+    (rp, rit, rcrlb), (p, it, crlb) = ref, ours
+    tol = np.array(POS_TOL[kind])
+    npos = len(tol)
+    pos_ok = np.all(np.abs(p[:, :npos] - rp[:, :npos]) <= tol, axis=1)
+    phot = np.abs(p[:, npos:npos + 2] - rp[:, npos:npos + 2]) / np.maximum(np.abs(rp[:, npos:npos + 2]), 1e-6)
+    phot_ok = np.all(phot <= 1e-4, axis=1)
+    crlb_ok = np.all(np.abs(crlb - rcrlb) <= 1e-4 * np.abs(rcrlb), axis=1)
+    conv_ref, conv = rit <= maxit, it <= maxit
+    both = conv_ref & conv
+    capped = ~conv_ref
+
+    def frac(m, sel):
+        return float(np.mean(m[sel])) if sel.any() else None
+
+    out = dict(n=int(len(it)), capped_ref=float(np.mean(capped)), it_match=float(np.mean(it == rit)),
+               conv_flag_match=float(np.mean(conv == conv_ref)))
+    for name, sel in (("converged", both), ("capped", capped)):
+        out[name] = {"n": int(sel.sum()), "pos_within_1e-3": frac(pos_ok, sel), "I_bg_within_1e-4": frac(phot_ok, sel),
+                     "crlb_within_1e-4": frac(crlb_ok, sel), "it_match": frac(it == rit, sel)}
+    return out
 
 
 class ClockSampler:
@@ -288,7 +335,14 @@ def run_reference(args):
     if rank != 0:
         return
     w = WORKLOADS[args.workload]
-    d = make_data(args.workload, min(args.n or w["n"], 200_000), seed=2 if args.workload == "sigmaxy" else 1)
+    # the same draws as rank 0 of the GPU arm: same seed, and the Poisson stream from the same
+    # torch generator on the GPU when one is present (the data path only; the fits run on the CPU)
+    try:
+        import torch
+        device = "cuda" if torch.cuda.is_available() else None
+    except ImportError:
+        device = None
+    d = make_data(args.workload, args.n or w["n"], seed=BASE_SEED[args.workload], device=device)
     from oracle import ref_lib
     n_cal = 2000
     t, kind = cpu_localize(d, d["samples"][:n_cal])
@@ -306,6 +360,8 @@ def run_reference(args):
                 warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f32", data="synthetic (seeded Poisson ROIs)",
                 config=dict(workload=w["desc"], roi_size=d["R"], model=d["kind"], rois_per_step=per_step,
+                            batch=len(d["samples"]), seed=BASE_SEED[args.workload],
+                            draws="torch generator on the GPU, as the GPU arm" if device else "numpy (no GPU)",
                             lm_iterations=MAX_IT, lm_lambda=LAMBDA),
                 cpu_baseline=dict(value=value, unit=UNIT, cores=os.cpu_count(), kind=kind,
                                   sample=f"{per_step} ROIs per step ({d['kind']} {d['R']}x{d['R']}), "
@@ -625,8 +681,7 @@ def main():
 
     w = WORKLOADS[args.workload]
     n = args.n or w["n"]
-    base_seed = {"sigmaxy": 2, "xyibg": 1, "astig": 3, "spline": 4}[args.workload]
-    d = make_data(args.workload, n, seed=base_seed + 1000 * rank, device=f"cuda:{local}")
+    d = make_data(args.workload, n, seed=BASE_SEED[args.workload] + 1000 * rank, device=f"cuda:{local}")
     smp = d["samples"]
     K = roofline.K_OF[d["kind"]]
 
@@ -693,10 +748,10 @@ def main():
             fn(est.inst, n, h_smp.data_ptr(), None, None, h_par.data_ptr(), h_its.data_ptr(), h_crlb.data_ptr(),
                h_chi.data_ptr())
         from photonpy_b200.lib import check_error
-        check_error("PB200_EstimateCRLB")
 
         for _ in range(2):
             e2e_step()
+        check_error("PB200_EstimateCRLB")
         if world > 1:
             dist.barrier()
         tt = []
@@ -704,6 +759,7 @@ def main():
             t0 = time.perf_counter()
             e2e_step()
             tt.append(time.perf_counter() - t0)
+        check_error("PB200_EstimateCRLB")
         et = torch.tensor([float(np.mean(tt))], device="cuda")
         if world > 1:
             dist.all_reduce(et, op=dist.ReduceOp.MAX)
@@ -714,9 +770,13 @@ def main():
         # results through the host path equal the device path
         assert np.array_equal(h_par.numpy(), out["params"].cpu().numpy())
 
-    cpu = ref_gpu = None
+    cpu = ref_gpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(d, args.cpu_seconds)
+        cpu, ref_res = cpu_baseline(d, args.cpu_seconds)
+        m = len(ref_res[1])
+        ours = (out["params"][:m].cpu().numpy(), out["iterations"][:m].cpu().numpy(), out["crlb"][:m].cpu().numpy())
+        parity = parity_summary(d["kind"], ref_res, ours)
+        parity["sample"] = f"the first {m} ROIs of the timed batch, against the CPU estimator ({cpu['kind']})"
         ref_gpu = reference_gpu_plain(d)
 
     if rank == 0:
@@ -740,7 +800,7 @@ def main():
             roofline_hbm=dict(bound="hbm", achieved=hbm_gbs, peak=hbm_peak(peaks)[0], unit="GB/s",
                               frac=hbm_gbs / hbm_peak(peaks)[0],
                               note="algorithmic ROI-stream bytes, " + hbm_peak(peaks)[1]),
-            e2e=e2e, cpu_baseline=cpu, reference_gpu_plain=ref_gpu, gpu_launches=int(launches),
+            e2e=e2e, cpu_baseline=cpu, parity=parity, reference_gpu_plain=ref_gpu, gpu_launches=int(launches),
             clocks=clk.summary(),
         )
         print(json.dumps(line), flush=True)
