@@ -381,7 +381,9 @@ void PB200_MixedPlanDestroy(MixedPlan* plan);
  * pools): it calls no cudaMalloc/cudaFree or other allocating routine. Its only scratch, the
  * packed Fisher rows, lives in a fixed device array of 32768 spots x 22 floats (2.75 MiB per
  * GPU that loads the library, kept until exit), so numspots above 32768 is rejected with an
- * error (split the batch). All pointers are device memory; d_crlb is required, d_iterations and
+ * error (split the batch), and so is an estimator of more than 6 parameters (the tilted-
+ * background SigmaXY Gaussian, the spline tilted-background mode), whose Fisher rows do not
+ * fit a 22-float row; such calls launch nothing. All pointers are device memory; d_crlb is required, d_iterations and
  * d_chisq may be NULL. The first call on a device looks up the array's device address; make
  * that first call before any stream capture. Every call shares the array and overwrites the
  * rows it uses, so calls whose kernels overlap on the GPU (other streams, other threads) race:

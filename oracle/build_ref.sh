@@ -9,16 +9,32 @@
 # under oracle/_ref/src, which is deleted again after the build so that only
 # the shared library remains. No reference source is kept in the repository.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT
+#    or: PHOTONPY_REFERENCE_ROOT=<photonpy checkout> oracle/build_ref.sh
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${PHOTONPY_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "usage: $0 REFERENCE_ROOT (or set PHOTONPY_REFERENCE_ROOT)" >&2
+  exit 2
+fi
 SRC_ROOT="$REF/cpp/SMLMLib"
 OUT="$HERE/_ref"
 TMP="$OUT/src"
 if [ ! -d "$SRC_ROOT" ]; then
   echo "reference sources not found at $SRC_ROOT" >&2
   exit 1
+fi
+# photonpy's own Python binding of the estimator, unmodified, beside the library (git-ignored
+# like it): the drop-in test loads it over libphotonpy_b200.so. PB_REF_PYTHON_ONLY=1 stops here.
+PY_OUT="$OUT/photonpy_cpp"
+mkdir -p "$PY_OUT"
+for f in lib context estimator gaussian cspline estim_queue; do
+  cp "$REF/photonpy/cpp/$f.py" "$PY_OUT/$f.py"
+done
+if [ "${PB_REF_PYTHON_ONLY:-0}" = 1 ]; then
+  echo "copied photonpy's binding to $PY_OUT"
+  exit 0
 fi
 rm -rf "$TMP"
 mkdir -p "$TMP"

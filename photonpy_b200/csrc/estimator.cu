@@ -1494,7 +1494,7 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
             a.flags = 0;
             const cudaStream_t s = (cudaStream_t)stream;
             launch_fit_fisher(e, a, s);
-            launch_crlb(e->K, scratch, d_crlb, d_chisq, numspots, s);
+            launch_crlb(e->K, scratch, d_crlb, d_chisq, numspots, s, e->crlbAbs);
             return 0;
         },
         -1);

@@ -135,10 +135,12 @@ inline int gauss_stride_conflicts(int S, int npix4, int R, int G, int CPL) {
     return worst + ytab;
 }
 
-// Group stride of the single-model column-blocked launches: of base, base + 4, ..., base + 28
-// floats (base = gauss_group_base_floats), the smallest with the fewest bank conflicts in the
-// pixel pass. With the 16-mod-32 stride every second group of a warp read the same banks: 8-way
-// conflicts on the sample reads of 2-lane groups, 4-way with 4 lanes of 3 columns.
+// Group stride of the single-model column-blocked launches: of base, base + 4, ... up to
+// round_up(base, 32) + 16 floats (base = gauss_group_base_floats; the upper end keeps a block's
+// shared memory, and so the block size that fits, no larger than with a fixed 16-mod-32 stride),
+// the smallest with the fewest bank conflicts in the pixel pass. With the 16-mod-32 stride every
+// second group of a warp read the same banks: 8-way conflicts on the sample reads of 2-lane
+// groups, 4-way with 4 lanes of 3 columns.
 template <int K>
 int gauss_group_stride(int R, int G, int CPL) {
     static std::mutex mtx;
@@ -149,7 +151,8 @@ int gauss_group_stride(int R, int G, int CPL) {
     if (it != cache.end()) return it->second;
     const int base = gauss_group_base_floats<K>(R), npix4 = round_up(R * R, 4);
     int best = base, bestCost = 1 << 30;
-    for (int S = base; S < base + 32; S += 4) {
+    const int last = round_up(base, 32) + 16;
+    for (int S = base; S <= last; S += 4) {
         const int c = gauss_stride_conflicts(S, npix4, R, G, CPL);
         if (c < bestCost) {
             bestCost = c;

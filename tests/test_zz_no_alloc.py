@@ -91,3 +91,55 @@ def test_no_alloc_rejects_batches_above_capacity(ctx):
     assert "32768" in msg
     pblib.clear_error()
     est.Destroy()
+
+
+def test_no_alloc_full_capacity_and_no_device_allocation(ctx):
+    """A batch of exactly 32768 spots uses the last row of the fixed array and still equals the
+    allocating entry point; warmed-up calls leave the device's free memory unchanged."""
+    import torch
+    import photonpy_b200 as pb
+    L = _bind(pb.load_library())
+    g = load_golden("xyibg_r10")
+    est = cuda_estimator("xyibg_r10", g, ctx)
+    reps = -(-MAX_SPOTS // len(g["samples"]))
+    smp = np.ascontiguousarray(np.tile(g["samples"], (reps, 1, 1))[:MAX_SPOTS])
+    x = torch.from_numpy(smp).cuda()
+    want = _run(L, est, x, None, False, torch)
+    got = _run(L, est, x, None, True, torch)
+    for w, h in zip(want, got):
+        assert np.array_equal(w, h)
+    # the last spot is a copy of a golden spot fitted in the first rows
+    j = (MAX_SPOTS - 1) % len(g["samples"])
+    assert np.array_equal(got[0][-1], got[0][j]) and np.array_equal(got[2][-1], got[2][j])
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        _run(L, est, x, None, True, torch)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    est.Destroy()
+
+
+def test_no_alloc_rejects_more_than_six_parameters(ctx):
+    """The tilted-background SigmaXY Gaussian has 8 parameters; its Fisher rows do not fit the
+    fixed array's rows, so the call fails before launching anything."""
+    import torch
+    import photonpy_b200 as pb
+    from photonpy_b200 import lib as pblib
+    L = _bind(pb.load_library())
+    g = load_golden("tiltedsxy_r11")
+    est = cuda_estimator("tiltedsxy_r11", g, ctx)
+    assert est.numparams == 8
+    x = torch.from_numpy(np.ascontiguousarray(g["samples"][:64])).cuda()
+    params = torch.full((64, 8), -1.0, device="cuda")
+    crlb = torch.full((64, 8), -1.0, device="cuda")
+    n0 = pb.launch_count()
+    rc = L.PB200_EstimateCRLBNoAlloc(est.inst, 64, x.data_ptr(), None, None, params.data_ptr(), None,
+                                     crlb.data_ptr(), None, torch.cuda.current_stream().cuda_stream)
+    assert rc == -1
+    assert "parameters" in pb.last_error()
+    assert pb.launch_count() == n0
+    torch.cuda.synchronize()
+    assert torch.all(params == -1.0) and torch.all(crlb == -1.0)
+    pblib.clear_error()
+    est.Destroy()
