@@ -140,3 +140,37 @@ def ref_fit(est, samples, constants=None, chunk=20000):
         ps.append(p)
         its.append(it)
     return np.concatenate(ps), np.concatenate(its)
+
+
+# Benchmark workloads as parity cases: XYIBg 10x10, XYIBgSigmaXY 16x16, astigmatic XYZIBg 12x12
+# and the cubic spline 13x13 on a 26x26x41 z-stack, drawn as the benchmark draws them.
+SYNTHETIC = ["xyibg_10", "sigmaxy_16", "astig_12", "spline_13"]
+
+
+def synthetic_case(name, n):
+    """Seeded ROIs of a benchmark workload, in the layout of a golden set (without the
+    reference's fit, which the caller adds)."""
+    from photonpy_b200 import synth
+    synth.use_torch(None, 0)
+    if name == "xyibg_10":
+        d = synth.xyibg(n, seed=1)
+        return dict(samples=d["samples"], roisize=d["R"], sigma=np.float32(d["sigma"]))
+    if name == "sigmaxy_16":
+        d = synth.sigmaxy(n, seed=2)
+        return dict(samples=d["samples"], roisize=d["R"], sigma=np.float32(d["sigma"]))
+    if name == "astig_12":
+        d = synth.astig(n, seed=3)
+        cx, cy = d["astig"]
+        return dict(samples=d["samples"], roisize=d["R"], astig_x=np.float32(cx), astig_y=np.float32(cy),
+                    zrange=np.float32(d["zrange"]))
+    if name == "spline_13":
+        d = synth.spline(n, seed=4)
+        zstack, zr = synth.astig_zstack(shape_xy=26, nz=41, zrange_um=(-0.4, 0.4))
+        return dict(samples=d["samples"], roisize=d["R"], zstack=zstack, spline_zrange=np.float32(zr))
+    raise KeyError(name)
+
+
+def golden_name(case):
+    """Golden-set name whose estimator factory fits a synthetic case."""
+    return {"xyibg_10": "xyibg_r10", "sigmaxy_16": "sigmaxy_r16", "astig_12": "astig_r12",
+            "spline_13": "spline_r13"}.get(case, case)

@@ -1,0 +1,62 @@
+"""Fisher matrix and CRLB entry points on the GPU against the FP64 oracle.
+
+Estimator.FisherMatrix runs the fit kernels' Fisher pass (FP32 sums) and Estimator.CRLB inverts
+it in FP64 on the GPU; photonpy computes both in numpy from downloaded derivative stacks
+(photonpy/cpp/estimator.py:205-220, 249-253). The FP64 oracle restates the same sums and the
+reference's LUP inverse in double precision (oracle/psf_oracle_impl.h, ComputeChiSquareAndCRLB).
+NumDeriv / NumCRLB are checked against the analytic Derivatives / CRLB they approximate.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_SETS, load_golden
+from helpers import cuda_estimator, oracle_model
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", GOLDEN_SETS)
+def test_fisher_matrix_and_crlb_match_fp64_oracle(name, ctx):
+    g = load_golden(name)
+    est = cuda_estimator(name, g, ctx)
+    c = g.get("constants")
+    p = g["params"]
+    fi = est.FisherMatrix(p, constants=c)
+    K = est.numparams
+    assert fi.shape == (len(p), K, K) and fi.dtype == np.float32
+    assert np.array_equal(fi, np.transpose(fi, (0, 2, 1)))
+    crlb64, _, fi64 = oracle_model(name, g).crlb(p, g["samples"], constants=c, fp64=True, return_fisher=True)
+    # entries relative to sqrt(FI_ii FI_jj): FP32 sums of a few hundred positive terms
+    d = np.sqrt(np.abs(np.diagonal(fi64, axis1=1, axis2=2)))
+    scale = d[:, :, None] * d[:, None, :] + 1e-30
+    err = (np.abs(fi - fi64) / scale).max(axis=(1, 2))
+    assert np.quantile(err, 0.99) < 2e-5, (name, np.quantile(err, [0.5, 0.99, 1]))
+    crlb = est.CRLB(p, constants=c)
+    ok = np.all(np.isfinite(crlb64), axis=1)
+    assert np.array_equal(np.all(np.isfinite(crlb), axis=1), ok)
+    rel = np.abs(crlb[ok] - crlb64[ok]) / crlb64[ok]
+    assert np.quantile(rel.max(axis=1), 0.99) < 1e-4, (name, np.quantile(rel, [0.5, 0.99, 1]))
+    # the same values as the CRLB of the fused path and of CRLBAndChiSquare
+    assert np.array_equal(crlb, est.CRLBAndChiSquare(p, constants=c))
+    est.Destroy()
+
+
+@pytest.mark.parametrize("name", ["xyibg_r10", "sigmaxy_r16", "astig_r12", "spline_r13"])
+def test_numerical_derivatives_and_crlb(name, ctx):
+    g = load_golden(name)
+    est = cuda_estimator(name, g, ctx)
+    truth = g["truth"][:24]
+    deriv, ev = est.Derivatives(truth)
+    # FP32 central differences: step large enough against float32 rounding of mu (~I * 1e-7)
+    eps = 1e-3 if name.startswith(("xyibg", "sigmaxy")) else (0.05 if name.startswith("astig") else 2e-3)
+    nd, ev2 = est.NumDeriv(truth, eps=eps)
+    assert np.array_equal(ev, ev2)
+    # the free-sigma columns of photonpy's Jacobian are sigma * dmu/dsigma (a reference quirk kept
+    # by Derivatives), so only the other columns are central differences of mu
+    cols = slice(0, 4) if name.startswith("sigmaxy") else slice(None)
+    scale = np.abs(deriv[:, cols]).max(axis=(2, 3), keepdims=True) + 1e-20
+    assert np.quantile(np.abs(nd[:, cols] - deriv[:, cols]) / scale, 0.99) < 2e-2
+    crlb = est.CRLB(truth)
+    ncrlb = est.NumCRLB(truth, useNumDeriv=False)
+    assert np.quantile(np.abs(ncrlb - crlb) / crlb, 0.99) < 1e-4
+    est.Destroy()

@@ -2,34 +2,72 @@
 
 Tolerances are those of the task statement: x/y within 1e-3 px (z within 1 nm, or 1e-3 um
 for the spline whose z is in micrometres), I and bg within 1e-4 relative, CRLB within 1e-4
-relative. Iteration-count agreement is asserted against per-model floors: photonpy's own
-FP32 result changes under a rounding-only perturbation (enabling FMA contraction in its CPU
-build changes the iteration count of 0.2% of XYIBg, 2.2% of SigmaXY and 34.8% of astig
-spots), and our pixel sums are reduced in a tree rather than sequentially.
+relative. Iteration counts and converged flags cannot match to 99.9%: photonpy's own results
+move under rounding alone. Its own CUDA build (one thread per ROI, the CPU's summation order,
+CUDA's erff/expf and FMA contraction) matches its CPU build on 98.7% (XYIBg 10x10), 94.3%
+(SigmaXY 16x16), 46.8% (astig 12x12) and 65.4% (spline 13x13) of 20,000 benchmark ROIs each.
+test_iteration_match_reaches_reference_gpu_floor measures that floor live and asserts this
+library reaches it; the golden-set floors below are that floor on each golden set, less one
+binomial standard deviation of a 300-400 spot set where this library sits below it.
 """
 import numpy as np
 import pytest
 
 from conftest import GOLDEN_SETS, load_golden
-from helpers import cuda_estimator, oracle_model, parity_stats, coefs_sha
+from helpers import (SYNTHETIC, coefs_sha, cuda_estimator, golden_name, oracle_model, parity_stats,
+                     ref_estimator, ref_fit, synthetic_case)
 
 pytestmark = pytest.mark.gpu
 
-# minimum fractions per golden set: iteration-count match, converged-spot position and
-# photometry agreement (I, bg within 1e-4 relative)
+# minimum fractions per golden set: iteration-count match (the reference GPU build's match on
+# the set, measured on a B200: 99.25 / 97.33 / 99.00 / 94.50 / 47.25 / 68.67 / 99.00 / 100 /
+# 66.33 / 70.33 %), converged-spot position and photometry agreement (I, bg within 1e-4 relative)
 FLOORS = {
-    "xyibg_r10": dict(it_match=0.97, pos_ok_converged=0.995, phot_ok_converged=0.97),
-    "constsigma_r9": dict(it_match=0.97, pos_ok_converged=0.995, phot_ok_converged=0.97),
-    "sigma_r11": dict(it_match=0.85, pos_ok_converged=0.97, phot_ok_converged=0.90),
-    "sigmaxy_r16": dict(it_match=0.75, pos_ok_converged=0.95, phot_ok_converged=0.85),
-    "astig_r12": dict(it_match=0.40, pos_ok_converged=0.97, phot_ok_converged=0.85),
-    "spline_r13": dict(it_match=0.40, pos_ok_converged=0.95, phot_ok_converged=0.85),
-    "tiltedbg_r11": dict(it_match=0.90, pos_ok_converged=0.99, phot_ok_converged=0.90),
+    "xyibg_r10": dict(it_match=0.99, conv_flag_match=1.0, pos_ok_converged=1.0, phot_ok_converged=1.0),
+    "constsigma_r9": dict(it_match=0.96, conv_flag_match=1.0, pos_ok_converged=1.0, phot_ok_converged=1.0),
+    "sigma_r11": dict(it_match=0.985, conv_flag_match=1.0, pos_ok_converged=1.0, phot_ok_converged=1.0),
+    "sigmaxy_r16": dict(it_match=0.94, conv_flag_match=0.965, pos_ok_converged=0.985, phot_ok_converged=0.985),
+    "astig_r12": dict(it_match=0.44, conv_flag_match=0.94, pos_ok_converged=1.0, phot_ok_converged=1.0),
+    "spline_r13": dict(it_match=0.68, conv_flag_match=0.97, pos_ok_converged=1.0, phot_ok_converged=1.0),
+    "tiltedbg_r11": dict(it_match=0.98, conv_flag_match=1.0, pos_ok_converged=1.0, phot_ok_converged=1.0),
     # every spot runs to the iteration cap in the reference (its tilt columns move mu not at all)
-    "tiltedsxy_r11": dict(conv_flag_match=0.99, pos_ok=0.5),
-    "spline_tilted_r13": dict(it_match=0.40, pos_ok_converged=0.95, phot_ok_converged=0.85),
-    "spline_bgimage_r13": dict(it_match=0.40, pos_ok_converged=0.95, phot_ok_converged=0.85),
+    "tiltedsxy_r11": dict(conv_flag_match=1.0, it_match=1.0, pos_ok=0.99),
+    "spline_tilted_r13": dict(it_match=0.66, conv_flag_match=0.97, pos_ok_converged=1.0, phot_ok_converged=1.0),
+    "spline_bgimage_r13": dict(it_match=0.70, conv_flag_match=0.94, pos_ok_converged=1.0, phot_ok_converged=1.0),
 }
+
+
+@pytest.mark.parametrize("name", SYNTHETIC)
+def test_iteration_match_reaches_reference_gpu_floor(name, ctx):
+    """20,000 ROIs of a benchmark workload: the reference's CPU build fits them (the oracle of
+    record), so does the reference's own CUDA build (the floor), so does this library. This
+    library's iteration-count and converged-flag match with the CPU build must reach the CUDA
+    build's, within 2.5 binomial standard deviations of the difference (about 0.25 percentage
+    points at these rates), and its converged positions must agree as well as the CUDA build's."""
+    from oracle import ref_lib
+    if not ref_lib.available():
+        pytest.skip("reference build absent (oracle/build_ref.sh)")
+    n = 20000
+    g = synthetic_case(name, n)
+    gname = golden_name(name)
+    cpu = ref_estimator(gname, g, cuda=False)
+    p_cpu, it_cpu = ref_fit(cpu, g["samples"])
+    cpu.close()
+    gpu = ref_estimator(gname, g, cuda=True)
+    p_gpu, it_gpu = ref_fit(gpu, g["samples"], chunk=n)
+    gpu.close()
+    est = cuda_estimator(gname, g, ctx)
+    p, _, _, its = est.Estimate(g["samples"], return_iterations=True)
+    est.Destroy()
+    floor = parity_stats(gname, p_cpu, it_cpu, p_gpu, it_gpu)
+    ours = parity_stats(gname, p_cpu, it_cpu, p, its)
+    print(name, "floor", floor, "ours", ours)
+    for key in ("it_match", "conv_flag_match"):
+        f = floor[key]
+        margin = 2.5 * np.sqrt(2 * f * (1 - f) / n) + 1e-4
+        assert ours[key] >= f - margin, (name, key, ours[key], f)
+    assert ours["pos_ok_converged"] >= floor["pos_ok_converged"] - 2e-3, (name, ours, floor)
+    assert ours["phot_ok_converged"] >= floor["phot_ok_converged"] - 2e-3, (name, ours, floor)
 
 
 @pytest.mark.parametrize("name", GOLDEN_SETS)
@@ -125,8 +163,9 @@ def test_kernel_variants_agree(name, lanes, ctx):
     p0, _, _, it0 = est.Estimate(g["samples"], constants=c, return_iterations=True)
     est.SetKernelConfig(lanes, 256, variant=1)
     p1, _, _, it1 = est.Estimate(g["samples"], constants=c, return_iterations=True)
-    conv = (it0 <= 50) & (it1 <= 50)
     st = parity_stats(name, p0, it0, p1, it1)
-    assert st["pos_ok_converged"] >= 0.97, st
-    assert np.mean(it0 == it1) >= 0.4, st
+    assert st["pos_ok_converged"] >= 0.98, st
+    # two summation orders differ by rounding only; the astig model's stop limit on I (1e-4
+    # photons, below FP32 resolution) makes its iteration count follow rounding noise
+    assert np.mean(it0 == it1) >= {"astig_r12": 0.4, "sigmaxy_r16": 0.88}.get(name, 0.93), st
     est.Destroy()
