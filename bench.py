@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--lanes", type=int, default=0, help="lanes per ROI (0 = library default)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library default)")
     ap.add_argument("--variant", type=int, default=None, help="Gaussian kernel family (0 column-blocked, 1 generic)")
+    ap.add_argument("--B", type=float, default=0.0, dest="astig_B",
+                    help="astig workload: quartic term B of sigma(z) (0: photonpy's 4-coefficient form; the "
+                         "reference cannot express B != 0, so its CPU baseline is then the oracle port)")
     return ap.parse_args()
 
 
@@ -82,7 +85,7 @@ WORKLOADS = {
 BASE_SEED = {"sigmaxy": 2, "xyibg": 1, "astig": 3, "spline": 4}
 
 
-def make_data(workload, n, seed, device=None):
+def make_data(workload, n, seed, device=None, astig_B=0.0):
     from photonpy_b200 import synth
     synth.use_torch(device, seed)
     if workload == "sigmaxy":
@@ -90,13 +93,19 @@ def make_data(workload, n, seed, device=None):
     if workload == "xyibg":
         return synth.xyibg(n, seed=seed)
     if workload == "astig":
-        return synth.astig(n, seed=seed)
+        return synth.astig(n, seed=seed, B=astig_B)
     if workload == "spline":
         d = synth.spline(n, seed=seed)
         zstack, zr = synth.astig_zstack(shape_xy=26, nz=41, zrange_um=(-0.4, 0.4))
         d["zstack"], d["spline_zrange"] = zstack, zr
         return d
     raise ValueError(workload)
+
+
+def workload_desc(args, w):
+    if args.workload == "astig" and args.astig_B:
+        return w["desc"].replace("(reference 4-term form)", f"(quartic term B = {args.astig_B:g}, FP64-oracle extension)")
+    return w["desc"]
 
 
 def make_estimator(pb, ctx, d):
@@ -108,6 +117,8 @@ def make_estimator(pb, ctx, d):
         return G.CreatePSF_XYIBgSigmaXY(d["R"], d["sigma"], True)
     if k == "XYZIBg":
         cx, cy = d["astig"]
+        if cx[4] != 0 or cy[4] != 0:
+            return G.CreatePSF_XYZIBg(d["R"], pb.Gauss3D_CalibrationB(cx, cy, d["zrange"]), True)
         return G.CreatePSF_XYZIBg(d["R"], pb.Gauss3D_Calibration(cx[:4], cy[:4], d["zrange"]), True)
     if k == "CSpline":
         sm = pb.CSplineMethods(ctx)
@@ -156,7 +167,7 @@ def cpu_localize(d, samples, keep=False):
     from oracle import ref_lib
     out = ([], [], [])
     t0 = time.perf_counter()
-    if ref_lib.available():
+    if ref_lib.available() and not has_quartic_term(d):
         est = ref_estimator(d)
         for s in range(0, len(samples), 20000):
             chunk = samples[s:s + 20000]
@@ -181,6 +192,11 @@ def cpu_localize(d, samples, keep=False):
     if keep:
         return dt, kind, tuple(np.concatenate(v) for v in out)
     return dt, kind
+
+
+def has_quartic_term(d):
+    """The astig workload with B != 0, which photonpy's model cannot express."""
+    return d["kind"] == "XYZIBg" and (d["astig"][0][4] != 0 or d["astig"][1][4] != 0)
 
 
 def cpu_baseline(d, budget_s):
@@ -342,7 +358,7 @@ def run_reference(args):
         device = "cuda" if torch.cuda.is_available() else None
     except ImportError:
         device = None
-    d = make_data(args.workload, args.n or w["n"], seed=BASE_SEED[args.workload], device=device)
+    d = make_data(args.workload, args.n or w["n"], seed=BASE_SEED[args.workload], device=device, astig_B=args.astig_B)
     from oracle import ref_lib
     n_cal = 2000
     t, kind = cpu_localize(d, d["samples"][:n_cal])
@@ -359,7 +375,7 @@ def run_reference(args):
     line = dict(impl="reference", metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
                 warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f32", data="synthetic (seeded Poisson ROIs)",
-                config=dict(workload=w["desc"], roi_size=d["R"], model=d["kind"], rois_per_step=per_step,
+                config=dict(workload=workload_desc(args, w), roi_size=d["R"], model=d["kind"], rois_per_step=per_step,
                             batch=len(d["samples"]), seed=BASE_SEED[args.workload],
                             draws="torch generator on the GPU, as the GPU arm" if device else "numpy (no GPU)",
                             lm_iterations=MAX_IT, lm_lambda=LAMBDA),
@@ -627,7 +643,7 @@ def reference_gpu_plain(d, m=50_000):
     through its host API, Estimate + ChiSquareAndCRLB, on the first m ROIs of the batch; host
     copies included, as photonpy always has them."""
     from oracle import ref_lib
-    if not ref_lib.available() or d["kind"] not in ("XYIBg", "XYIBgSigmaXY", "XYZIBg"):
+    if not ref_lib.available() or d["kind"] not in ("XYIBg", "XYIBgSigmaXY", "XYZIBg") or has_quartic_term(d):
         return None
     sub = d["samples"][:m]
     est = ref_gpu_estimator(d)
@@ -681,7 +697,8 @@ def main():
 
     w = WORKLOADS[args.workload]
     n = args.n or w["n"]
-    d = make_data(args.workload, n, seed=BASE_SEED[args.workload] + 1000 * rank, device=f"cuda:{local}")
+    d = make_data(args.workload, n, seed=BASE_SEED[args.workload] + 1000 * rank, device=f"cuda:{local}",
+                  astig_B=args.astig_B)
     smp = d["samples"]
     K = roofline.K_OF[d["kind"]]
 
@@ -788,7 +805,8 @@ def main():
             metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
             ms_per_step=ms_max, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
             data="synthetic (seeded Poisson ROIs, photonpy_b200.synth)",
-            config=dict(workload=w["desc"], model=d["kind"], roi_size=d["R"], rois_per_gpu=n, global_rois=world * n,
+            config=dict(workload=workload_desc(args, w), model=d["kind"], roi_size=d["R"], rois_per_gpu=n,
+                        global_rois=world * n,
                         lm_iterations=MAX_IT, lm_lambda=LAMBDA, mean_iterations=float(np.minimum(its, MAX_IT).mean()),
                         kernel_config=list(est.GetKernelConfig()),
                         l2="inputs of %.2f GB per step exceed the 126 MB L2; no flush needed" % (smp.nbytes / 1e9),

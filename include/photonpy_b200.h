@@ -345,6 +345,23 @@ void PB200_EstimateDeviceDiag(Estimator* e, int numspots, const float* d_sample,
                               float* d_crlb, float* d_chisq, void* stream);
 void PB200_ChiSquareAndCRLBDevice(Estimator* e, int numspots, const float* d_params, const float* d_sample,
                                   const float* d_constants, float* d_crlb, float* d_chisq, void* stream);
+/* PB200_EstimateDevice without the CRLB, reporting per spot whether any LM step of its fit was
+ * re-solved in FP64 (d_rescued[numspots]: 1 or 0). The FP32 damped Cholesky solve hands a step to
+ * an FP64 re-solve when a pivot keeps less than a millionth of its diagonal entry (v <= 1e-6 a_kk,
+ * or v < 0), where the reference's FP32 Cholesky (SolveMatrix.h:107-125) returns an inaccurate or
+ * NaN step; an exactly zero pivot still ends the fit as in the reference. */
+void PB200_EstimateDeviceRescued(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                                 const float* d_initial, float* d_params, int* d_iterations, float* d_trace,
+                                 int traceBufLen, int* d_rescued, void* stream);
+/* Replaces photonpy's numpy Estimator.FisherMatrix (photonpy/cpp/estimator.py:205-220), which
+ * sums Derivatives/ExpectedValue on the host: the Fisher matrices of the Poisson likelihood at
+ * params, FI_ij = sum_p J_i J_j / max(mu_p, 1e-8) (FP32 sums, the matrix the CRLB inverts),
+ * computed on the GPU by the Fisher pass. Host pointers; fisher[numspots][K][K] (symmetric). */
+void PB200_FisherMatrix(Estimator* e, int numspots, const float* params, const float* constants, float* fisher);
+/* Device form: packed rows d_fisherRows[numspots][K(K+1)/2 + 1], the upper triangle row by row
+ * (FI_00, FI_01, ..., FI_0K-1, FI_11, ...) then one float left 0 (no samples, no chi-square). */
+void PB200_FisherMatrixDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
+                              float* d_fisherRows, void* stream);
 /* Adjoint of the summed Poisson NLL (no reference counterpart). For each spot n:
  * nll[n] = sum_p mu_p - x_p log(max(mu_p, 1e-6)); dparams[n][k] = g_n dNLL_n/dtheta_k (true
  * derivatives, also for sigma); d_dcalib is ACCUMULATED into (zero it first): sum_n g_n dNLL_n/dcal

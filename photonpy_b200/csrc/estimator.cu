@@ -378,9 +378,11 @@ void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) { e->fit_
 
 // Host-pointer fit through the slot pipeline: H2D(c) + kernel(c) on slot c % slots are issued
 // before D2H(c - slots + 1), so the copies of one chunk overlap the fits of the others.
+// h_fisher (with FIT_CRLB_ONLY): the packed FP32 Fisher rows [n][K(K+1)/2 + 1] themselves are
+// copied out instead of (or besides) being inverted.
 void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, const float* h_initial,
               float* h_params, int* h_iters, float* h_trace, int traceLen, float* h_crlb, float* h_chisq,
-              int flags, float* h_glrt = nullptr) {
+              int flags, float* h_glrt = nullptr, float* h_fisher = nullptr) {
     std::lock_guard<std::mutex> g(e->mtx);
     PB_CUDA(cudaSetDevice(e->device));
     const int K = e->K, NC = e->numconst, npix = e->npix();
@@ -434,6 +436,10 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         if (wantGlrt)
             PB_CUDA(cudaMemcpyAsync(h_glrt + (size_t)p.start * 3, s.glrt.as<float>(), sizeof(float) * 3 * p.count,
                                     cudaMemcpyDeviceToHost, s.stream));
+        if (h_fisher)
+            PB_CUDA(cudaMemcpyAsync(h_fisher + (size_t)p.start * fisher_row_floats(K), s.fisher.as<float>(),
+                                    sizeof(float) * fisher_row_floats(K) * p.count, cudaMemcpyDeviceToHost,
+                                    s.stream));
     };
     for (int c = 0; c < nchunks; c++) {
         const int start = chunks[c].first, count = chunks[c].second;
@@ -460,10 +466,8 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
             s.trace.ensure(sizeof(float) * (size_t)traceLen * K * count);
             PB_CUDA(cudaMemsetAsync(s.trace.p, 0, sizeof(float) * (size_t)traceLen * K * count, s.stream));
         }
-        if (h_crlb) {
-            s.crlb.ensure(sizeof(float) * K * count);
-            s.fisher.ensure(sizeof(float) * fisher_row_floats(K) * count);
-        }
+        if (h_crlb) s.crlb.ensure(sizeof(float) * K * count);
+        if (h_crlb || h_fisher) s.fisher.ensure(sizeof(float) * fisher_row_floats(K) * count);
         if (h_chisq || h_crlb) s.chisq.ensure(sizeof(float) * count);
         FitArgs a{};
         a.smp = h_smp ? s.smp.as<float>() : nullptr;
@@ -479,7 +483,7 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         a.maxIter = e->lm.iterations;
         a.lambda = e->lm.lambda;
         a.flags = flags;
-        a.fisher = h_crlb ? s.fisher.as<float>() : nullptr;
+        a.fisher = (h_crlb || h_fisher) ? s.fisher.as<float>() : nullptr;
         if (wantGlrt) {
             s.glrt.ensure(sizeof(float) * 3 * count);
             a.glrt = s.glrt.as<float>();
@@ -1069,6 +1073,37 @@ void Estimator_ChiSquareAndCRLB(Estimator* e, const float* params, const float* 
            });
 }
 
+void PB200_FisherMatrix(Estimator* e, int numspots, const float* params, const float* constants, float* fisher) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e);
+        if (numspots < 0 || !params || !fisher) throw Error("FisherMatrix: bad arguments");
+        const int K = e->K, R = fisher_row_floats(K);
+        std::vector<float> rows((size_t)numspots * R);
+        host_fit(e, numspots, nullptr, constants, params, nullptr, nullptr, nullptr, 0, nullptr, nullptr,
+                 FIT_CRLB_ONLY, nullptr, rows.data());
+        for (size_t i = 0; i < (size_t)numspots; i++) {
+            const float* r = rows.data() + i * R;
+            float* f = fisher + i * K * K;
+            for (int a = 0, q = 0; a < K; a++)
+                for (int b = a; b < K; b++, q++) f[a * K + b] = f[b * K + a] = r[q];
+        }
+    });
+}
+
+void PB200_FisherMatrixDevice(Estimator* e, int numspots, const float* d_params, const float* d_constants,
+                              float* d_fisherRows, void* stream) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e);
+        if (numspots < 0 || !d_params || !d_fisherRows) throw Error("FisherMatrixDevice: bad arguments");
+        if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+        FitArgs a{}; a.smp = nullptr; a.consts = d_constants; a.initial = d_params; a.params = nullptr;
+        a.fisher = d_fisherRows; a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda;
+        a.flags = FIT_CRLB_ONLY;
+        launch_fit_fisher(e, a, (cudaStream_t)stream);});
+}
+
 void PB200_EstimateCRLB(Estimator* e, int numspots, const float* sample, const float* constants,
                         const float* initial, float* params, int* iterations, float* crlb, float* chisq) {
     if (numspots == 0) return;
@@ -1105,6 +1140,21 @@ void PB200_EstimateDeviceDiag(Estimator* e, int numspots, const float* d_sample,
             a.glrt = d_diag;
             a.glrtMeanRoi = e->glrtRefMean ? d_sample : nullptr;
         }
+        run_fit_device(e, a, (cudaStream_t)stream);});
+}
+
+void PB200_EstimateDeviceRescued(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
+                                 const float* d_initial, float* d_params, int* d_iterations, float* d_trace,
+                                 int traceBufLen, int* d_rescued, void* stream) {
+    if (numspots == 0) return;
+    guarded_void([&]() {
+        check_estimator(e);
+        if (numspots < 0 || !d_sample || !d_params || !d_rescued) throw Error("EstimateDeviceRescued: bad arguments");
+        if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
+        FitArgs a{}; a.smp = d_sample; a.consts = d_constants; a.initial = d_initial; a.params = d_params;
+        a.iterations = d_iterations; a.trace = traceBufLen > 0 ? d_trace : nullptr;
+        a.traceLen = traceBufLen > 0 && d_trace ? traceBufLen : 0; a.diag = d_rescued;
+        a.n = numspots; a.maxIter = e->lm.iterations; a.lambda = e->lm.lambda; a.flags = 0;
         run_fit_device(e, a, (cudaStream_t)stream);});
 }
 

@@ -246,14 +246,17 @@ __device__ __forceinline__ int lm_solve(const float (&acc)[NACC], float lambda, 
 }
 
 // FP64 Cholesky solve by one lane. A: packed upper (float, NA), b: K, dk: damped diagonal.
-// Scratch: D packed lower (double, NA), y (double, K). Writes x (float, K); false on a zero pivot.
+// Scratch: D packed lower (double, NA), y (double, K). Writes x (float, K). Returns false when a
+// pivot is zero or negative: the FP32 Hessian is then not positive definite even in FP64 (its
+// accumulation rounding exceeds what is left of the pivot), and the fit stops at its current
+// parameters, as the reference's fit does on a zero pivot, instead of taking a NaN step.
 static __device__ __noinline__ bool lm_solve_fp64_lane(int K, const float* A, const float* b, const float* dk, double* D,
                                                double* y, float* x) {
     for (int k = 0; k < K; ++k) {
         double sum = 0.0;
         for (int p = 0; p < k; ++p) sum += D[lok(k, p)] * D[lok(k, p)];
         const double v = (double)dk[k] - sum;
-        if (v == 0.0) return false;
+        if (!(v > 0.0)) return false;
         D[lok(k, k)] = sqrt(v);
         for (int i = k + 1; i < K; ++i) {
             double s2 = 0.0;

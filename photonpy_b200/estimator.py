@@ -76,6 +76,8 @@ class Estimator:
         self._Estimator_SetLMParams.argtypes = [Inst, ct.POINTER(LevMarParams)]
         self._Estimator_GetLMParams = lib.Estimator_GetLMParams
         self._Estimator_GetLMParams.argtypes = [Inst, ct.POINTER(LevMarParams)]
+        lib.PB200_FisherMatrix.argtypes = [Inst, ct.c_int32, _F32, _F32, _F32]
+        lib.PB200_FisherMatrix.restype = None
         self._EstimateCRLB = lib.PB200_EstimateCRLB
         self._EstimateCRLB.argtypes = [Inst, ct.c_int32, _F32, NullableFloatArrayType, NullableFloatArrayType, _F32,
                                        NullableIntArrayType, NullableFloatArrayType, NullableFloatArrayType]
@@ -97,36 +99,39 @@ class Estimator:
 
     # ------------------------------------------------------------------ helpers
     def _checkparams(self, params, constants, roipos):
-        params = np.array(params)
-        if len(params.shape) == 1:
-            params = [params]
-        params = np.ascontiguousarray(params, dtype=np.float32)
-        numspots = len(params)
+        """Normalise the per-spot arguments of one call (the contract of photonpy's Estimator,
+        photonpy/cpp/estimator.py:155-186): params as float32 [n, K] (one parameter vector is one
+        spot), constants as float32 [n, numconst] (required when the model has constants; any
+        array with n*numconst values, or one that broadcasts to [n, numconst]), ROI positions as
+        int32 [n, indexdims] (zeros when omitted). Raises ValueError when a shape does not fit."""
+        p = np.asarray(params, dtype=np.float32)
+        if p.ndim == 1:
+            p = p.reshape(1, -1)
+        p = np.ascontiguousarray(p)
+        n = p.shape[0]
+        nc = self.numconst
         if constants is None:
-            if self.numconst != 0:
-                raise ValueError(f"Estimator is expecting constant array with shape {[len(params), self.numconst]} "
-                                 f"(None given) ")
-            constants = np.zeros((numspots, self.numconst), dtype=np.float32)
+            if nc:
+                raise ValueError(f"the estimator needs {nc} constants per spot: pass an array of shape {(n, nc)}")
+            c = np.zeros((n, 0), dtype=np.float32)
         else:
-            constants = np.ascontiguousarray(constants, dtype=np.float32)
-            if constants.size != numspots * self.numconst:
+            c = np.asarray(constants, dtype=np.float32)
+            if c.size == n * nc:
+                c = np.ascontiguousarray(c.reshape(n, nc))
+            else:
                 try:
-                    constants_ = np.zeros([numspots, self.numconst], dtype=np.float32)
-                    constants_[:, :] = constants
-                    constants = constants_
-                except Exception:
-                    raise ValueError(f"Provided constants with shape {constants.shape}, expecting "
-                                     f"{[numspots, self.numconst]}")
+                    c = np.ascontiguousarray(np.broadcast_to(c, (n, nc)))
+                except ValueError:
+                    raise ValueError(f"constants of shape {c.shape} do not fit {(n, nc)}") from None
         if roipos is None:
-            roipos = np.zeros((numspots, self.indexdims), dtype=np.int32)
+            rp = np.zeros((n, self.indexdims), dtype=np.int32)
         else:
-            roipos = np.ascontiguousarray(roipos, dtype=np.int32)
-            if not np.array_equal(roipos.shape, [numspots, self.indexdims]):
-                raise ValueError(f"Provided roi positions have incorrect shape: {roipos.shape} should be "
-                                 f"{[numspots, self.indexdims]}")
-        if params.shape[1] != self.numparams:
-            raise ValueError(f"{self.fmt} expected, {params.shape[1]} parameters given")
-        return params, constants, roipos
+            rp = np.ascontiguousarray(roipos, dtype=np.int32)
+            if rp.shape != (n, self.indexdims):
+                raise ValueError(f"ROI positions of shape {rp.shape}, expected {(n, self.indexdims)}")
+        if p.ndim != 2 or p.shape[1] != self.numparams:
+            raise ValueError(f"expected {self.numparams} parameters per spot ({self.fmt}), got shape {p.shape}")
+        return p, c, rp
 
     # ------------------------------------------------------------------ reference API
     def ExpectedValue(self, params, roipos=None, constants=None):
@@ -142,17 +147,15 @@ class Estimator:
         return np.random.poisson(ev)
 
     def FisherMatrix(self, params, roipos=None, constants=None):
+        """Fisher information of the Poisson likelihood at each spot's parameters, float32
+        [n, K, K]: FI_ij = sum over pixels of dmu/dtheta_i dmu/dtheta_j / mu, computed on the GPU by
+        the fit kernels' Fisher pass (FP32 sums, mu clamped at 1e-8 as the C++ CRLB path does;
+        photonpy's numpy version clamps at 1e-9, photonpy/cpp/estimator.py:205-220)."""
         params, constants, roipos = self._checkparams(params, constants, roipos)
         fi = np.zeros((len(params), self.numparams, self.numparams), dtype=np.float32)
         if len(params) > 0:
-            deriv, ev = self.Derivatives(params, roipos, constants)
-            K = self.numparams
-            ev = np.reshape(ev, (len(params), self.samplecount))
-            deriv = np.reshape(deriv, (len(params), K, self.samplecount))
-            ev[ev < 1e-9] = 1e-9
-            for i in range(K):
-                for j in range(K):
-                    fi[:, i, j] = np.sum(1 / ev * (deriv[:, i] * deriv[:, j]), axis=1)
+            self._lib.PB200_FisherMatrix(self.inst, len(params), params, constants, fi)
+            check_error("FisherMatrix")
         return fi
 
     def CRLBAndChiSquare(self, params, samples=None, roipos=None, constants=None):
@@ -175,9 +178,11 @@ class Estimator:
         return self.CRLBAndChiSquare(params, samples, roipos, constants)[1]
 
     def CRLB(self, params, roipos=None, constants=None):
-        fisher = self.FisherMatrix(params, roipos, constants)
-        var = np.linalg.pinv(fisher)
-        return np.sqrt(np.abs(var[:, np.arange(self.numparams), np.arange(self.numparams)]))
+        """Cramer-Rao lower bound sqrt(diag(FI^-1)) at each spot's parameters, float32 [n, K]: the
+        Fisher matrix from the GPU's Fisher pass, inverted in FP64 on the GPU (LUP with partial
+        pivoting; +Inf where it is singular, where photonpy's numpy version takes a
+        pseudo-inverse, photonpy/cpp/estimator.py:249-253)."""
+        return self.CRLBAndChiSquare(params, None, roipos, constants)
 
     def Derivatives(self, params, roipos=None, constants=None):
         """(deriv, ev) with deriv shaped [numspots, numparams, *roishape]."""
@@ -189,35 +194,35 @@ class Estimator:
         return deriv, ev
 
     def NumDeriv(self, params, roipos=None, constants=None, eps=1e-6):
-        """Central-difference derivative of ExpectedValue."""
+        """Central differences of ExpectedValue: deriv[:, k] = (mu(theta + eps e_k) -
+        mu(theta - eps e_k)) / (2 eps) in float32, with the 2K shifted parameter sets of all spots
+        evaluated in one GPU call. Returns (deriv [n, K, *sampleshape], mu(theta))."""
         params, constants, roipos = self._checkparams(params, constants, roipos)
+        n, K = params.shape
         ev = self.ExpectedValue(params, roipos, constants)
-        deriv = np.zeros((len(params), self.numparams, *self.sampleshape), dtype=np.float32)
-        for k in range(self.numparams):
-            params_min = params * 1
-            params_min[:, k] -= eps
-            params_max = params * 1
-            params_max[:, k] += eps
-            ev_min = self.ExpectedValue(params_min, roipos, constants)
-            ev_max = self.ExpectedValue(params_max, roipos, constants)
-            deriv[:, k] = (ev_max - ev_min) / (2 * eps)
+        shifted = np.empty((n, 2 * K, K), dtype=np.float32)
+        shifted[...] = params[:, None, :]
+        for k in range(K):  # theta_k +- eps rounded to float32, as a float32 parameter array holds it
+            shifted[:, k, k] = params[:, k] + np.float32(eps)
+            shifted[:, K + k, k] = params[:, k] - np.float32(eps)
+        ev_s = self.ExpectedValue(shifted.reshape(n * 2 * K, K), np.repeat(roipos, 2 * K, axis=0),
+                                  np.repeat(constants, 2 * K, axis=0))
+        ev_s = ev_s.reshape(n, 2 * K, *self.sampleshape)
+        deriv = ((ev_s[:, :K] - ev_s[:, K:]) / np.float32(2 * eps)).astype(np.float32)
         return deriv, ev
 
     def NumCRLB(self, params, roipos=None, constants=None, eps=1e-4, useNumDeriv=True):
-        if useNumDeriv:
-            deriv, ev = self.NumDeriv(params, roipos, constants, eps)
-        else:
-            deriv, ev = self.Derivatives(params, roipos, constants)
-        K = self.numparams
-        deriv = np.reshape(deriv, (len(params), K, self.samplecount))
-        ev = np.reshape(ev, (len(params), self.samplecount))
-        ev[ev < 1e-9] = 1e-9
-        fi = np.zeros((len(params), K, K))
-        for i in range(K):
-            for j in range(K):
-                fi[:, i, j] = np.sum(1 / ev * (deriv[:, i] * deriv[:, j]), axis=1)
+        """CRLB from the definition, in float64 on the host: FI = J diag(1/mu) J^T over the
+        pixels, with J the numerical (NumDeriv, step eps) or analytic (Derivatives) Jacobian and
+        mu clamped at 1e-9; CRLB = sqrt(|diag(FI^-1)|)."""
+        deriv, ev = (self.NumDeriv(params, roipos, constants, eps) if useNumDeriv
+                     else self.Derivatives(params, roipos, constants))
+        n, K = deriv.shape[:2]
+        J = deriv.reshape(n, K, -1).astype(np.float64)
+        w = 1.0 / np.maximum(ev.reshape(n, -1).astype(np.float64), 1e-9)
+        fi = np.einsum("nkp,np,nlp->nkl", J, w, J)
         var = np.linalg.inv(fi)
-        return np.sqrt(np.abs(var[:, np.arange(self.numparams), np.arange(self.numparams)]))
+        return np.sqrt(np.abs(np.diagonal(var, axis1=1, axis2=2)))
 
     def GetLevMarParams(self):
         lmp = LevMarParams()
