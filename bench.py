@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--lanes", type=int, default=0, help="lanes per ROI (0 = library default)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library default)")
     ap.add_argument("--variant", type=int, default=None, help="Gaussian kernel family (0 column-blocked, 1 generic)")
+    ap.add_argument("--xy-step", type=float, default=1.0, dest="xy_step",
+                    help="spline workload: xy step of the 26x26x41 calibration in ROI pixels (1: photonpy's one "
+                         "voxel per pixel; 0.5: the oversampled extension, whose CPU baseline is the oracle port)")
     ap.add_argument("--B", type=float, default=0.0, dest="astig_B",
                     help="astig workload: quartic term B of sigma(z) (0: photonpy's 4-coefficient form; the "
                          "reference cannot express B != 0, so its CPU baseline is then the oracle port)")
@@ -85,7 +88,7 @@ WORKLOADS = {
 BASE_SEED = {"sigmaxy": 2, "xyibg": 1, "astig": 3, "spline": 4}
 
 
-def make_data(workload, n, seed, device=None, astig_B=0.0):
+def make_data(workload, n, seed, device=None, astig_B=0.0, xy_step=1.0):
     from photonpy_b200 import synth
     synth.use_torch(device, seed)
     if workload == "sigmaxy":
@@ -95,9 +98,9 @@ def make_data(workload, n, seed, device=None, astig_B=0.0):
     if workload == "astig":
         return synth.astig(n, seed=seed, B=astig_B)
     if workload == "spline":
-        d = synth.spline(n, seed=seed)
-        zstack, zr = synth.astig_zstack(shape_xy=26, nz=41, zrange_um=(-0.4, 0.4))
-        d["zstack"], d["spline_zrange"] = zstack, zr
+        d = synth.spline(n, seed=seed, B=astig_B)
+        zstack, zr = synth.astig_zstack(shape_xy=26, nz=41, zrange_um=(-0.4, 0.4), B=astig_B, step_px=xy_step)
+        d["zstack"], d["spline_zrange"], d["xy_step"] = zstack, zr, xy_step
         return d
     raise ValueError(workload)
 
@@ -105,6 +108,10 @@ def make_data(workload, n, seed, device=None, astig_B=0.0):
 def workload_desc(args, w):
     if args.workload == "astig" and args.astig_B:
         return w["desc"].replace("(reference 4-term form)", f"(quartic term B = {args.astig_B:g}, FP64-oracle extension)")
+    if args.workload == "spline":
+        step = "1 px (photonpy's form)" if args.xy_step == 1.0 else f"{args.xy_step:g} px (oversampled extension)"
+        return w["desc"] + f", 26x26x41 calibration, xy step {step}, z step 20 nm" + (
+            f", astig model with B = {args.astig_B:g}" if args.astig_B else "")
     return w["desc"]
 
 
@@ -124,7 +131,7 @@ def make_estimator(pb, ctx, d):
         sm = pb.CSplineMethods(ctx)
         coefs = sm.ComputeSplineCoeff(d["zstack"], border=1)
         calib = pb.CSplineCalibration(d["spline_zrange"][0], d["spline_zrange"][1], coefs)
-        e = sm.CreatePSF_XYZIBg(d["R"], calib, sm.FlatBg, True)
+        e = sm.CreatePSF_XYZIBg(d["R"], calib, sm.FlatBg, True, xyStep=d.get("xy_step", 1.0))
         e._calib = calib
         return e
     raise ValueError(k)
@@ -156,7 +163,7 @@ def oracle_model(d):
         return O.Model(O.XYZIBG, d["R"], astig_x=cx, astig_y=cy, zrange=d["zrange"])
     if k == "CSpline":
         return O.Model(O.CSPLINE, d["R"], coefs=O.spline_compute(d["zstack"], border=1),
-                       spline_zrange=d["spline_zrange"])
+                       spline_zrange=d["spline_zrange"], spline_xy_step=d.get("xy_step", 1.0))
     raise ValueError(k)
 
 
@@ -167,7 +174,7 @@ def cpu_localize(d, samples, keep=False):
     from oracle import ref_lib
     out = ([], [], [])
     t0 = time.perf_counter()
-    if ref_lib.available() and not has_quartic_term(d):
+    if ref_lib.available() and not beyond_reference_model(d):
         est = ref_estimator(d)
         for s in range(0, len(samples), 20000):
             chunk = samples[s:s + 20000]
@@ -194,8 +201,11 @@ def cpu_localize(d, samples, keep=False):
     return dt, kind
 
 
-def has_quartic_term(d):
-    """The astig workload with B != 0, which photonpy's model cannot express."""
+def beyond_reference_model(d):
+    """Workloads photonpy's models cannot express: the astig workload with B != 0, the spline
+    workload with a calibration sampled finer than one ROI pixel."""
+    if d["kind"] == "CSpline":
+        return d.get("xy_step", 1.0) != 1.0
     return d["kind"] == "XYZIBg" and (d["astig"][0][4] != 0 or d["astig"][1][4] != 0)
 
 
@@ -358,7 +368,8 @@ def run_reference(args):
         device = "cuda" if torch.cuda.is_available() else None
     except ImportError:
         device = None
-    d = make_data(args.workload, args.n or w["n"], seed=BASE_SEED[args.workload], device=device, astig_B=args.astig_B)
+    d = make_data(args.workload, args.n or w["n"], seed=BASE_SEED[args.workload], device=device, astig_B=args.astig_B,
+                  xy_step=args.xy_step)
     from oracle import ref_lib
     n_cal = 2000
     t, kind = cpu_localize(d, d["samples"][:n_cal])
@@ -643,7 +654,7 @@ def reference_gpu_plain(d, m=50_000):
     through its host API, Estimate + ChiSquareAndCRLB, on the first m ROIs of the batch; host
     copies included, as photonpy always has them."""
     from oracle import ref_lib
-    if not ref_lib.available() or d["kind"] not in ("XYIBg", "XYIBgSigmaXY", "XYZIBg") or has_quartic_term(d):
+    if not ref_lib.available() or d["kind"] not in ("XYIBg", "XYIBgSigmaXY", "XYZIBg") or beyond_reference_model(d):
         return None
     sub = d["samples"][:m]
     est = ref_gpu_estimator(d)
@@ -698,7 +709,7 @@ def main():
     w = WORKLOADS[args.workload]
     n = args.n or w["n"]
     d = make_data(args.workload, n, seed=BASE_SEED[args.workload] + 1000 * rank, device=f"cuda:{local}",
-                  astig_B=args.astig_B)
+                  astig_B=args.astig_B, xy_step=args.xy_step)
     smp = d["samples"]
     K = roofline.K_OF[d["kind"]]
 

@@ -112,6 +112,14 @@ Estimator* CSpline_CreatePSF(int roisize, const CSpline_Calibration* calib, cons
                              Context* ctx);
 /* Estimators/CSpline/CubicSplinePSF.cu:135-146: z-stack file (header v1) -> coefficients (border 0). */
 Estimator* CSpline_CreatePSF_FromFile(int roisize, const char* filename, int mode, bool cuda, Context* ctx);
+/* Extension (no reference counterpart; photonpy's spline has one voxel per ROI pixel,
+ * CubicSplinePSFModels.h:79-96,120-141): a spline calibration sampled every xyStep ROI pixels in
+ * x and y (0 < xyStep <= 1, e.g. 0.5 for a 2x oversampled PSF). Pixel (x, y) of a spot at
+ * (theta_x, theta_y) reads the spline at grid coordinate (x - theta_x)/xyStep + N/2; the x/y
+ * derivatives scale by 1/xyStep. Modes 0 (flat) and 1 (tilted background). xyStep = 1 gives
+ * results identical to CSpline_CreatePSF. */
+Estimator* CSpline_CreatePSF_Oversampled(int roisize, const CSpline_Calibration* calib, const float* coefs, int mode,
+                                         float xyStep, bool cuda, Context* ctx);
 /* Estimators/CSpline/CubicSplinePSF.cu:151-204: spline coefficients of a z-stack, computed on the
  * GPU with the reference's double-precision LUP solve (bit-identical output).
  * coefs[shape-3+2*border][64]. */
@@ -373,6 +381,14 @@ void PB200_FisherMatrixDevice(Estimator* e, int numspots, const float* d_params,
 int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, const float* d_params,
                             const float* d_constants, const float* calib, const float* d_coefs, const float* d_gradOut,
                             float* d_nll, float* d_dparams, float* d_dcalib, void* stream);
+/* Spline calibration step (no reference counterpart): for a flat-background spline estimator and
+ * spots with known parameters d_params[n][5], in one pass over the ROIs: d_nll[n] (nullable), the
+ * gradient of the summed NLL with respect to every coefficient ACCUMULATED into d_grad (nullable,
+ * the coefficient array's shape), and the diagonal of the Fisher information with respect to the
+ * coefficients, sum_n sum_p I_n^2 f_m^2 / mu_p, ACCUMULATED into d_fisherDiag (nullable).
+ * d_coefs (device, nullable) replaces the estimator's coefficients. Returns 0 or -1. */
+int PB200_SplineCoefGradient(Estimator* e, int numspots, const float* d_sample, const float* d_params,
+                             const float* d_coefs, float* d_nll, float* d_grad, float* d_fisherDiag, void* stream);
 /* Mixed batches (no reference counterpart; photonpy runs one estimator, i.e. one model and
  * ROI size, per call). A plan binds nbuckets (estimator, count, device buffers) groups; one
  * run fits all of them with two persistent launches (the LM pass over every bucket, then the

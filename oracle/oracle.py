@@ -43,6 +43,7 @@ class PsoModel(ct.Structure):
         ("spline_zmin", ct.c_float),
         ("spline_zmax", ct.c_float),
         ("coefs", ct.c_void_p),
+        ("spline_q", ct.c_float),
     ]
 
 
@@ -107,7 +108,7 @@ class Model:
     """Description of one PSF model instance, mirroring the reference's creation calls."""
 
     def __init__(self, model: int, roisize: int, sigma=(1.0, 1.0), astig_x=None, astig_y=None, zrange=(0, 0),
-                 coefs=None, spline_zrange=(0, 0)):
+                 coefs=None, spline_zrange=(0, 0), spline_xy_step=1.0):
         self.model = model
         self.roisize = int(roisize)
         self.K = NUM_PARAMS[model]
@@ -133,6 +134,7 @@ class Model:
             s.spline_shape[0], s.spline_shape[1], s.spline_shape[2] = nz, ny, nx
             s.spline_zmin, s.spline_zmax = spline_zrange
             s.coefs = self._coefs.ctypes.data
+        s.spline_q = 1.0 / float(spline_xy_step)
         self.s = s
 
     # -- oracle entry points -------------------------------------------------------------

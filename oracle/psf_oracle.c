@@ -47,6 +47,8 @@ typedef struct {
     int spline_shape[3];    /* coefficient grid (z, y, x)                                      */
     float spline_zmin, spline_zmax;
     const float* coefs;     /* [Nz][Ny][Nx][64]                                                */
+    float spline_q;         /* spline voxels per ROI pixel in x and y (0 or 1: photonpy's      */
+                            /* one voxel per pixel; 2: a calibration sampled at 0.5 px)        */
 } pso_model_t;
 
 int pso_num_params(int model)

@@ -25,6 +25,8 @@
 
 /* clamp(f,a,b) = fmax(a, fmin(f, b)) exactly as CudaMath.h:1152-1155 */
 static inline REAL FN(o_clamp)(REAL f, REAL a, REAL b) { return FMAX(a, FMIN(f, b)); }
+/* largest integer <= f, in the REAL type */
+static inline REAL FN(o_floor)(REAL f) { REAL t = (REAL)(long long)f; return t > f ? t - 1 : t; }
 
 /* Per-pixel model values: mu[p] and jac[k*npix + p], row-major pixels. */
 static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float* consts,
@@ -233,6 +235,9 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
         const float du_f = (m->spline_zmax - m->spline_zmin) / (float)Nz;
         const REAL du = (REAL)du_f;
         REAL tx = theta[0], ty = theta[1], tz = theta[2], tI = theta[3], tbg = theta[4];
+        /* voxels per ROI pixel: 1 reproduces the reference; the oversampled extension scales the
+         * grid coordinate of pixel x to q x - tx and the x/y derivatives by q */
+        const REAL q = m->spline_q > 0 ? (REAL)m->spline_q : (REAL)1;
         if (m->model == PSO_CSPLINE_BGIMAGE) {
             const float wf = (float)W;
             tx = tx - (REAL)(wf / 2.0f) + (REAL)((wf - (float)Nx + 1) / 2.0f);
@@ -240,14 +245,14 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
             tx += (REAL)0.5f;
             ty += (REAL)0.5f;
         } else {
-            tx -= (REAL)(Nx * 0.5f);
-            ty -= (REAL)(Ny * 0.5f);
+            tx = tx * q - (REAL)(Nx * 0.5f);
+            ty = ty * q - (REAL)(Ny * 0.5f);
         }
         const REAL halfw = (REAL)((float)W * 0.5f);
         REAL df[64], dxf[64], dyf[64], dzf[64];
         for (int i = 0; i < 64; i++) df[i] = dxf[i] = dyf[i] = dzf[i] = 0;
-        REAL spx = -tx; spx -= (REAL)(int)spx;
-        REAL spy = -ty; spy -= (REAL)(int)spy;
+        REAL spx = -tx; spx -= q == 1 ? (REAL)(int)spx : FN(o_floor)(spx);
+        REAL spy = -ty; spy -= q == 1 ? (REAL)(int)spy : FN(o_floor)(spy);
         REAL spz = (tz - (REAL)m->spline_zmin) / du;
         int k = (int)spz; if (k < 0) k = 0; if (k > Nz - 1) k = Nz - 1;
         spz = FN(o_clamp)(spz - (REAL)k, 0, 1);
@@ -269,10 +274,10 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
             zzz *= spz;
         }
         for (int y = 0; y < H; y++) {
-            REAL yy = (REAL)y - ty;
+            REAL yy = (REAL)y * q - ty;
             int j = (int)yy; if (j < 0) j = 0; if (j > Ny - 1) j = Ny - 1;
             for (int x = 0; x < W; x++) {
-                REAL xx = (REAL)x - tx;
+                REAL xx = (REAL)x * q - tx;
                 int i = (int)xx; if (i < 0) i = 0; if (i > Nx - 1) i = Nx - 1;
                 REAL psf = 0, dx = 0, dy = 0, dz = 0;
                 const float* c = m->coefs + 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i);
@@ -283,8 +288,8 @@ static void FN(model_eval)(const pso_model_t* m, const REAL* theta, const float*
                     dy += dyf[idx] * coef;
                     dz += dzf[idx] * coef;
                 }
-                dx *= -tI;
-                dy *= -tI;
+                dx *= -(tI * q);
+                dy *= -(tI * q);
                 dz *= tI / du;
                 if (psf < 0) psf = 0;
                 int p = y * W + x;

@@ -64,6 +64,11 @@ class CSplineMethods:
         self._CSpline_CreatePSF_FromFile.argtypes = [ctypes.c_int32, ctypes.c_char_p, ctypes.c_int32, ctypes.c_bool,
                                                      ctypes.c_void_p]
         self._CSpline_CreatePSF_FromFile.restype = ctypes.c_void_p
+        self._CSpline_CreatePSF_Oversampled = smlmlib.CSpline_CreatePSF_Oversampled
+        self._CSpline_CreatePSF_Oversampled.argtypes = [ctypes.c_int32, ctypes.POINTER(CSplineCalibration),
+                                                        NullableFloatArrayType, ctypes.c_int32, ctypes.c_float,
+                                                        ctypes.c_bool, ctypes.c_void_p]
+        self._CSpline_CreatePSF_Oversampled.restype = ctypes.c_void_p
         self._CSpline_Compute = smlmlib.CSpline_Compute
         self._CSpline_Compute.argtypes = [ctl.ndpointer(np.int32, flags="aligned, c_contiguous"),
                                           ctl.ndpointer(np.float32, flags="aligned, c_contiguous"),
@@ -74,8 +79,15 @@ class CSplineMethods:
                                            ctl.ndpointer(np.float32, flags="aligned, c_contiguous"), ctypes.c_int32,
                                            ctl.ndpointer(np.float32, flags="aligned, c_contiguous")]
 
-    def CreatePSF_XYZIBg(self, roisize, calib: CSplineCalibration, fitMode=FlatBg, cuda=True) -> CSplinePSF:
-        inst = self._CSpline_CreatePSF(roisize, calib, None, fitMode, cuda, self.ctx.inst)
+    def CreatePSF_XYZIBg(self, roisize, calib: CSplineCalibration, fitMode=FlatBg, cuda=True,
+                         xyStep=1.0) -> CSplinePSF:
+        """Spline PSF estimator (x, y, z, I, bg[, bgx, bgy]). Extension: xyStep < 1 for a calibration
+        sampled every xyStep ROI pixels in x and y (e.g. 0.5 for a 2x oversampled z-stack)."""
+        if xyStep == 1.0:
+            inst = self._CSpline_CreatePSF(roisize, calib, None, fitMode, cuda, self.ctx.inst)
+        else:
+            inst = self._CSpline_CreatePSF_Oversampled(roisize, calib, None, fitMode, float(xyStep), cuda,
+                                                       self.ctx.inst)
         return CSplinePSF(self.ctx, inst, calib)
 
     def ComputeSplineCoeff(self, data, border=0):

@@ -13,7 +13,9 @@
 //                sigma = s0 sqrt(1 + t^2/d^2 + A t^3/d^2 + B t^4/d^4), t = z - gamma
 //   CSpline      d/dcoef[k][j][i][m] = sum g_n r_p I delta_f[m] over the pixels that read voxel
 //                (k, j, i) (zero where the PSF value is clamped at 0), scattered with 16-byte
-//                vector atomics
+//                vector atomics; optionally also the diagonal of the Fisher information with
+//                respect to the coefficients, sum g_n I^2 delta_f[m]^2 / mu_p (the Gauss-Newton
+//                curvature a calibration step divides by)
 // Nothing per pixel is stored: mu and its derivatives are recomputed from the model table.
 #pragma once
 #include "fit_common.cuh"
@@ -29,6 +31,8 @@ struct AdjointArgs {
     float* nll;            // [n] or null
     float* dparams;        // [n][K] or null
     float* dcalib;         // XYIBg [2], XYZIBg [10], CSpline [Nz*Ny*Nx*64], or null; accumulated into
+    float* curv;           // CSpline only: [Nz*Ny*Nx*64] Fisher diagonal of the coefficients, or null;
+                           // accumulated into
     int n;
     int smemStride;        // floats per group (model table + extra sigma-derivative table)
 };
@@ -108,14 +112,26 @@ __global__ void __launch_bounds__(256) adjoint_kernel(const ModelDesc d, const A
                 cal[0] += r * Y.y * X.w;  // (tI DeltaY) G21x = dmu/dsigma_x
                 cal[1] += r * X.y * Y.w;  // (tI DeltaX) G21y = dmu/dsigma_y
             } else if constexpr (kSpline) {
-                if (a.dcalib && J[3] > 0.0f) {  // J[3] is the PSF value, clamped at 0 by the model
-                    const float w = g * r * th[3];
-                    float4* dst = reinterpret_cast<float4*>(a.dcalib + m.coef_offset(x, y));
+                if ((a.dcalib || a.curv) && J[3] > 0.0f) {  // J[3] is the PSF value, clamped at 0 by the model
+                    const size_t off = m.coef_offset(x, y);
                     const float4* df = reinterpret_cast<const float4*>(tab);
+                    if (a.dcalib) {
+                        const float w = g * r * th[3];
+                        float4* dst = reinterpret_cast<float4*>(a.dcalib + off);
 #pragma unroll 4
-                    for (int q = 0; q < 16; q++) {
-                        const float4 f = df[q];
-                        atomicAdd(dst + q, make_float4(w * f.x, w * f.y, w * f.z, w * f.w));
+                        for (int q = 0; q < 16; q++) {
+                            const float4 f = df[q];
+                            atomicAdd(dst + q, make_float4(w * f.x, w * f.y, w * f.z, w * f.w));
+                        }
+                    }
+                    if (a.curv) {
+                        const float w2 = g * th[3] * th[3] / muc;
+                        float4* dst = reinterpret_cast<float4*>(a.curv + off);
+#pragma unroll 4
+                        for (int q = 0; q < 16; q++) {
+                            const float4 f = df[q];
+                            atomicAdd(dst + q, make_float4(w2 * f.x * f.x, w2 * f.y * f.y, w2 * f.z * f.z, w2 * f.w * f.w));
+                        }
                     }
                 }
             }

@@ -699,9 +699,11 @@ void build_coefs_qmajor(Estimator* e) {
 }
 
 Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const float* h_coefs, int mode, Context* ctx,
-                       const float* d_coefs_src) {
+                       const float* d_coefs_src, float xyStep = 1.0f) {
     // modes CSPLINE_FLATBG 0, CSPLINE_TILTEDBG 1, CSPLINE_BGIMAGE 2 (CubicSplinePSF.cu:76-101)
     if (mode < 0 || mode > 2) throw Error("Invalid model background mode");
+    if (!(xyStep > 0.0f) || !(xyStep <= 1.0f)) throw Error("CSpline_CreatePSF_Oversampled: xyStep must be in (0, 1]");
+    if (xyStep != 1.0f && mode == 2) throw Error("CSpline_CreatePSF_Oversampled: the background-image mode takes 1 px voxels");
     if (roisize < 3 || roisize > 64) throw Error("roisize must be in [3, 64]");
     if (!calib) throw Error("CSpline_CreatePSF: calibration is null");
     const int nz = calib->shape[0], ny = calib->shape[1], nx = calib->shape[2];
@@ -715,6 +717,7 @@ Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const floa
         e->desc.spline_shape[2] = nx;
         e->desc.spline_zmin = calib->z_min;
         e->desc.spline_zmax = calib->z_max;
+        e->desc.spline_q = 1.0f / xyStep;
         const size_t ncoef = (size_t)nz * ny * nx * 64;
         e->coefs.ensure(sizeof(float) * ncoef);
         if (d_coefs_src)
@@ -872,6 +875,12 @@ Estimator* Gauss2D_CreatePSF_XYZIBgB(int roisize, const Gauss3D_CalibrationB* ca
 Estimator* CSpline_CreatePSF(int roisize, const CSpline_Calibration* calib, const float* coefs, int mode, bool,
                              Context* ctx) {
     return guarded([&]() -> Estimator* {return make_spline(roisize, calib, coefs, mode, ctx, nullptr);}, (Estimator*)nullptr);
+}
+
+Estimator* CSpline_CreatePSF_Oversampled(int roisize, const CSpline_Calibration* calib, const float* coefs, int mode,
+                                         float xyStep, bool, Context* ctx) {
+    return guarded([&]() -> Estimator* { return make_spline(roisize, calib, coefs, mode, ctx, nullptr, xyStep); },
+                   (Estimator*)nullptr);
 }
 
 Estimator* CSpline_CreatePSF_FromFile(int roisize, const char* filename, int mode, bool, Context* ctx) {
@@ -1256,6 +1265,32 @@ int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, c
             a.nll = d_nll;
             a.dparams = d_dparams;
             a.dcalib = d_dcalib;
+            a.n = numspots;
+            adjoint_launcher_for(d.model)(d, a, (cudaStream_t)stream);
+            return 0;
+        },
+        -1);
+}
+
+int PB200_SplineCoefGradient(Estimator* e, int numspots, const float* d_sample, const float* d_params,
+                             const float* d_coefs, float* d_nll, float* d_grad, float* d_fisherDiag, void* stream) {
+    if (numspots == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            check_estimator(e);
+            if (e->desc.model != MODEL_CSPLINE) throw Error("SplineCoefGradient: a flat-background spline estimator is needed");
+            if (numspots < 0 || !d_sample || !d_params) throw Error("SplineCoefGradient: bad arguments");
+            ModelDesc d = e->desc;
+            if (d_coefs) {
+                d.coefs = d_coefs;
+                d.coefsQ = nullptr;  // the caller's coefficients in the reference layout
+            }
+            AdjointArgs a{};
+            a.smp = d_sample;
+            a.params = d_params;
+            a.nll = d_nll;
+            a.dcalib = d_grad;
+            a.curv = d_fisherDiag;
             a.n = numspots;
             adjoint_launcher_for(d.model)(d, a, (cudaStream_t)stream);
             return 0;

@@ -57,6 +57,9 @@ struct ModelDesc {
     int spline_shape[3];  // Nz, Ny, Nx of the coefficient grid
     float spline_zmin, spline_zmax;
     const float* coefs;   // device, [Nz][Ny][Nx][64]
+    // spline voxels per ROI pixel along x and y: 1 for photonpy's spline (one voxel per pixel); 2
+    // for a calibration sampled at 0.5 px (extension; the reference has no xy scale)
+    float spline_q;
     // device, the same coefficients q-major: float4 q (coefficients 4q..4q+3) of voxel v at
     // coefsQ[q * Nz*Ny*Nx + v], so that lanes reading neighbouring voxels read neighbouring
     // addresses (the fit kernels' copy; null when the caller supplies coefs directly)
@@ -557,6 +560,7 @@ struct SplineModelT {
     static __host__ __device__ constexpr int table_floats(int) { return 256; }
 
     float tx, ty, tI, tbg, du;
+    float q;  // voxels per ROI pixel (1: the reference's model)
     float spx, spy, spz;
     float bgx, bgy, halfw;
     const float* img;  // MODE 2: this spot's background image [R][R]
@@ -568,13 +572,15 @@ struct SplineModelT {
         Ny = d.spline_shape[1];
         Nx = d.spline_shape[2];
         du = DIV(SUB(d.spline_zmax, d.spline_zmin), (float)Nz);
+        q = d.spline_q;
         if (MODE == 2) {
             const float w = (float)d.roisize;
             tx = ADD(ADD(SUB(th[0], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Nx), 1.0f), 2.0f)), 0.5f);
             ty = ADD(ADD(SUB(th[1], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Ny), 1.0f), 2.0f)), 0.5f);
         } else {
-            tx = SUB(th[0], MUL((float)Nx, 0.5f));
-            ty = SUB(th[1], MUL((float)Ny, 0.5f));
+            // grid coordinate of pixel x: q x - tx (q = 1: x - (theta_x - Nx/2), the reference)
+            tx = SUB(MUL(th[0], q), MUL((float)Nx, 0.5f));
+            ty = SUB(MUL(th[1], q), MUL((float)Ny, 0.5f));
         }
         tI = th[3];
         tbg = th[4];
@@ -582,10 +588,13 @@ struct SplineModelT {
         bgy = (MODE == 1) ? th[6 % K] : 0.0f;
         halfw = MUL((float)d.roisize, 0.5f);
         img = nullptr;
+        // sub-voxel offset: the reference truncates toward zero (CubicSplinePSFModels.h:89-91),
+        // which is its fractional part wherever the model is valid (Nx/2 >= max x); the
+        // oversampled extension takes the fractional part (floor) everywhere
         float sx = -tx;
-        spx = SUB(sx, (float)(int)sx);
+        spx = SUB(sx, q == 1.0f ? (float)(int)sx : floorf(sx));
         float sy = -ty;
-        spy = SUB(sy, (float)(int)sy);
+        spy = SUB(sy, q == 1.0f ? (float)(int)sy : floorf(sy));
         float sz = DIV(SUB(th[2], d.spline_zmin), du);
         int kk = (int)sz;
         kk = max(0, min(kk, Nz - 1));
@@ -619,9 +628,9 @@ struct SplineModelT {
 
     __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
                                           float (&J)[K]) const {
-        const float yy = SUB((float)y, ty);
+        const float yy = SUB(MUL((float)y, q), ty);
         const int j = max(0, min((int)yy, Ny - 1));
-        const float xx = SUB((float)x, tx);
+        const float xx = SUB(MUL((float)x, q), tx);
         const int i = max(0, min((int)xx, Nx - 1));
         const float4* c4 = reinterpret_cast<const float4*>(d.coefs + 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i));
         const float4* f4 = reinterpret_cast<const float4*>(tab);
@@ -635,8 +644,8 @@ struct SplineModelT {
             dy = ADD(ADD(ADD(ADD(dy, MUL(e.x, c.x)), MUL(e.y, c.y)), MUL(e.z, c.z)), MUL(e.w, c.w));
             dz = ADD(ADD(ADD(ADD(dz, MUL(g.x, c.x)), MUL(g.y, c.y)), MUL(g.z, c.z)), MUL(g.w, c.w));
         }
-        dx = MUL(dx, -tI);
-        dy = MUL(dy, -tI);
+        dx = MUL(dx, -MUL(tI, q));
+        dy = MUL(dy, -MUL(tI, q));
         dz = MUL(dz, DIV(tI, du));
         if (psf < 0.0f) psf = 0.0f;
         J[0] = dx;
@@ -673,8 +682,8 @@ struct SplineModelT {
         const size_t qstride = qmajor ? nvox : 1;
 #pragma unroll
         for (int t = 0; t < PB; t++) {
-            const int j = max(0, min((int)SUB((float)y[t], ty), Ny - 1));
-            const int i = max(0, min((int)SUB((float)x[t], tx), Nx - 1));
+            const int j = max(0, min((int)SUB(MUL((float)y[t], q), ty), Ny - 1));
+            const int i = max(0, min((int)SUB(MUL((float)x[t], q), tx), Nx - 1));
             const size_t v = (size_t)k * Nx * Ny + (size_t)j * Nx + i;
             cp[t] = qmajor ? d.coefsQ + v : reinterpret_cast<const float4*>(d.coefs) + 16 * v;
             psf[t] = ddx[t] = ddy[t] = ddz[t] = 0.0f;
@@ -693,12 +702,13 @@ struct SplineModelT {
             }
         }
         const float zs = DIV(tI, du);
+        const float xs = -MUL(tI, q);
 #pragma unroll
         for (int t = 0; t < PB; t++) {
             float p = psf[t];
             if (p < 0.0f) p = 0.0f;
-            J[t][0] = MUL(ddx[t], -tI);
-            J[t][1] = MUL(ddy[t], -tI);
+            J[t][0] = MUL(ddx[t], xs);
+            J[t][1] = MUL(ddy[t], xs);
             J[t][2] = MUL(ddz[t], zs);
             J[t][3] = p;
             if (MODE == 1) {
@@ -720,8 +730,8 @@ struct SplineModelT {
 
     // Offset of the 64 coefficients pixel (x, y) reads (same voxel choice as pixel()).
     __device__ __forceinline__ size_t coef_offset(int x, int y) const {
-        const int j = max(0, min((int)SUB((float)y, ty), Ny - 1));
-        const int i = max(0, min((int)SUB((float)x, tx), Nx - 1));
+        const int j = max(0, min((int)SUB(MUL((float)y, q), ty), Ny - 1));
+        const int i = max(0, min((int)SUB(MUL((float)x, q), tx), Nx - 1));
         return 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i);
     }
 
