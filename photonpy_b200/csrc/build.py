@@ -60,11 +60,22 @@ def build(force: bool = False, verbose: bool = False, defines=(), out: str | Non
     if verbose:
         common += ["-Xptxas", "-v"]
 
+    newest_header = max(os.path.getmtime(os.path.join(HERE, h)) for h in HEADERS)
+    newest_header = max(newest_header, os.path.getmtime(os.path.join(ROOT, "include", "photonpy_b200.h")))
+
     def compile_unit(u):
         src = os.path.join(HERE, u)
         obj = os.path.join(obj_dir, os.path.splitext(u)[0] + ".o")
         cmd = [nvcc(), *common, "-c", src, "-o", obj]
+        stamp = obj + ".cmd"
+        # an object is reused when it is newer than its sources and was built with the same command
+        if (not force and os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
+                and os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header)):
+            return obj, ""
         r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode == 0:
+            with open(stamp, "w") as f:
+                f.write(" ".join(cmd))
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {u}:\n{r.stdout}\n{r.stderr}")
         return obj, r.stderr

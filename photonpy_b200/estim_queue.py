@@ -23,59 +23,57 @@ from .lib import NullableFloatArrayType, NullableIntArrayType, check_error
 
 
 class EstimQueue_Results:
-    """Results of a queue (photonpy/cpp/estim_queue.py:14-74)."""
+    """The results a queue hands back (the attributes and methods of photonpy's
+    EstimQueue_Results, photonpy/cpp/estim_queue.py:14-74): per-spot arrays estim [n, K],
+    diagnostics [n, numDiag], crlb [n, K], roipos [n, dims], iterations [n], chisq [n], ids [n] and,
+    when the queue keeps them, samples [n, *sampleshape]; all selections act on every one of them."""
+
+    _PER_SPOT = ("estim", "diagnostics", "crlb", "roipos", "iterations", "chisq", "ids", "samples")
 
     def __init__(self, param_names, sampleshape, estim, diag, crlb, iterations, chisq, roipos, samples, ids):
-        self.estim = estim
-        self.sampleshape = sampleshape
-        self.diagnostics = diag
-        self.crlb = crlb
-        self.roipos = roipos
-        self.iterations = iterations
-        self.chisq = chisq
-        self.ids = ids
-        self.samples = samples
         self.param_names = param_names
+        self.sampleshape = sampleshape
+        self.estim, self.diagnostics, self.crlb = estim, diag, crlb
+        self.iterations, self.chisq, self.roipos = iterations, chisq, roipos
+        self.ids, self.samples = ids, samples
 
     def CRLB(self):
         return self.crlb
 
-    def SortByID(self, isUnique=False):
-        """Reorder by spot id; with isUnique the ids must be a permutation of 0..n-1."""
-        if isUnique:
-            order = np.arange(len(self.ids))
-            order[self.ids] = order * 1
-        else:
-            order = np.argsort(self.ids, kind="stable")
-        self.Filter(order)
-        return order
-
     def Filter(self, indices):
+        """Keep the spots selected by `indices` (a boolean mask or an index array, in the order
+        given) in every per-spot array; returns the index array."""
+        indices = np.asarray(indices)
         if indices.dtype == bool:
-            indices = np.nonzero(indices)[0]
-        if len(indices) != len(self.ids):
-            print(f"Removing {len(self.ids) - len(indices)}/{len(self.ids)}")
-        self.estim = self.estim[indices]
-        self.diagnostics = self.diagnostics[indices]
-        self.crlb = self.crlb[indices]
-        self.roipos = self.roipos[indices]
-        self.iterations = self.iterations[indices]
-        self.chisq = self.chisq[indices]
-        self.ids = self.ids[indices]
-        if self.samples is not None:
-            self.samples = self.samples[indices]
+            indices = np.flatnonzero(indices)
+        for name in self._PER_SPOT:
+            arr = getattr(self, name)
+            if arr is not None:
+                setattr(self, name, arr[indices])
         return indices
 
+    def SortByID(self, isUnique=False):
+        """Order the spots by ascending id and return the permutation applied (old index of each
+        new position). isUnique: the ids are exactly 0..n-1, so the permutation is their inverse."""
+        if isUnique:
+            perm = np.empty(len(self.ids), dtype=np.int64)
+            perm[np.asarray(self.ids)] = np.arange(len(self.ids))
+        else:
+            perm = np.argsort(self.ids, kind="stable")
+        return self.Filter(perm)
+
     def FilterXY(self, minX, minY, maxX, maxY):
-        return self.Filter(np.where(np.logical_and(np.logical_and(self.estim[:, 0] > minX, self.estim[:, 1] > minY),
-                                                   np.logical_and(self.estim[:, 0] < maxX,
-                                                                  self.estim[:, 1] < maxY)))[0])
+        """Keep the spots whose x and y lie strictly inside (minX, maxX) x (minY, maxY)."""
+        x, y = self.estim[:, 0], self.estim[:, 1]
+        return self.Filter((x > minX) & (x < maxX) & (y > minY) & (y < maxY))
 
     def Clone(self):
         return copy.deepcopy(self)
 
     def ColIdx(self, *names):
-        return np.squeeze(np.array([self.param_names.index(n) for n in names], dtype=np.int64))
+        """Column index of each named parameter (a scalar for one name)."""
+        idx = [self.param_names.index(n) for n in names]
+        return idx[0] if len(idx) == 1 else np.array(idx, dtype=np.int64)
 
 
 # EstimatorResult (Estimators/EstimationQueue.h:21-25)
