@@ -287,10 +287,10 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                 for (int k = 0; k < K; k++) a.trace[((size_t)roi * a.traceLen + it) * K + k] = th[k];
             }
             M m;
-            m.begin(d, th, cs);
+            m.template begin_group<G>(d, th, cs, lane, mask);
             float4 X[CPL], Yown[CPL];
-            m.template term_block<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, X);
-            m.template term_block<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, Yown);
+            m.template term_block<CPL>(c0, m.tx, m.cx1, m.cx2, m.sigx, m.gax, X);
+            m.template term_block<CPL>(c0, m.ty, m.cy1, m.cy2, m.sigy, m.gay, Yown);
             __syncwarp(mask);  // previous readers of ytab / scratch are done
 #pragma unroll
             for (int q = 0; q < CPL; q++)
