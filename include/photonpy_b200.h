@@ -444,6 +444,11 @@ uint64_t PB200_LaunchCount(void);
  * 8 independent FMA chains for iters x 16 steps on `stream`; returns the FLOPs issued (time the
  * launch with events) or -1 on a launch error. d_out: device buffer of `blocks` floats. */
 double PB200_Fp32ProbeLaunch(int blocks, int threads, int iters, float* d_out, void* stream);
+/* Self-check (diagnostic): the float constants sqrt(2 pi), sqrt(2), 1/sqrt(pi) the model set-ups
+ * use, and the host-computed fixed-sigma scales 1/(sqrt(2 pi) s), 1/(sqrt(2) s) of the n sigmas
+ * h_sigmas, against the device's IEEE square roots and divisions. *mismatches = number of values
+ * that differ (0 expected). Returns 0, or -1 on a CUDA error. */
+int PB200_CheckModelConstants(int n, const float* h_sigmas, int* mismatches);
 /* Model id (0 XYIBg, 1 XYIBgConstSigma, 2 XYIBgSigma, 3 XYIBgSigmaXY, 4 XYZIBg, 5 CSpline) and ROI size. */
 int PB200_ModelInfo(Estimator* e, int* roisize);
 

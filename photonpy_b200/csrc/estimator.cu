@@ -324,6 +324,7 @@ Estimator* make_gauss(int model, int roisize, float s0, float s1, const float* a
     }
     e->desc.minz = minz;
     e->desc.maxz = maxz;
+    if (model == MODEL_XYIBG) model_desc_fixed_sigma(e->desc);
     e->K = model_num_params(model);
     e->numconst = model_num_consts(model);
     // Exported limits (GaussianPSF.cu:42-48, 92-97, 115-120, 141-147, 168-175).
@@ -1246,6 +1247,7 @@ int PB200_PoissonNLLAdjoint(Estimator* e, int numspots, const float* d_sample, c
                 if (d.model == MODEL_XYIBG) {
                     d.sigma[0] = calib[0];
                     d.sigma[1] = calib[1];
+                    model_desc_fixed_sigma(d);
                 } else if (d.model == MODEL_XYZIBG) {
                     for (int i = 0; i < 5; i++) {
                         d.astig_x[i] = calib[i];

@@ -64,7 +64,13 @@ struct ModelDesc {
     // coefsQ[q * Nz*Ny*Nx + v], so that lanes reading neighbouring voxels read neighbouring
     // addresses (the fit kernels' copy; null when the caller supplies coefs directly)
     const float4* coefsQ;
+    // fixed-sigma XYIBg: 1/(sqrt(2 pi) sigma_x), 1/(sqrt(2) sigma_x), then the same for y, computed
+    // once per estimator with the reference's float operations (model_desc_fixed_sigma); the other
+    // models compute their scales per ROI and iteration
+    float fixed_c[4];
+    int fixed_c_set;
 };
+
 
 __host__ __device__ constexpr int model_num_params(int m) {
     return (m == MODEL_XYIBG || m == MODEL_XYIBG_CONSTSIGMA)            ? 4
@@ -80,6 +86,23 @@ __host__ __device__ constexpr int model_num_consts(int m) {
 
 // MATH_PI in the reference is the float literal 3.141592653589793f (MathUtils.h:95).
 #define PB_PI 3.141592653589793f
+// sqrt(2 pi), sqrt(2) and 1/sqrt(pi) as the reference's float arithmetic produces them (IEEE
+// square root and division of float operands, MATH_PI being the float literal above). Every set-up
+// starts from these instead of recomputing them per ROI and iteration; PB200_CheckModelConstants
+// compares them with the device's own __fsqrt_rn / __fdiv_rn results.
+constexpr float kSqrt2Pi = 0x1.40d932p+1f;
+constexpr float kSqrt2 = 0x1.6a09e6p+0f;
+constexpr float kInvSqrtPi = 0x1.20dd74p-1f;
+
+// Host side: the fixed-sigma scales of an XYIBg description from its sigma pair (IEEE float
+// multiply and divide, as MUL/DIV on the device). Call whenever sigma changes.
+inline void model_desc_fixed_sigma(ModelDesc& d) {
+    d.fixed_c[0] = 1.0f / (kSqrt2Pi * d.sigma[0]);
+    d.fixed_c[1] = 1.0f / (kSqrt2 * d.sigma[0]);
+    d.fixed_c[2] = 1.0f / (kSqrt2Pi * d.sigma[1]);
+    d.fixed_c[3] = 1.0f / (kSqrt2 * d.sigma[1]);
+    d.fixed_c_set = 1;
+}
 #define MUL(a, b) __fmul_rn((a), (b))
 #define ADD(a, b) __fadd_rn((a), (b))
 #define SUB(a, b) __fsub_rn((a), (b))
@@ -132,8 +155,8 @@ struct GaussModel {
     __device__ __forceinline__ void begin(const ModelDesc& d, const float* th, const float* consts) {
         tx = th[0];
         ty = th[1];
-        const float s2pi = __fsqrt_rn(MUL(2.0f, PB_PI));
-        const float s2 = __fsqrt_rn(2.0f);
+        const float s2pi = kSqrt2Pi;
+        const float s2 = kSqrt2;
         if (MID == MODEL_XYZIBG) {
             tI = th[3];
             tbg = th[4];
@@ -171,11 +194,18 @@ struct GaussModel {
             else if (MID == MODEL_XYIBG_CONSTSIGMA) { sx = consts[0]; sy = consts[1]; }
             else if (MID == MODEL_XYIBG_SIGMA) { sx = th[4]; sy = th[4]; }
             else { sx = th[4]; sy = th[5]; }
-            invSqrtPi = DIV(1.0f, __fsqrt_rn(PB_PI));
-            cx2 = DIV(1.0f, MUL(s2pi, sx));
-            cy2 = DIV(1.0f, MUL(s2pi, sy));
-            cx1 = DIV(1.0f, MUL(s2, sx));
-            cy1 = DIV(1.0f, MUL(s2, sy));
+            invSqrtPi = kInvSqrtPi;
+            if (MID == MODEL_XYIBG && d.fixed_c_set) {
+                cx2 = d.fixed_c[0];
+                cx1 = d.fixed_c[1];
+                cy2 = d.fixed_c[2];
+                cy1 = d.fixed_c[3];
+            } else {
+                cx2 = DIV(1.0f, MUL(s2pi, sx));
+                cy2 = DIV(1.0f, MUL(s2pi, sy));
+                cx1 = DIV(1.0f, MUL(s2, sx));
+                cy1 = DIV(1.0f, MUL(s2, sy));
+            }
             sigx = sx;
             sigy = sy;
             gax = gay = 0.0f;
@@ -195,8 +225,8 @@ struct GaussModel {
                                                 unsigned mask) {
         tx = th[0];
         ty = th[1];
-        const float s2pi = __fsqrt_rn(MUL(2.0f, PB_PI));
-        const float s2 = __fsqrt_rn(2.0f);
+        const float s2pi = kSqrt2Pi;
+        const float s2 = kSqrt2;
         if (MID == MODEL_XYZIBG) {
             tI = th[3];
             tbg = th[4];
@@ -271,7 +301,7 @@ struct GaussModel {
             // G21 = 1/(sqrt(2 pi) s s) * ((c-t-.5) exp(-(c-t-.5)^2/(2 s s)) - (c-t+.5) exp(-(c-t+.5)^2/(2 s s)))
             const float m = SUB(d0, 0.5f), p = ADD(d0, 0.5f);
             const float ss2 = MUL(MUL(2.0f, sig), sig);
-            const float a = DIV(1.0f, MUL(MUL(__fsqrt_rn(MUL(2.0f, PB_PI)), sig), sig));
+            const float a = DIV(1.0f, MUL(MUL(kSqrt2Pi, sig), sig));
             const float g = MUL(a, SUB(MUL(m, expf(DIV(MUL(-m, m), ss2))), MUL(p, expf(DIV(MUL(-p, p), ss2)))));
             r.z = MUL(tI, dE);
             r.w = g;
@@ -490,8 +520,8 @@ struct TiltedGaussModel {
         bgy = th[5];
         const float sx = kFreeSigma ? th[6 % K] : consts[0];
         const float sy = kFreeSigma ? th[7 % K] : consts[1];
-        const float s2pi = __fsqrt_rn(MUL(2.0f, PB_PI)), s2 = __fsqrt_rn(2.0f);
-        invSqrtPi = DIV(1.0f, __fsqrt_rn(PB_PI));
+        const float s2pi = kSqrt2Pi, s2 = kSqrt2;
+        invSqrtPi = kInvSqrtPi;
         cx2 = DIV(1.0f, MUL(s2pi, sx));
         cy2 = DIV(1.0f, MUL(s2pi, sy));
         cx1 = DIV(1.0f, MUL(s2, sx));
@@ -597,7 +627,7 @@ struct IntensityBgModel {
         tbg = th[1];
         tx = consts[0];
         ty = consts[1];
-        c1 = DIV(1.0f, MUL(__fsqrt_rn(2.0f), consts[2]));
+        c1 = DIV(1.0f, MUL(kSqrt2, consts[2]));
     }
 
     __device__ __forceinline__ void build_table(const ModelDesc& d, float* tab, int lane, int G) const {

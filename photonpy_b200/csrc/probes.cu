@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/photonpy_b200.h"
+#include "models.cuh"
 
 namespace {
 __global__ void __launch_bounds__(256) fma_probe_kernel(int iters, float a, float b, float* out) {
@@ -26,4 +29,46 @@ extern "C" double PB200_Fp32ProbeLaunch(int blocks, int threads, int iters, floa
     fma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, 0.9999999f, 1e-7f, d_out);
     if (cudaGetLastError() != cudaSuccess) return -1.0;
     return 2.0 * 8.0 * 16.0 * (double)iters * (double)blocks * (double)threads;  // FLOPs issued
+}
+
+namespace {
+// The set-up constants and the host-computed fixed-sigma scales against the device's own IEEE
+// square roots and divisions.
+__global__ void model_constants_kernel(const float* sigmas, int n, int* mismatches) {
+    int bad = 0;
+    if (pb200::kSqrt2Pi != __fsqrt_rn(__fmul_rn(2.0f, PB_PI))) bad++;
+    if (pb200::kSqrt2 != __fsqrt_rn(2.0f)) bad++;
+    if (pb200::kInvSqrtPi != __fdiv_rn(1.0f, __fsqrt_rn(PB_PI))) bad++;
+    for (int i = 0; i < n; i++) {
+        pb200::ModelDesc d{};
+        d.sigma[0] = sigmas[i];
+        d.sigma[1] = sigmas[i];
+        const float s2pi = __fsqrt_rn(__fmul_rn(2.0f, PB_PI)), s2 = __fsqrt_rn(2.0f);
+        if (__fdiv_rn(1.0f, __fmul_rn(s2pi, sigmas[i])) != sigmas[n + 2 * i]) bad++;
+        if (__fdiv_rn(1.0f, __fmul_rn(s2, sigmas[i])) != sigmas[n + 2 * i + 1]) bad++;
+    }
+    *mismatches = bad;
+}
+}  // namespace
+
+extern "C" int PB200_CheckModelConstants(int n, const float* h_sigmas, int* mismatches) {
+    float* d = nullptr;
+    int* dm = nullptr;
+    std::vector<float> buf((size_t)3 * n);
+    for (int i = 0; i < n; i++) {
+        pb200::ModelDesc m{};
+        m.sigma[0] = m.sigma[1] = h_sigmas[i];
+        pb200::model_desc_fixed_sigma(m);
+        buf[i] = h_sigmas[i];
+        buf[n + 2 * i] = m.fixed_c[0];
+        buf[n + 2 * i + 1] = m.fixed_c[1];
+    }
+    if (cudaMalloc(&d, sizeof(float) * buf.size()) != cudaSuccess) return -1;
+    if (cudaMalloc(&dm, sizeof(int)) != cudaSuccess) { cudaFree(d); return -1; }
+    cudaMemcpy(d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice);
+    model_constants_kernel<<<1, 1>>>(d, n, dm);
+    const cudaError_t e = cudaMemcpy(mismatches, dm, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    cudaFree(dm);
+    return e == cudaSuccess ? 0 : -1;
 }

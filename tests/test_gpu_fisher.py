@@ -75,3 +75,18 @@ def test_numerical_crlb_from_analytic_derivatives(name, ctx):
     ncrlb = est.NumCRLB(truth, useNumDeriv=False)
     assert np.quantile(np.abs(ncrlb - crlb) / crlb, 0.99) < 1e-4
     est.Destroy()
+
+
+def test_model_constants_match_device_arithmetic():
+    """The set-up constants and the host-computed fixed-sigma scales equal what the device's IEEE
+    square root and division give, so the fixed-sigma model's results do not depend on where
+    they were computed."""
+    import ctypes as ct
+    import photonpy_b200 as pb
+    L = pb.load_library()
+    sig = np.concatenate([np.linspace(0.5, 5.0, 4001), np.random.default_rng(5).uniform(0.3, 50, 4000)]).astype(
+        np.float32)
+    bad = ct.c_int(-1)
+    L.PB200_CheckModelConstants.argtypes = [ct.c_int, ct.c_void_p, ct.POINTER(ct.c_int)]
+    assert L.PB200_CheckModelConstants(len(sig), sig.ctypes.data, ct.byref(bad)) == 0
+    assert bad.value == 0
