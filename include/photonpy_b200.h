@@ -433,7 +433,9 @@ int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
  * roisPerChunk (0: automatic), with `slots` chunks (2..4) in flight: while one chunk is fitted
  * the next ones are copied in and the previous ones copied out. Returns 0 or -1. */
 int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots);
-/* Lanes per ROI and threads per block the fit kernel of this estimator launches with. */
+/* Lanes per ROI and threads per block the fit kernel of this estimator launches with (for large
+ * ROIs the block is smaller than the configured threads per block, so that its groups' shared
+ * memory fits). */
 void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock);
 /* Fit kernel family for the Gaussian models: 0 = column-blocked (default), 1 = generic
  * per-pixel table kernel (the spline model always uses 1). Returns 0 on success. */

@@ -281,6 +281,39 @@ struct Estimator {
         fit_shape(G, cpl);
         return (cpl && G == 2) ? 128 : 256;
     }
+    // Shared-memory floats per group of the fit kernel this configuration launches.
+    int group_stride_floats() const {
+        int G, cpl;
+        fit_shape(G, cpl);
+        const int R = desc.roisize;
+        if (cpl) {
+            switch (K) {
+            case 4: return gauss_group_stride<4>(R, G, cpl);
+            case 5: return gauss_group_stride<5>(R, G, cpl);
+            default: return gauss_group_stride<6>(R, G, cpl);
+            }
+        }
+        switch (desc.model) {
+        case MODEL_XYIBG: return group_smem_floats<GaussModel<MODEL_XYIBG>>(R);
+        case MODEL_XYIBG_CONSTSIGMA: return group_smem_floats<GaussModel<MODEL_XYIBG_CONSTSIGMA>>(R);
+        case MODEL_XYIBG_SIGMA: return group_smem_floats<GaussModel<MODEL_XYIBG_SIGMA>>(R);
+        case MODEL_XYIBG_SIGMAXY: return group_smem_floats<GaussModel<MODEL_XYIBG_SIGMAXY>>(R);
+        case MODEL_XYZIBG: return group_smem_floats<GaussModel<MODEL_XYZIBG>>(R);
+        case MODEL_XYITILTEDBG: return group_smem_floats<TiltedGaussModel<MODEL_XYITILTEDBG>>(R);
+        case MODEL_XYITILTEDBG_SIGMAXY: return group_smem_floats<TiltedGaussModel<MODEL_XYITILTEDBG_SIGMAXY>>(R);
+        case MODEL_INTENSITYBG: return group_smem_floats<IntensityBgModel>(R);
+        case MODEL_CSPLINE_TILTED: return group_smem_floats<SplineModelT<1>>(R);
+        case MODEL_CSPLINE_BGIMAGE: return group_smem_floats<SplineModelT<2>>(R);
+        default: return group_smem_floats<SplineModelT<0>>(R);
+        }
+    }
+    // Threads per block the fit kernel actually launches with: threads_for(), halved where the
+    // groups of a block would need more shared memory than a block may have (large ROIs).
+    int launched_threads_for() const {
+        int G, cpl;
+        fit_shape(G, cpl);
+        return launched_threads(threads_for(), G, group_stride_floats());
+    }
     // Fit launcher for this estimator's model, ROI size and kernel configuration.
     FitLaunch fit_launch() const {
         int G, cpl;
@@ -1224,7 +1257,7 @@ void PB200_GetKernelConfig(Estimator* e, int* lanesPerRoi, int* threadsPerBlock)
         int cpl;
         e->fit_shape(*lanesPerRoi, cpl);
     }
-    if (threadsPerBlock) *threadsPerBlock = e->threads_for();
+    if (threadsPerBlock) *threadsPerBlock = e->launched_threads_for();
 }
 
 int PB200_ModelInfo(Estimator* e, int* roisize) {

@@ -43,17 +43,21 @@ inline void set_smem_attr(KernelT kern, size_t smem) {
     }
 }
 
+// Threads per block a group kernel launches with: the requested count, halved while the block's
+// shared memory (threads / G groups of strideFloats floats) exceeds kMaxSmemPerBlock.
+inline int launched_threads(int threads, int G, int strideFloats) {
+    while ((size_t)(threads / G) * strideFloats * sizeof(float) > (size_t)kMaxSmemPerBlock && threads > 32)
+        threads /= 2;
+    return threads;
+}
+
 // Launch a persistent group kernel: `strideFloats` of shared memory per group of G lanes.
 template <class KernelT>
 inline void launch_groups(KernelT kern, int G, int threads, int strideFloats, int n, const ModelDesc& d, FitArgs a,
                           cudaStream_t s) {
-    int gpb = threads / G;
-    size_t smem = (size_t)gpb * strideFloats * sizeof(float);
-    while (smem > (size_t)kMaxSmemPerBlock && threads > 32) {
-        threads /= 2;
-        gpb = threads / G;
-        smem = (size_t)gpb * strideFloats * sizeof(float);
-    }
+    threads = launched_threads(threads, G, strideFloats);
+    const int gpb = threads / G;
+    const size_t smem = (size_t)gpb * strideFloats * sizeof(float);
     if (smem > (size_t)kMaxSmemPerBlock || gpb < 1) throw std::runtime_error("ROI too large for shared memory");
     set_smem_attr(kern, smem);
     int perSM = 0;
