@@ -430,7 +430,7 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
  * Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
 /* Extension: the host-pointer pipeline of the Estimate/CRLB calls. The ROIs are fitted in chunks of
- * roisPerChunk (0: automatic), with `slots` chunks (2..4) in flight: while one chunk is fitted
+ * roisPerChunk (0: automatic), with `slots` chunks (2..8) in flight: while one chunk is fitted
  * the next ones are copied in and the previous ones copied out. Returns 0 or -1. */
 int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots);
 /* Lanes per ROI and threads per block the fit kernel of this estimator launches with (for large

@@ -248,8 +248,9 @@ struct Estimator {
     std::mutex mtx;
     // host-pointer pipeline: ROIs per chunk (0: automatic) and slots (chunks in flight, 2..4)
     int hostChunk = 0;
+    static constexpr int kMaxSlots = 8;
     int hostSlots = 4;
-    Slot slots[4];
+    Slot slots[kMaxSlots];
 
     Estimator() { PB_CUDA(cudaGetDevice(&device)); }
     ~Estimator() {
@@ -532,7 +533,7 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         }
     }
     for (auto& p : pend) d2h(p);
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < Estimator::kMaxSlots; i++)
         if (e->slots[i].stream) PB_CUDA(cudaStreamSynchronize(e->slots[i].stream));
 }
 
@@ -1237,7 +1238,7 @@ int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock) {
 }
 
 int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots) {
-    if (!e || roisPerChunk < 0 || slots < 2 || slots > 4) return -1;
+    if (!e || roisPerChunk < 0 || slots < 2 || slots > Estimator::kMaxSlots) return -1;
     std::lock_guard<std::mutex> g(e->mtx);
     e->hostChunk = roisPerChunk;
     e->hostSlots = slots;
