@@ -266,6 +266,38 @@ FitLaunch generic_fit_table(int G) {
     }
 }
 
+// Spline launchers: the reference-form instance (one voxel per pixel, OVS = false) unless the
+// description carries a finer calibration (spline_q != 1), which runs the OVS instance.
+template <int MODE, int G>
+void launch_fit_spline(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s) {
+    if (d.spline_q == 1.0f) launch_fit_generic<SplineModelT<MODE, false>, G>(d, a, threads, s);
+    else launch_fit_generic<SplineModelT<MODE, true>, G>(d, a, threads, s);
+}
+template <int MODE>
+FitLaunch spline_fit_table(int G) {
+    switch (G) {
+    case 2:
+    case 4: return launch_fit_spline<MODE, 4>;
+    case 8: return launch_fit_spline<MODE, 8>;
+    case 16: return launch_fit_spline<MODE, 16>;
+    default: return launch_fit_spline<MODE, 32>;
+    }
+}
+template <int MODE, int G>
+void launch_eval_spline(const ModelDesc& d, const float* params, const float* consts, float* ev, float* deriv, int n,
+                        int threads, cudaStream_t s) {
+    if (d.spline_q == 1.0f) launch_eval<SplineModelT<MODE, false>, G>(d, params, consts, ev, deriv, n, threads, s);
+    else launch_eval<SplineModelT<MODE, true>, G>(d, params, consts, ev, deriv, n, threads, s);
+}
+template <int MODE>
+EvalLaunch spline_eval_table(int G) {
+    switch (G) {
+    case 8: return launch_eval_spline<MODE, 8>;
+    case 16: return launch_eval_spline<MODE, 16>;
+    default: return launch_eval_spline<MODE, 32>;
+    }
+}
+
 template <class M>
 EvalLaunch eval_table(int G) {
     switch (G) {

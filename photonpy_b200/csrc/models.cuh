@@ -65,10 +65,9 @@ struct ModelDesc {
     // addresses (the fit kernels' copy; null when the caller supplies coefs directly)
     const float4* coefsQ;
     // fixed-sigma XYIBg: 1/(sqrt(2 pi) sigma_x), 1/(sqrt(2) sigma_x), then the same for y, computed
-    // once per estimator with the reference's float operations (model_desc_fixed_sigma); the other
-    // models compute their scales per ROI and iteration
+    // once per estimator with the reference's float operations (model_desc_fixed_sigma; all 0 when
+    // not computed); the other models compute their scales per ROI and iteration
     float fixed_c[4];
-    int fixed_c_set;
 };
 
 
@@ -101,7 +100,6 @@ inline void model_desc_fixed_sigma(ModelDesc& d) {
     d.fixed_c[1] = 1.0f / (kSqrt2 * d.sigma[0]);
     d.fixed_c[2] = 1.0f / (kSqrt2Pi * d.sigma[1]);
     d.fixed_c[3] = 1.0f / (kSqrt2 * d.sigma[1]);
-    d.fixed_c_set = 1;
 }
 #define MUL(a, b) __fmul_rn((a), (b))
 #define ADD(a, b) __fadd_rn((a), (b))
@@ -195,7 +193,7 @@ struct GaussModel {
             else if (MID == MODEL_XYIBG_SIGMA) { sx = th[4]; sy = th[4]; }
             else { sx = th[4]; sy = th[5]; }
             invSqrtPi = kInvSqrtPi;
-            if (MID == MODEL_XYIBG && d.fixed_c_set) {
+            if (MID == MODEL_XYIBG && d.fixed_c[0] > 0.0f) {
                 cx2 = d.fixed_c[0];
                 cx1 = d.fixed_c[1];
                 cy2 = d.fixed_c[2];
@@ -664,12 +662,14 @@ struct IntensityBgModel {
 };
 
 // ---------------------------------------------------------------------------------------
-// Cubic spline: table = delta_f, delta_dxf, delta_dyf, delta_dzf [4][64]. MODE 0 flat
+// Cubic spline: table = delta_f, delta_dxf, delta_dyf, delta_dzf [4][64]. OVS: the calibration is
+// sampled finer than a pixel (ModelDesc::spline_q voxels per pixel, the oversampled extension);
+// without it the voxel scale is 1 at compile time, photonpy's model exactly. MODE 0 flat
 // background, 1 tilted background (theta += bgx, bgy; mu += bgx (x - W/2) + bgy (y - W/2)),
 // 2 background image (mu = I psf + bg * image; the image is the spot's R*R constants, read
 // per pixel through `img`; this mode centres tx, ty differently, CubicSplinePSFModels.h:371-374).
 // ---------------------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, bool OVS = false>
 struct SplineModelT {
     static constexpr int K = (MODE == 1) ? 7 : 5;
     static constexpr int kId = (MODE == 0) ? MODEL_CSPLINE : (MODE == 1 ? MODEL_CSPLINE_TILTED : MODEL_CSPLINE_BGIMAGE);
@@ -679,6 +679,9 @@ struct SplineModelT {
 
     float tx, ty, tI, tbg, du;
     float q;  // voxels per ROI pixel (1: the reference's model)
+
+    // pixel index c in spline-grid units before the centre offset: q c (c itself without OVS)
+    __device__ __forceinline__ float gridc(int c) const { return OVS ? MUL((float)c, q) : (float)c; }
     float spx, spy, spz;
     float bgx, bgy, halfw;
     const float* img;  // MODE 2: this spot's background image [R][R]
@@ -690,15 +693,15 @@ struct SplineModelT {
         Ny = d.spline_shape[1];
         Nx = d.spline_shape[2];
         du = DIV(SUB(d.spline_zmax, d.spline_zmin), (float)Nz);
-        q = d.spline_q;
+        q = OVS ? d.spline_q : 1.0f;
         if (MODE == 2) {
             const float w = (float)d.roisize;
             tx = ADD(ADD(SUB(th[0], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Nx), 1.0f), 2.0f)), 0.5f);
             ty = ADD(ADD(SUB(th[1], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Ny), 1.0f), 2.0f)), 0.5f);
         } else {
             // grid coordinate of pixel x: q x - tx (q = 1: x - (theta_x - Nx/2), the reference)
-            tx = SUB(MUL(th[0], q), MUL((float)Nx, 0.5f));
-            ty = SUB(MUL(th[1], q), MUL((float)Ny, 0.5f));
+            tx = SUB(OVS ? MUL(th[0], q) : th[0], MUL((float)Nx, 0.5f));
+            ty = SUB(OVS ? MUL(th[1], q) : th[1], MUL((float)Ny, 0.5f));
         }
         tI = th[3];
         tbg = th[4];
@@ -710,9 +713,9 @@ struct SplineModelT {
         // which is its fractional part wherever the model is valid (Nx/2 >= max x); the
         // oversampled extension takes the fractional part (floor) everywhere
         float sx = -tx;
-        spx = SUB(sx, q == 1.0f ? (float)(int)sx : floorf(sx));
+        spx = SUB(sx, OVS ? floorf(sx) : (float)(int)sx);
         float sy = -ty;
-        spy = SUB(sy, q == 1.0f ? (float)(int)sy : floorf(sy));
+        spy = SUB(sy, OVS ? floorf(sy) : (float)(int)sy);
         float sz = DIV(SUB(th[2], d.spline_zmin), du);
         int kk = (int)sz;
         kk = max(0, min(kk, Nz - 1));
@@ -746,9 +749,9 @@ struct SplineModelT {
 
     __device__ __forceinline__ void pixel(const ModelDesc& d, const float* tab, int x, int y, float& mu,
                                           float (&J)[K]) const {
-        const float yy = SUB(MUL((float)y, q), ty);
+        const float yy = SUB(gridc(y), ty);
         const int j = max(0, min((int)yy, Ny - 1));
-        const float xx = SUB(MUL((float)x, q), tx);
+        const float xx = SUB(gridc(x), tx);
         const int i = max(0, min((int)xx, Nx - 1));
         const float4* c4 = reinterpret_cast<const float4*>(d.coefs + 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i));
         const float4* f4 = reinterpret_cast<const float4*>(tab);
@@ -762,8 +765,8 @@ struct SplineModelT {
             dy = ADD(ADD(ADD(ADD(dy, MUL(e.x, c.x)), MUL(e.y, c.y)), MUL(e.z, c.z)), MUL(e.w, c.w));
             dz = ADD(ADD(ADD(ADD(dz, MUL(g.x, c.x)), MUL(g.y, c.y)), MUL(g.z, c.z)), MUL(g.w, c.w));
         }
-        dx = MUL(dx, -MUL(tI, q));
-        dy = MUL(dy, -MUL(tI, q));
+        dx = MUL(dx, OVS ? -MUL(tI, q) : -tI);
+        dy = MUL(dy, OVS ? -MUL(tI, q) : -tI);
         dz = MUL(dz, DIV(tI, du));
         if (psf < 0.0f) psf = 0.0f;
         J[0] = dx;
@@ -800,8 +803,8 @@ struct SplineModelT {
         const size_t qstride = qmajor ? nvox : 1;
 #pragma unroll
         for (int t = 0; t < PB; t++) {
-            const int j = max(0, min((int)SUB(MUL((float)y[t], q), ty), Ny - 1));
-            const int i = max(0, min((int)SUB(MUL((float)x[t], q), tx), Nx - 1));
+            const int j = max(0, min((int)SUB(gridc(y[t]), ty), Ny - 1));
+            const int i = max(0, min((int)SUB(gridc(x[t]), tx), Nx - 1));
             const size_t v = (size_t)k * Nx * Ny + (size_t)j * Nx + i;
             cp[t] = qmajor ? d.coefsQ + v : reinterpret_cast<const float4*>(d.coefs) + 16 * v;
             psf[t] = ddx[t] = ddy[t] = ddz[t] = 0.0f;
@@ -820,7 +823,7 @@ struct SplineModelT {
             }
         }
         const float zs = DIV(tI, du);
-        const float xs = -MUL(tI, q);
+        const float xs = OVS ? -MUL(tI, q) : -tI;
 #pragma unroll
         for (int t = 0; t < PB; t++) {
             float p = psf[t];
@@ -848,8 +851,8 @@ struct SplineModelT {
 
     // Offset of the 64 coefficients pixel (x, y) reads (same voxel choice as pixel()).
     __device__ __forceinline__ size_t coef_offset(int x, int y) const {
-        const int j = max(0, min((int)SUB(MUL((float)y, q), ty), Ny - 1));
-        const int i = max(0, min((int)SUB(MUL((float)x, q), tx), Nx - 1));
+        const int j = max(0, min((int)SUB(gridc(y), ty), Ny - 1));
+        const int i = max(0, min((int)SUB(gridc(x), tx), Nx - 1));
         return 64 * ((size_t)k * Nx * Ny + (size_t)j * Nx + i);
     }
 
