@@ -44,6 +44,12 @@ def localization_flops(kind: str, R: int, iterations, max_iterations: int = 50) 
     return float(per_it * it.sum() + fisher * it.size)
 
 
+def lm_flops(kind: str, R: int, iterations, max_iterations: int = 50) -> float:
+    """The LM launch's share of localization_flops (everything but the Fisher pass)."""
+    it = np.minimum(np.asarray(iterations, dtype=np.int64), max_iterations).astype(np.float64)
+    return float((R * R * flops_per_pixel_iteration(kind) + flops_per_solve(kind)) * it.sum())
+
+
 def transcendental_ops(kind: str, R: int, iterations, max_iterations: int = 50) -> float:
     """erf/exp evaluations (separable form: 2R 1D terms per iteration)."""
     it = np.minimum(np.asarray(iterations, dtype=np.int64), max_iterations).astype(np.float64)
