@@ -1337,11 +1337,16 @@ int PB200_SplineCoefGradient(Estimator* e, int numspots, const float* d_sample, 
 // ---- mixed-model, mixed-size batches in one persistent launch ----
 }  // extern "C"
 
+#ifndef PB200_MIXED_TWO_LANES
+#define PB200_MIXED_TWO_LANES 1
+#endif
+
 struct MixedPlan {
     int device = 0;
     int ntasks = 0, totalTiles = 0, tileRois = 32, variant = 0, strideFloats = 0;
     std::vector<MixedTask> tasks;
     std::vector<int> K;
+    std::vector<int> twoLane;  // per bucket: its LM pass runs 2 lanes per ROI
     DevBuf dTasks, dTasksFisher, dCounter, dFisher;  // dCounter: per-bucket ROI counters of the two passes
     bool anyFisher = false;
     cudaGraph_t graph = nullptr;
@@ -1430,28 +1435,50 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                         a.fisher = p->dFisher.as<float>() + off;
                         off += (size_t)fisher_row_floats(e->K) * counts[b];
                     }
-                    const int cpl = (e->desc.roisize + G - 1) / G;
-                    t.handler = e->desc.model * 4 + cpl - 1;
+                    const int R = e->desc.roisize;
+                    const int cpl = (R + G - 1) / G;
+                    t.handler = mixed_handler(e->desc.model, G, cpl);
                     p->totalTiles += (counts[b] + tileRois - 1) / tileRois;
+                    int base4 = 0;
                     switch (e->K) {
-                    case 4: p->strideFloats = std::max(p->strideFloats, gauss_group_base_floats<4>(e->desc.roisize)); break;
-                    case 5: p->strideFloats = std::max(p->strideFloats, gauss_group_base_floats<5>(e->desc.roisize)); break;
-                    default: p->strideFloats = std::max(p->strideFloats, gauss_group_base_floats<6>(e->desc.roisize)); break;
+                    case 4: base4 = gauss_group_base_floats<4>(R); break;
+                    case 5: base4 = gauss_group_base_floats<5>(R); break;
+                    default: base4 = gauss_group_base_floats<6>(R); break;
+                    }
+                    p->strideFloats = std::max(p->strideFloats, base4);
+                    // 7..10 px buckets in two 2-lane groups per 4-lane slot, each with half of the
+                    // slot (pixels + y-terms or FP64 re-solve scratch; the Fisher pass stores its rows
+                    // in the plan's scratch, so neither pass needs in-kernel Fisher scratch)
+                    if (PB200_MIXED_TWO_LANES && R >= 7 && R <= 10) {
+                        p->twoLane.push_back(1);
+                        p->strideFloats = std::max(p->strideFloats,
+                                                   2 * round_up(round_up(R * R, 4) + cmax(4 * R, rescue_floats(e->K)), 4));
+                    } else {
+                        p->twoLane.push_back(0);
                     }
                     p->tasks.push_back(t);
                     p->K.push_back(e->K);
                 }
                 p->ntasks = (int)p->tasks.size();
+                bool anyTwo = false;
+                for (int b = 0; b < p->ntasks; b++) anyTwo = anyTwo || p->twoLane[b];
                 {
-                    // group stride: of the largest bucket's floats + 0, 4, ..., 28, the one with the
-                    // fewest modelled bank conflicts over the buckets, weighted by their ROI counts
-                    const int base = p->strideFloats;
+                    // group stride: of the largest bucket's floats + 0, 4, ..., 28 (multiples of 8 when
+                    // 2-lane groups take half a slot each, so that each half stays 16-byte aligned), the
+                    // one with the fewest modelled bank conflicts over the buckets, weighted by their
+                    // ROI counts
+                    const int step = anyTwo ? 8 : 4;
+                    const int base = round_up(p->strideFloats, step);
                     long long bestCost = -1;
-                    for (int S = base; S < base + 32; S += 4) {
+                    for (int S = base; S < base + 32; S += step) {
                         long long cost = 0;
-                        for (const MixedTask& t : p->tasks) {
+                        for (int b = 0; b < p->ntasks; b++) {
+                            const MixedTask& t = p->tasks[b];
                             const int R = t.d.roisize;
-                            cost += (long long)t.a.n * gauss_stride_conflicts(S, round_up(R * R, 4), R, G, (R + G - 1) / G);
+                            if (p->twoLane[b])
+                                cost += (long long)t.a.n * gauss_stride_conflicts(S / 2, round_up(R * R, 4), R, 2, (R + 1) / 2);
+                            else
+                                cost += (long long)t.a.n * gauss_stride_conflicts(S, round_up(R * R, 4), R, G, (R + G - 1) / G);
                         }
                         if (bestCost < 0 || cost < bestCost) {
                             bestCost = cost;
@@ -1461,6 +1488,10 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                 }
                 std::vector<MixedTask> lmTasks(p->tasks), fiTasks(p->tasks);
                 for (int b = 0; b < p->ntasks; b++) {
+                    if (p->twoLane[b]) {
+                        lmTasks[b].handler = mixed_handler(lmTasks[b].d.model, 2, (lmTasks[b].d.roisize + 1) / 2);
+                        fiTasks[b].handler = lmTasks[b].handler;
+                    }
                     lmTasks[b].a = lm_pass_args(p->tasks[b].a);
                     fiTasks[b].a = fisher_pass_args(p->tasks[b].a);
                     if (!p->tasks[b].a.crlb) fiTasks[b].a.n = 0;  // its tiles end at once

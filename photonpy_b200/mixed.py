@@ -98,12 +98,12 @@ class MixedBatch:
         self.captured = True
         return self
 
-    def run_plain(self, stream=None, lanes=4):
+    def run_plain(self, stream=None, lanes=None):
         """The same work as single-model launches, bucket by bucket (LM, Fisher and CRLB
-        launches each). With lanes=4, the mixed kernel's lanes per ROI, the results are
-        bit-identical to run(); lanes=None keeps each estimator's own kernel configuration
-        (2 lanes per ROI for 7..10 pixel Gaussians by default, whose pixel sums then run in
-        another order)."""
+        launches each). lanes=None keeps each estimator's own kernel configuration (by default 2
+        lanes per ROI for 7..10 pixel Gaussians, 4 for larger ones, as the mixed kernel runs
+        them), whose results are bit-identical to run(); lanes=4 runs every bucket with 4 lanes
+        per ROI (the 7..10 pixel buckets then sum their pixels in another order)."""
         for b in self.buckets:
             est, o = b["est"], b["out"]
             saved = est.kernel_config_setting()

@@ -1,5 +1,6 @@
 """One persistent launch over mixed PSF models and ROI sizes gives exactly the results of
-one launch per (model, ROI size); a captured CUDA graph replays the same results."""
+one launch per (model, ROI size) at each estimator's default configuration (2 lanes per ROI for
+the 7..10 px buckets, 4 for the larger ones); a captured CUDA graph replays the same results."""
 import numpy as np
 import pytest
 
@@ -33,7 +34,7 @@ def test_mixed_launch_equals_plain_launches(ctx, tile):
     mb = MixedBatch(buckets, tile_rois=tile).run()
     torch.cuda.synchronize()
     fused = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
-    mb.run_plain()
+    mb.run_plain(lanes=None)
     torch.cuda.synchronize()
     for f, p in zip(fused, mb.results()):
         for k in f:
@@ -41,10 +42,10 @@ def test_mixed_launch_equals_plain_launches(ctx, tile):
     mb.close()
 
 
-def test_mixed_launch_close_to_default_config_launches(ctx):
-    """With each estimator's own configuration (2 lanes per ROI for the 7 and 9 px buckets)
-    the per-bucket launches sum pixels in another order: the fits agree to within float
-    rounding on the ROIs both sides converge on, and the estimators' settings are restored."""
+def test_mixed_launch_close_to_four_lane_launches(ctx):
+    """With 4 lanes per ROI for every bucket the per-bucket launches sum the pixels of the 7 and
+    9 px buckets in another order: the fits agree to within float rounding on the ROIs both
+    sides converge on, and the estimators' settings are restored."""
     import torch
     from photonpy_b200.mixed import MixedBatch
     buckets = _buckets(ctx, n=3000, seed=7)
@@ -56,9 +57,8 @@ def test_mixed_launch_close_to_default_config_launches(ctx):
     mb.run_plain(lanes=None)
     torch.cuda.synchronize()
     assert [b[0].GetKernelConfig() for b in buckets] == before
-    mb.run_plain()
+    mb.run_plain(lanes=4)
     assert [b[0].GetKernelConfig() for b in buckets] == before
-    mb.run_plain(lanes=None)
     torch.cuda.synchronize()
     for f, p in zip(fused, mb.results()):
         conv = ((f["iterations"] < 50) & (p["iterations"] < 50)).cpu().numpy()
