@@ -454,9 +454,10 @@ def run_mixed(args):
             mb.run(s)  # launches of one step, counted outside the timed loop (which has warm-up runs)
             launches = (pb.launch_count() - n0) * args.steps
         n0 = pb.launch_count()
-        mb.run_plain(s, lanes=None)
+        mb.run_plain(s)
         plain_launches = pb.launch_count() - n0
-        ms_plain = timed(lambda: mb.run_plain(s, lanes=None), args.steps)
+        ms_plain = timed(lambda: mb.run_plain(s), args.steps)
+        ms_plain_default = timed(lambda: mb.run_plain(s, lanes=None), args.steps)
         ms_plain_4 = timed(lambda: mb.run_plain(s, lanes=4), args.steps)
         mb.run(s)  # results of the fused path for the flop count below
     flops = 0.0
@@ -493,13 +494,15 @@ def run_mixed(args):
         data="synthetic (seeded Poisson ROIs, photonpy_b200.synth)",
         config=dict(workload=w["desc"], rois=n, buckets=len(groups), tile_rois=tile, threads_per_block=threads,
                     autotuned=(tuned["timings"] if tuned else None),
-                    lanes_per_roi="2 for the 7 and 9 px buckets, 4 for the 11 and 16 px buckets",
+                    lanes_per_roi=dict(zip([f"{g['kind']}_{g['R']}" for g in groups], mb.lanes())),
                     graph_replay=True, lm_iterations=MAX_IT, lm_lambda=LAMBDA,
                     l2="inputs of %.2f GB per step exceed the 126 MB L2" % (sum(x.numel() for x in xs) * 4 / 1e9)),
         plain_gpu=dict(value=n / (ms_plain * 1e-3), ms_per_step=ms_plain, launches_per_step=plain_launches,
-                       what="the LM, Fisher and CRLB launches of every (model, ROI size) bucket at each "
-                            "estimator's default kernel configuration, the same lanes per ROI and results "
-                            "as the fused form"),
+                       what="the LM, Fisher and CRLB launches of every (model, ROI size) bucket with the "
+                            "fused form's lanes per ROI (the same results bit for bit)"),
+        plain_gpu_default_config=dict(value=n / (ms_plain_default * 1e-3), ms_per_step=ms_plain_default,
+                                      what="the same per-bucket launches at each estimator's default "
+                                           "configuration (2 lanes per ROI for the 7 and 9 px buckets)"),
         plain_gpu_4_lanes=dict(value=n / (ms_plain_4 * 1e-3), ms_per_step=ms_plain_4,
                                what="the same per-bucket launches with 4 lanes per ROI for every bucket"),
         fused_over_plain=ms_plain / ms_fused,

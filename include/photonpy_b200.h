@@ -407,6 +407,11 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
 int PB200_MixedPlanRun(MixedPlan* plan, void* stream);
 int PB200_MixedPlanCapture(MixedPlan* plan, void* stream);
 int PB200_MixedPlanInfo(MixedPlan* plan, int* ntasks, int* totalTiles, int* strideFloats);
+/* Lanes per ROI each bucket of the plan runs with (lanes[nbuckets], in the order passed to
+ * PB200_MixedPlanCreate): 4, or 2 for 7..10 px buckets of at least 1024 ROIs per SM (as the
+ * per-bucket launches do by default). Per-bucket launches with these lanes per ROI give the
+ * plan's results bit for bit. Returns 0, or -1 on a bad argument. */
+int PB200_MixedPlanLanes(MixedPlan* plan, int nbuckets, int* lanes);
 void PB200_MixedPlanDestroy(MixedPlan* plan);
 /* No counterpart in the reference. Fit + CRLB + chi-square in one call like PB200_EstimateDevice,
  * for callers that must not allocate device memory during a fit (real-time acquisition loops

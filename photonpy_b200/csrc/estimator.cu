@@ -1340,13 +1340,17 @@ int PB200_SplineCoefGradient(Estimator* e, int numspots, const float* d_sample, 
 #ifndef PB200_MIXED_TWO_LANES
 #define PB200_MIXED_TWO_LANES 1
 #endif
+// ROIs per SM from which a 7..10 px bucket of a mixed plan runs 2 lanes per ROI (about 4 per
+// resident 2-lane group at 2 blocks of 256 threads per SM)
+constexpr int kTwoLaneMinRoisPerSM = 1024;
 
 struct MixedPlan {
     int device = 0;
     int ntasks = 0, totalTiles = 0, tileRois = 32, variant = 0, strideFloats = 0;
     std::vector<MixedTask> tasks;
     std::vector<int> K;
-    std::vector<int> twoLane;  // per bucket: its LM pass runs 2 lanes per ROI
+    std::vector<int> twoLane;      // per task: it runs 2 lanes per ROI
+    std::vector<int> bucketLanes;  // per bucket as passed in: lanes per ROI of its launches
     DevBuf dTasks, dTasksFisher, dCounter, dFisher;  // dCounter: per-bucket ROI counters of the two passes
     bool anyFisher = false;
     cudaGraph_t graph = nullptr;
@@ -1446,10 +1450,15 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     default: base4 = gauss_group_base_floats<6>(R); break;
                     }
                     p->strideFloats = std::max(p->strideFloats, base4);
-                    // 7..10 px buckets in two 2-lane groups per 4-lane slot, each with half of the
-                    // slot (pixels + y-terms or FP64 re-solve scratch; the Fisher pass stores its rows
-                    // in the plan's scratch, so neither pass needs in-kernel Fisher scratch)
-                    if (PB200_MIXED_TWO_LANES && R >= 7 && R <= 10) {
+                    // 7..10 px buckets with at least kTwoLaneMinRoisPerSM ROIs per SM in two 2-lane
+                    // groups per 4-lane slot, each with half of the slot (pixels + y-terms or FP64
+                    // re-solve scratch; the Fisher pass stores its rows in the plan's scratch, so
+                    // neither pass needs in-kernel Fisher scratch). A 2-lane group takes about twice
+                    // as long per ROI: with few ROIs per group the last ROIs of a bucket would end
+                    // late (a 12-bucket batch of 40k ROIs: 24.2 against 28.8 M/s), with many the
+                    // fuller lanes win (4M ROIs: 118.7 against 112.9 M/s).
+                    if (PB200_MIXED_TWO_LANES && R >= 7 && R <= 10 &&
+                        (long long)counts[b] >= (long long)kTwoLaneMinRoisPerSM * num_sms()) {
                         p->twoLane.push_back(1);
                         p->strideFloats = std::max(p->strideFloats,
                                                    2 * round_up(round_up(R * R, 4) + cmax(4 * R, rescue_floats(e->K)), 4));
@@ -1460,6 +1469,8 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     p->K.push_back(e->K);
                 }
                 p->ntasks = (int)p->tasks.size();
+                for (int b = 0, t = 0; b < nbuckets; b++)
+                    p->bucketLanes.push_back(counts[b] == 0 ? G : (p->twoLane[t++] ? 2 : G));
                 bool anyTwo = false;
                 for (int b = 0; b < p->ntasks; b++) anyTwo = anyTwo || p->twoLane[b];
                 {
@@ -1572,6 +1583,12 @@ int PB200_MixedPlanInfo(MixedPlan* p, int* ntasks, int* totalTiles, int* strideF
     if (ntasks) *ntasks = p->ntasks;
     if (totalTiles) *totalTiles = p->totalTiles;
     if (strideFloats) *strideFloats = p->strideFloats;
+    return 0;
+}
+
+int PB200_MixedPlanLanes(MixedPlan* p, int nbuckets, int* lanes) {
+    if (!p || !lanes || nbuckets != (int)p->bucketLanes.size()) return -1;
+    for (int b = 0; b < nbuckets; b++) lanes[b] = p->bucketLanes[b];
     return 0;
 }
 

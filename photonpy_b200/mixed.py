@@ -26,6 +26,8 @@ def _bind(L):
     L.PB200_MixedPlanInfo.argtypes = [vp, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
     L.PB200_MixedPlanInfo.restype = ct.c_int
     L.PB200_MixedPlanDestroy.argtypes = [vp]
+    L.PB200_MixedPlanLanes.argtypes = [vp, ct.c_int, vp]
+    L.PB200_MixedPlanLanes.restype = ct.c_int
     return L
 
 
@@ -98,17 +100,27 @@ class MixedBatch:
         self.captured = True
         return self
 
-    def run_plain(self, stream=None, lanes=None):
+    def lanes(self):
+        """Lanes per ROI each bucket runs with in the fused launches (4, or 2 for large 7..10 px
+        buckets)."""
+        arr = (ct.c_int * len(self.buckets))()
+        if self._L.PB200_MixedPlanLanes(self.plan, len(self.buckets), arr) != 0:
+            check_error("MixedPlanLanes")
+        return list(arr)
+
+    def run_plain(self, stream=None, lanes="plan"):
         """The same work as single-model launches, bucket by bucket (LM, Fisher and CRLB
-        launches each). lanes=None keeps each estimator's own kernel configuration (by default 2
-        lanes per ROI for 7..10 pixel Gaussians, 4 for larger ones, as the mixed kernel runs
-        them), whose results are bit-identical to run(); lanes=4 runs every bucket with 4 lanes
-        per ROI (the 7..10 pixel buckets then sum their pixels in another order)."""
-        for b in self.buckets:
+        launches each). lanes="plan" uses the lanes per ROI the fused launches chose for each
+        bucket (lanes()), which gives run()'s results bit for bit; None keeps each estimator's own
+        kernel configuration (2 lanes per ROI for 7..10 pixel Gaussians by default); an int
+        runs every bucket with that many lanes per ROI."""
+        plan_lanes = self.lanes() if lanes == "plan" else None
+        for i, b in enumerate(self.buckets):
             est, o = b["est"], b["out"]
             saved = est.kernel_config_setting()
-            if lanes is not None:
-                est.SetKernelConfig(lanes, 0, variant=0)
+            g = plan_lanes[i] if plan_lanes is not None else lanes
+            if g is not None:
+                est.SetKernelConfig(g, 0, variant=0)
             try:
                 est.EstimateDevice(b["samples"], constants=b["constants"], with_crlb=self.with_crlb, stream=stream,
                                    out=o)

@@ -1,6 +1,6 @@
 """One persistent launch over mixed PSF models and ROI sizes gives exactly the results of
-one launch per (model, ROI size) at each estimator's default configuration (2 lanes per ROI for
-the 7..10 px buckets, 4 for the larger ones); a captured CUDA graph replays the same results."""
+one launch per (model, ROI size) with the lanes per ROI the plan chose (4, or 2 for large 7..10 px
+buckets, as the per-bucket launches' default); a captured CUDA graph replays the same results."""
 import numpy as np
 import pytest
 
@@ -34,7 +34,8 @@ def test_mixed_launch_equals_plain_launches(ctx, tile):
     mb = MixedBatch(buckets, tile_rois=tile).run()
     torch.cuda.synchronize()
     fused = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
-    mb.run_plain(lanes=None)
+    assert mb.lanes() == [4] * len(buckets)  # 3000 ROIs: no bucket is large enough for 2 lanes
+    mb.run_plain()
     torch.cuda.synchronize()
     for f, p in zip(fused, mb.results()):
         for k in f:
@@ -42,10 +43,41 @@ def test_mixed_launch_equals_plain_launches(ctx, tile):
     mb.close()
 
 
-def test_mixed_launch_close_to_four_lane_launches(ctx):
-    """With 4 lanes per ROI for every bucket the per-bucket launches sum the pixels of the 7 and
-    9 px buckets in another order: the fits agree to within float rounding on the ROIs both
-    sides converge on, and the estimators' settings are restored."""
+def test_large_small_roi_buckets_run_two_lanes(ctx):
+    """A 9 px bucket of 200k ROIs runs 2 lanes per ROI (two groups per 4-lane slot) beside a
+    4-lane 16 px bucket: its results equal the per-bucket launch at the estimator's default
+    configuration (2 lanes per ROI) bit for bit."""
+    import torch
+    import photonpy_b200 as pb
+    from photonpy_b200 import synth
+    from photonpy_b200.mixed import MixedBatch
+    synth.use_torch("cuda", 41)
+    small = synth.xyibg(200_000, seed=41, R=9, xy=(3.0, 5.0))
+    big = synth.sigmaxy(3000, seed=42)
+    synth.use_torch(None, 0)
+    G = pb.GaussianPSFMethods(ctx)
+    e1 = G.CreatePSF_XYIBg(9, small["sigma"], True)
+    e2 = G.CreatePSF_XYIBgSigmaXY(16, big["sigma"], True)
+    buckets = [(e1, torch.from_numpy(small["samples"]).cuda()), (e2, torch.from_numpy(big["samples"]).cuda())]
+    mb = MixedBatch(buckets, tile_rois=1).run()
+    torch.cuda.synchronize()
+    assert mb.lanes() == [2, 4]
+    assert e1.GetKernelConfig()[0] == 2
+    fused = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
+    for lanes in ("plan", None):
+        mb.run_plain(lanes=lanes)
+        torch.cuda.synchronize()
+        for f, p in zip(fused, mb.results()):
+            for k in f:
+                assert torch.equal(f[k], p[k]), (lanes, k)
+    mb.close()
+
+
+def test_mixed_launch_close_to_default_config_launches(ctx):
+    """With each estimator's own configuration (2 lanes per ROI for the 7 and 9 px buckets) the
+    per-bucket launches sum those buckets' pixels in another order than the plan's 4 lanes: the
+    fits agree to within float rounding on the ROIs both sides converge on, and the estimators'
+    settings are restored."""
     import torch
     from photonpy_b200.mixed import MixedBatch
     buckets = _buckets(ctx, n=3000, seed=7)
@@ -54,11 +86,12 @@ def test_mixed_launch_close_to_four_lane_launches(ctx):
     mb = MixedBatch(buckets, tile_rois=1).run()
     torch.cuda.synchronize()
     fused = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
-    mb.run_plain(lanes=None)
+    mb.run_plain(lanes=4)
     torch.cuda.synchronize()
     assert [b[0].GetKernelConfig() for b in buckets] == before
-    mb.run_plain(lanes=4)
+    mb.run_plain()
     assert [b[0].GetKernelConfig() for b in buckets] == before
+    mb.run_plain(lanes=None)
     torch.cuda.synchronize()
     for f, p in zip(fused, mb.results()):
         conv = ((f["iterations"] < 50) & (p["iterations"] < 50)).cpu().numpy()
