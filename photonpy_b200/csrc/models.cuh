@@ -678,10 +678,10 @@ struct SplineModelT {
     static __host__ __device__ constexpr int table_floats(int) { return 256; }
 
     float tx, ty, tI, tbg, du;
-    float q;  // voxels per ROI pixel (1: the reference's model)
+    float vq;  // voxels per ROI pixel (1: the reference's model)
 
-    // pixel index c in spline-grid units before the centre offset: q c (c itself without OVS)
-    __device__ __forceinline__ float gridc(int c) const { return OVS ? MUL((float)c, q) : (float)c; }
+    // pixel index c in spline-grid units before the centre offset: vq c (c itself without OVS)
+    __device__ __forceinline__ float gridc(int c) const { return OVS ? MUL((float)c, vq) : (float)c; }
     float spx, spy, spz;
     float bgx, bgy, halfw;
     const float* img;  // MODE 2: this spot's background image [R][R]
@@ -693,15 +693,15 @@ struct SplineModelT {
         Ny = d.spline_shape[1];
         Nx = d.spline_shape[2];
         du = DIV(SUB(d.spline_zmax, d.spline_zmin), (float)Nz);
-        q = OVS ? d.spline_q : 1.0f;
+        vq = OVS ? d.spline_q : 1.0f;
         if (MODE == 2) {
             const float w = (float)d.roisize;
             tx = ADD(ADD(SUB(th[0], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Nx), 1.0f), 2.0f)), 0.5f);
             ty = ADD(ADD(SUB(th[1], DIV(w, 2.0f)), DIV(ADD(SUB(w, (float)Ny), 1.0f), 2.0f)), 0.5f);
         } else {
-            // grid coordinate of pixel x: q x - tx (q = 1: x - (theta_x - Nx/2), the reference)
-            tx = SUB(OVS ? MUL(th[0], q) : th[0], MUL((float)Nx, 0.5f));
-            ty = SUB(OVS ? MUL(th[1], q) : th[1], MUL((float)Ny, 0.5f));
+            // grid coordinate of pixel x: vq x - tx (vq = 1: x - (theta_x - Nx/2), the reference)
+            tx = SUB(OVS ? MUL(th[0], vq) : th[0], MUL((float)Nx, 0.5f));
+            ty = SUB(OVS ? MUL(th[1], vq) : th[1], MUL((float)Ny, 0.5f));
         }
         tI = th[3];
         tbg = th[4];
@@ -765,8 +765,8 @@ struct SplineModelT {
             dy = ADD(ADD(ADD(ADD(dy, MUL(e.x, c.x)), MUL(e.y, c.y)), MUL(e.z, c.z)), MUL(e.w, c.w));
             dz = ADD(ADD(ADD(ADD(dz, MUL(g.x, c.x)), MUL(g.y, c.y)), MUL(g.z, c.z)), MUL(g.w, c.w));
         }
-        dx = MUL(dx, OVS ? -MUL(tI, q) : -tI);
-        dy = MUL(dy, OVS ? -MUL(tI, q) : -tI);
+        dx = MUL(dx, OVS ? -MUL(tI, vq) : -tI);
+        dy = MUL(dy, OVS ? -MUL(tI, vq) : -tI);
         dz = MUL(dz, DIV(tI, du));
         if (psf < 0.0f) psf = 0.0f;
         J[0] = dx;
@@ -823,7 +823,7 @@ struct SplineModelT {
             }
         }
         const float zs = DIV(tI, du);
-        const float xs = OVS ? -MUL(tI, q) : -tI;
+        const float xs = OVS ? -MUL(tI, vq) : -tI;
 #pragma unroll
         for (int t = 0; t < PB; t++) {
             float p = psf[t];
