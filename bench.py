@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per ROI (0 = library default)")
+    ap.add_argument("--standalone-min", type=int, default=None, dest="standalone_min",
+                    help="mixed workload: ROIs per SM from which a bucket runs as launches of its own "
+                         "(default: the library's)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library default)")
     ap.add_argument("--variant", type=int, default=None, help="Gaussian kernel family (0 column-blocked, 1 generic)")
     ap.add_argument("--xy-step", type=float, default=1.0, dest="xy_step",
@@ -408,13 +411,14 @@ def mixed_estimator(pb, ctx, g):
 
 
 def run_mixed(args):
-    """Mixed workload: persistent graph-replayed launches (fused) vs one launch per (model, ROI
-    size) bucket (plain), device-resident inputs; claim size and register budget picked by the
-    autotuner unless --tile is given; CPU and reference-GPU baselines."""
+    """Mixed workload: one graph-replayed MixedBatch run (buckets as launches of their own on
+    forked streams, or in the persistent mixed kernel, as the autotuner picks unless --tile is
+    given) vs one launch per (model, ROI size) bucket in sequence on one stream (plain),
+    device-resident inputs; CPU and reference-GPU baselines."""
     import torch
     import photonpy_b200 as pb
     from photonpy_b200 import roofline, synth
-    from photonpy_b200.mixed import MixedBatch
+    from photonpy_b200.mixed import MixedBatch, set_standalone_min, standalone_min
     w = WORKLOADS["mixed"]
     n = args.n or w["n"]
     synth.use_torch("cuda", 5)
@@ -422,12 +426,16 @@ def run_mixed(args):
     ctx = pb.Context()
     ests = [mixed_estimator(pb, ctx, g) for g in groups]
     xs = [torch.from_numpy(g["samples"]).cuda() for g in groups]
+    if args.standalone_min is not None:
+        set_standalone_min(args.standalone_min)
     tuned = None
     tile, threads = args.tile, args.threads or 256
     if tile <= 0:
         from photonpy_b200.autotune import tune_mixed
-        tuned = tune_mixed(list(zip(ests, xs)))
+        tuned = tune_mixed(list(zip(ests, xs)), standalone_mins=(0, None) if args.standalone_min is None
+                           else (args.standalone_min,))
         tile, threads = tuned["tile"], tuned["threads"]
+        set_standalone_min(tuned["standalone_min"])
     mb = MixedBatch(list(zip(ests, xs)), tile_rois=tile, threads=threads)
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
@@ -495,6 +503,8 @@ def run_mixed(args):
         config=dict(workload=w["desc"], rois=n, buckets=len(groups), tile_rois=tile, threads_per_block=threads,
                     autotuned=(tuned["timings"] if tuned else None),
                     lanes_per_roi=dict(zip([f"{g['kind']}_{g['R']}" for g in groups], mb.lanes())),
+                    standalone_min_rois_per_sm=standalone_min(),
+                    standalone_buckets=[f"{g['kind']}_{g['R']}" for g, a in zip(groups, mb.standalone()) if a],
                     graph_replay=True, lm_iterations=MAX_IT, lm_lambda=LAMBDA,
                     l2="inputs of %.2f GB per step exceed the 126 MB L2" % (sum(x.numel() for x in xs) * 4 / 1e9)),
         plain_gpu=dict(value=n / (ms_plain * 1e-3), ms_per_step=ms_plain, launches_per_step=plain_launches,

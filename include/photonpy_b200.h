@@ -412,19 +412,31 @@ int PB200_MixedPlanInfo(MixedPlan* plan, int* ntasks, int* totalTiles, int* stri
  * per-bucket launches do by default). Per-bucket launches with these lanes per ROI give the
  * plan's results bit for bit. Returns 0, or -1 on a bad argument. */
 int PB200_MixedPlanLanes(MixedPlan* plan, int nbuckets, int* lanes);
+/* No counterpart in the reference. standalone[b] = 1 for each bucket that runs as launches of
+ * its own (the single-model LM, Fisher and CRLB launches at the default configuration, on a stream
+ * forked from the run's stream, because it holds at least PB200_GetMixedStandaloneMin() ROIs per
+ * SM), 0 for those fitted inside the persistent mixed kernel.
+ * Returns 0, or -1 on a bad argument. */
+int PB200_MixedPlanStandalone(MixedPlan* plan, int nbuckets, int* standalone);
+/* No counterpart in the reference. ROIs per SM from which a bucket of the mixed plans created
+ * afterwards runs as launches of its own (default 0: every bucket; a negative value restores it, a
+ * value above any bucket size keeps every bucket in the persistent kernel). Process-wide. */
+void PB200_SetMixedStandaloneMin(int roisPerSM);
+int PB200_GetMixedStandaloneMin(void);
 void PB200_MixedPlanDestroy(MixedPlan* plan);
 /* No counterpart in the reference. Fit + CRLB + chi-square in one call like PB200_EstimateDevice,
  * for callers that must not allocate device memory during a fit (real-time acquisition loops
  * with all device memory reserved in advance, hosts whose memory must come from their own
- * pools): it calls no cudaMalloc/cudaFree or other allocating routine. Its only scratch, the
- * packed Fisher rows, lives in a fixed device array of 32768 spots x 22 floats (2.75 MiB per
- * GPU that loads the library, kept until exit), so numspots above 32768 is rejected with an
+ * pools): it calls no cudaMalloc/cudaFree or other allocating routine. Its scratch, the
+ * packed Fisher rows and the ROI counter of the LM launch (zeroed with cudaMemsetAsync), lives in
+ * fixed device arrays of 32768 spots x 22 floats (2.75 MiB per GPU that loads the library, kept
+ * until exit) and 4 ints, so numspots above 32768 is rejected with an
  * error (split the batch), and so is an estimator of more than 6 parameters (the tilted-
  * background SigmaXY Gaussian, the spline tilted-background mode), whose Fisher rows do not
  * fit a 22-float row; such calls launch nothing. All pointers are device memory; d_crlb is required, d_iterations and
- * d_chisq may be NULL. The first call on a device looks up the array's device address; make
- * that first call before any stream capture. Every call shares the array and overwrites the
- * rows it uses, so calls whose kernels overlap on the GPU (other streams, other threads) race:
+ * d_chisq may be NULL. The first call on a device looks up the arrays' device addresses; make
+ * that first call before any stream capture. Every call shares the arrays and overwrites the
+ * rows and the counter it uses, so calls whose kernels overlap on the GPU (other streams, other threads) race:
  * serialise them. Returns 0 on success, -1 on error (message in PB200_GetLastError). */
 int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample, const float* d_constants,
                               const float* d_initial, float* d_params, int* d_iterations, float* d_crlb,

@@ -150,31 +150,53 @@ def tune_estimator(est, samples=None, constants=None, n=65536, reps=3, use_cache
     return dict(config=(v, g, t), ms=ms, timings={str(k): ms_ for k, ms_ in timings.items()}, cached=False)
 
 
-def tune_mixed(buckets, tiles=(1, 2, 4, 8), budgets=(256, 129, 128), reps=3):
-    """Time MixedBatch tile sizes and register budgets for these buckets; returns
-    dict(tile=..., threads=..., ms=..., timings={...}) (the caller builds its MixedBatch with them)."""
+def tune_mixed(buckets, tiles=(1, 2, 4, 8), budgets=(256, 129, 128), reps=3, standalone_mins=(0, None)):
+    """Time MixedBatch configurations for these buckets: for each threshold of standalone_mins
+    (ROIs per SM from which a bucket runs as launches of its own; None = every bucket in the
+    persistent mixed kernel), the persistent kernel's claim sizes and register budgets when it
+    has buckets. Returns dict(standalone_min=..., tile=..., threads=..., ms=..., timings={...});
+    the caller calls mixed.set_standalone_min(standalone_min) and builds its MixedBatch with
+    tile and threads. The process-wide threshold is restored before returning."""
     import torch
-    from .mixed import MixedBatch
+    from .mixed import MixedBatch, set_standalone_min, standalone_min
+    never = 1 << 30
+    saved = standalone_min()
     s = torch.cuda.Stream()
     timings = {}
-    with torch.cuda.stream(s):
-        for thr in budgets:
-            for tile in tiles:
-                mb = MixedBatch(buckets, tile_rois=tile, threads=thr)
-                try:
-                    mb.run(s)
-                    s.synchronize()
-                    mb.capture(s)
-                    for _ in range(2):
-                        mb.run(s)
-                    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
-                    e0.record(s)
-                    for _ in range(reps):
-                        mb.run(s)
-                    e1.record(s)
-                    e1.synchronize()
-                    timings[(tile, thr)] = e0.elapsed_time(e1) / reps
-                finally:
-                    mb.close()
-    (tile, thr), ms = choose_best(timings)
-    return dict(tile=tile, threads=thr, ms=ms, timings={str(k): v for k, v in timings.items()})
+    try:
+        with torch.cuda.stream(s):
+            for smin in standalone_mins:
+                set_standalone_min(never if smin is None else smin)
+                for thr in budgets:
+                    for tile in tiles:
+                        mb = MixedBatch(buckets, tile_rois=tile, threads=thr)
+                        all_alone = all(mb.standalone())
+                        try:
+                            _time_mixed(mb, s, reps, timings, (smin, tile, thr))
+                        finally:
+                            mb.close()
+                        if all_alone:  # no bucket in the persistent kernel: tile and budget do not matter
+                            break
+                    if all_alone:
+                        break
+    finally:
+        set_standalone_min(saved)
+    (smin, tile, thr), ms = choose_best(timings)
+    return dict(standalone_min=never if smin is None else smin, tile=tile, threads=thr, ms=ms,
+                timings={str(k): v for k, v in timings.items()})
+
+
+def _time_mixed(mb, s, reps, timings, key):
+    import torch
+    mb.run(s)
+    s.synchronize()
+    mb.capture(s)
+    for _ in range(2):
+        mb.run(s)
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    e0.record(s)
+    for _ in range(reps):
+        mb.run(s)
+    e1.record(s)
+    e1.synchronize()
+    timings[key] = e0.elapsed_time(e1) / reps

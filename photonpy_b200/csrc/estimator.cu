@@ -181,6 +181,14 @@ int default_lanes(int model, int R) {
     return 16;
 }
 
+// Lanes per ROI and columns per lane of the column-blocked kernel at its default configuration
+// (a flat-background Gaussian; the shape Estimator::fit_shape gives without a configuration).
+void gauss_default_shape(int model, int R, int& G, int& cpl) {
+    G = default_lanes(model, R);
+    while (G < 32 && (R + G - 1) / G > gauss_max_cpl(G)) G *= 2;
+    cpl = (R + G - 1) / G;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------
@@ -227,6 +235,7 @@ void set_last_error(const std::string& msg) {
 struct Slot {
     cudaStream_t stream = nullptr;
     DevBuf smp, consts, initial, params, iters, trace, crlb, chisq, fisher, glrt;
+    DevBuf claim;  // ROI counter of the slot's LM launches
 };
 
 struct Estimator {
@@ -519,6 +528,8 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         a.lambda = e->lm.lambda;
         a.flags = flags;
         a.fisher = (h_crlb || h_fisher) ? s.fisher.as<float>() : nullptr;
+        s.claim.ensure(sizeof(int));
+        a.claim = s.claim.as<int>();
         if (wantGlrt) {
             s.glrt.ensure(sizeof(float) * 3 * count);
             a.glrt = s.glrt.as<float>();
@@ -782,9 +793,10 @@ Estimator* make_spline(int roisize, const CSpline_Calibration* calib, const floa
     return e;
 }
 
-// Device-pointer fit on a caller stream. With a CRLB request the packed Fisher rows go to a
-// stream-ordered scratch allocation (cudaMallocAsync), which is freed on the same stream after
-// crlb_kernel has consumed it; concurrent calls on different streams therefore never share it.
+// Device-pointer fit on a caller stream. The LM launch's ROI counter and, with a CRLB request,
+// the packed Fisher rows go to a stream-ordered scratch allocation (cudaMallocAsync), which is
+// freed on the same stream after the last launch has used it; concurrent calls on different
+// streams therefore never share it.
 // Keep freed stream-ordered allocations in the device's default pool instead of returning them
 // to the driver at every synchronisation (repeated calls would otherwise remap memory each time).
 void keep_pool_memory() {
@@ -800,23 +812,21 @@ void keep_pool_memory() {
 }
 
 void run_fit_device(Estimator* e, FitArgs a, cudaStream_t s) {
-    if (a.crlb) {
-        keep_pool_memory();
-        void* scratch = nullptr;
-        const size_t bytes = sizeof(float) * fisher_row_floats(e->K) * (size_t)a.n;
-        PB_CUDA(cudaMallocAsync(&scratch, bytes, s));
-        a.fisher = static_cast<float*>(scratch);
-        try {
-            launch_fit_fisher(e, a, s);
-            launch_crlb(e->K, a.fisher, a.crlb, a.chisq, a.n, s, e->crlbAbs);
-        } catch (...) {
-            cudaFreeAsync(scratch, s);
-            throw;
-        }
-        PB_CUDA(cudaFreeAsync(scratch, s));
-    } else {
+    keep_pool_memory();
+    constexpr size_t kHead = 256;  // the counter, padded so that the Fisher rows start aligned
+    const size_t bytes = kHead + (a.crlb ? sizeof(float) * fisher_row_floats(e->K) * (size_t)a.n : 0);
+    void* scratch = nullptr;
+    PB_CUDA(cudaMallocAsync(&scratch, bytes, s));
+    a.claim = static_cast<int*>(scratch);
+    if (a.crlb) a.fisher = reinterpret_cast<float*>(static_cast<char*>(scratch) + kHead);
+    try {
         launch_fit_fisher(e, a, s);
+        if (a.crlb) launch_crlb(e->K, a.fisher, a.crlb, a.chisq, a.n, s, e->crlbAbs);
+    } catch (...) {
+        cudaFreeAsync(scratch, s);
+        throw;
     }
+    PB_CUDA(cudaFreeAsync(scratch, s));
 }
 
 void check_estimator(Estimator* e) {
@@ -1340,31 +1350,60 @@ int PB200_SplineCoefGradient(Estimator* e, int numspots, const float* d_sample, 
 #ifndef PB200_MIXED_TWO_LANES
 #define PB200_MIXED_TWO_LANES 1
 #endif
+// ROIs per SM from which a bucket of a mixed plan runs as launches of its own (the single-model
+// kernels at their default configuration, on a stream of its own) instead of inside the
+// persistent mixed kernel. The single-model kernels fit a ROI faster than the mixed kernel,
+// which carries every model's handler in one register budget, and launches on several streams
+// share the GPU, so that the small buckets fill it together: on a B200 a 12-bucket batch ran
+// 1.03x (4M ROIs) to 1.7x (40k ROIs) faster with every bucket alone than in the persistent
+// kernel. Default 0 (every bucket); PB200_SetMixedStandaloneMin changes it for the plans created
+// afterwards.
+std::atomic<int> g_aloneMinRoisPerSM{0};
 // ROIs per SM from which a 7..10 px bucket of a mixed plan runs 2 lanes per ROI (about 4 per
 // resident 2-lane group at 2 blocks of 256 threads per SM)
 constexpr int kTwoLaneMinRoisPerSM = 1024;
 
+// A bucket of a mixed plan that runs as launches of its own: the LM and Fisher launches of the
+// single-model kernel, then the FP64 CRLB.
+struct MixedAlone {
+    FitLaunch launch = nullptr;
+    ModelDesc d{};
+    FitArgs a{};  // a.fisher: the plan's Fisher rows; a.claim: the plan's counter of this bucket
+    int threads = 0, K = 0;
+};
+
 struct MixedPlan {
     int device = 0;
     int ntasks = 0, totalTiles = 0, tileRois = 32, variant = 0, strideFloats = 0;
-    std::vector<MixedTask> tasks;
+    std::vector<MixedTask> tasks;  // the buckets of the persistent mixed kernel
     std::vector<int> K;
     std::vector<int> twoLane;      // per task: it runs 2 lanes per ROI
     std::vector<int> bucketLanes;  // per bucket as passed in: lanes per ROI of its launches
+    std::vector<MixedAlone> alone;  // the buckets that run as launches of their own
+    std::vector<int> bucketAlone;   // per bucket as passed in: 1 if it runs as launches of its own
     DevBuf dTasks, dTasksFisher, dCounter, dFisher;  // dCounter: per-bucket ROI counters of the two passes
+    DevBuf dAloneClaims;
+    // one stream per bucket that runs alone, forked from the caller's stream and joined back
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> sideDone;
+    cudaEvent_t fork = nullptr;
     bool anyFisher = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
     ~MixedPlan() {
         if (graphExec) cudaGraphExecDestroy(graphExec);
         if (graph) cudaGraphDestroy(graph);
+        for (cudaStream_t st : side) cudaStreamDestroy(st);
+        for (cudaEvent_t ev : sideDone) cudaEventDestroy(ev);
+        if (fork) cudaEventDestroy(fork);
     }
 };
 
 namespace {
-// The LM pass over every bucket, then the Fisher pass at the fitted parameters (buckets without
-// a CRLB request have no ROIs in it), then the FP64 CRLB of each bucket.
-void mixed_enqueue(MixedPlan* p, cudaStream_t s) {
+// The persistent mixed kernel's buckets: the LM pass over every bucket, the Fisher pass at the
+// fitted parameters (buckets without a CRLB request have no ROIs in it), then the FP64 CRLB of
+// each bucket.
+void mixed_enqueue_kernel(MixedPlan* p, cudaStream_t s) {
     PB_CUDA(cudaMemsetAsync(p->dCounter.p, 0, 2 * sizeof(int) * p->ntasks, s));
     launch_mixed(p->dTasks.as<MixedTask>(), p->ntasks, p->totalTiles, p->tileRois, p->dCounter.as<int>(),
                  p->strideFloats, p->variant, false, s);
@@ -1384,6 +1423,25 @@ void mixed_enqueue(MixedPlan* p, cudaStream_t s) {
         const FitArgs& a = p->tasks[b].a;
         if (a.crlb) launch_crlb(p->K[b], a.fisher, a.crlb, a.chisq, a.n, s);
     }
+}
+
+// The launches of each bucket that runs alone on a stream of its own, forked from `s`, and on
+// `s` the persistent mixed kernel for the others; `s` then waits for the forked streams. The GPU
+// runs the launches side by side, so that one bucket's last ROIs share the SMs with another
+// bucket's ROIs instead of leaving them idle. In a stream capture the fork and join become graph
+// edges.
+void mixed_enqueue(MixedPlan* p, cudaStream_t s) {
+    if (!p->alone.empty()) PB_CUDA(cudaEventRecord(p->fork, s));
+    for (size_t i = 0; i < p->alone.size(); i++) {
+        const MixedAlone& m = p->alone[i];
+        const cudaStream_t si = p->side[i];
+        PB_CUDA(cudaStreamWaitEvent(si, p->fork, 0));
+        m.launch(m.d, m.a, m.threads, si);
+        if (m.a.crlb) launch_crlb(m.K, m.a.fisher, m.a.crlb, m.a.chisq, m.a.n, si);
+        PB_CUDA(cudaEventRecord(p->sideDone[i], si));
+    }
+    if (p->ntasks) mixed_enqueue_kernel(p, s);
+    for (size_t i = 0; i < p->alone.size(); i++) PB_CUDA(cudaStreamWaitEvent(s, p->sideDone[i], 0));
 }
 }  // namespace
 
@@ -1420,6 +1478,8 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                 }
                 p->dFisher.ensure(sizeof(float) * (fisherFloats ? fisherFloats : 1));
                 size_t off = 0;
+                std::vector<int> laneOf(nbuckets, G), aloneOf(nbuckets, 0);
+                const int aloneMin = g_aloneMinRoisPerSM.load();
                 for (int b = 0; b < nbuckets; b++) {
                     Estimator* e = ests[b];
                     if (counts[b] == 0) continue;
@@ -1440,6 +1500,20 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                         off += (size_t)fisher_row_floats(e->K) * counts[b];
                     }
                     const int R = e->desc.roisize;
+                    if ((long long)counts[b] >= (long long)aloneMin * num_sms()) {
+                        MixedAlone m;
+                        int Ga = 0, cpla = 0;
+                        gauss_default_shape(e->desc.model, R, Ga, cpla);
+                        m.launch = fit_launcher_for(e->desc.model, Ga, cpla, 0);
+                        m.d = e->desc;
+                        m.a = a;
+                        m.threads = Ga == 2 ? 128 : 256;
+                        m.K = e->K;
+                        p->alone.push_back(m);
+                        laneOf[b] = Ga;
+                        aloneOf[b] = 1;
+                        continue;
+                    }
                     const int cpl = (R + G - 1) / G;
                     t.handler = mixed_handler(e->desc.model, G, cpl);
                     p->totalTiles += (counts[b] + tileRois - 1) / tileRois;
@@ -1460,6 +1534,7 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     if (PB200_MIXED_TWO_LANES && R >= 7 && R <= 10 &&
                         (long long)counts[b] >= (long long)kTwoLaneMinRoisPerSM * num_sms()) {
                         p->twoLane.push_back(1);
+                        laneOf[b] = 2;
                         p->strideFloats = std::max(p->strideFloats,
                                                    2 * round_up(round_up(R * R, 4) + cmax(4 * R, rescue_floats(e->K)), 4));
                     } else {
@@ -1469,8 +1544,19 @@ MixedPlan* PB200_MixedPlanCreate(int nbuckets, Estimator* const* ests, const int
                     p->K.push_back(e->K);
                 }
                 p->ntasks = (int)p->tasks.size();
-                for (int b = 0, t = 0; b < nbuckets; b++)
-                    p->bucketLanes.push_back(counts[b] == 0 ? G : (p->twoLane[t++] ? 2 : G));
+                p->bucketLanes = laneOf;
+                p->bucketAlone = aloneOf;
+                p->dAloneClaims.ensure(sizeof(int) * std::max<size_t>(1, p->alone.size()));
+                for (size_t i = 0; i < p->alone.size(); i++) p->alone[i].a.claim = p->dAloneClaims.as<int>() + i;
+                if (!p->alone.empty()) PB_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
+                for (size_t i = 0; i < p->alone.size(); i++) {
+                    cudaStream_t st = nullptr;
+                    cudaEvent_t ev = nullptr;
+                    PB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                    p->side.push_back(st);
+                    PB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                    p->sideDone.push_back(ev);
+                }
                 bool anyTwo = false;
                 for (int b = 0; b < p->ntasks; b++) anyTwo = anyTwo || p->twoLane[b];
                 {
@@ -1530,12 +1616,20 @@ int PB200_MixedPlanRun(MixedPlan* p, void* stream) {
     return guarded(
         [&]() -> int {
             if (!p) throw Error("MixedPlanRun: null plan");
-            if (p->ntasks == 0) return 0;
+            if (p->ntasks == 0 && p->alone.empty()) return 0;
             const cudaStream_t s = (cudaStream_t)stream;
             if (p->graphExec) {
                 PB_CUDA(cudaGraphLaunch(p->graphExec, s));
-                // the graph holds the LM and Fisher passes and one CRLB kernel per bucket
-                count_launch();
+                // the graph holds the LM (+ Fisher and CRLB) launches of each bucket that runs
+                // alone, the LM and Fisher passes of the mixed kernel and one CRLB kernel per bucket
+                for (const MixedAlone& m : p->alone) {
+                    count_launch();
+                    if (m.a.crlb) {
+                        count_launch();
+                        count_launch();
+                    }
+                }
+                if (p->ntasks) count_launch();
                 if (p->anyFisher) count_launch();
                 for (int b = 0; b < p->ntasks; b++)
                     if (p->tasks[b].a.crlb) count_launch();
@@ -1551,7 +1645,7 @@ int PB200_MixedPlanCapture(MixedPlan* p, void* stream) {
     return guarded(
         [&]() -> int {
             if (!p) throw Error("MixedPlanCapture: null plan");
-            if (p->ntasks == 0) return 0;
+            if (p->ntasks == 0 && p->alone.empty()) return 0;
             const cudaStream_t s = (cudaStream_t)stream;
             if (!s) throw Error("MixedPlanCapture: needs a non-default stream");
             if (p->graphExec) {
@@ -1592,6 +1686,15 @@ int PB200_MixedPlanLanes(MixedPlan* p, int nbuckets, int* lanes) {
     return 0;
 }
 
+void PB200_SetMixedStandaloneMin(int roisPerSM) { g_aloneMinRoisPerSM.store(roisPerSM < 0 ? 0 : roisPerSM); }
+int PB200_GetMixedStandaloneMin(void) { return g_aloneMinRoisPerSM.load(); }
+
+int PB200_MixedPlanStandalone(MixedPlan* p, int nbuckets, int* standalone) {
+    if (!p || !standalone || nbuckets != (int)p->bucketAlone.size()) return -1;
+    for (int b = 0; b < nbuckets; b++) standalone[b] = p->bucketAlone[b];
+    return 0;
+}
+
 void PB200_MixedPlanDestroy(MixedPlan* p) { delete p; }
 
 // ---- allocation-free fused fit + CRLB ----
@@ -1599,7 +1702,8 @@ void PB200_MixedPlanDestroy(MixedPlan* p) { delete p; }
 // fits frames from a real-time loop with all of its device memory reserved up front (a
 // cudaMalloc or cudaFree there can stall until other streams finish, or fail half-way through
 // a run), and host frameworks whose memory may only come from their own pools. For them the
-// fused path keeps its one piece of scratch, the packed Fisher rows, in the fixed array below.
+// fused path keeps its scratch, the packed Fisher rows and the LM launch's ROI counter, in the
+// fixed arrays below.
 }  // extern "C"
 
 namespace {
@@ -1609,24 +1713,32 @@ constexpr int kNoAllocMaxSpots = 32768;
 constexpr int kNoAllocRowFloats = 22;
 // 32768 x 22 floats = 2.75 MiB, reserved on every GPU that loads this library until exit.
 static __device__ __align__(256) float g_noallocFisher[kNoAllocMaxSpots * kNoAllocRowFloats];
+// ROI counter of the LM launch (FitArgs::claim)
+static __device__ __align__(16) int g_noallocClaim[4];
 
-// Device address of g_noallocFisher on the current device. In host code the array's name is
-// only a host-side stand-in, so the real address is looked up once per device, with that
-// device current, and cached.
-float* noalloc_scratch() {
+// Device addresses of g_noallocFisher and g_noallocClaim on the current device. In host code the
+// arrays' names are only host-side stand-ins, so the real addresses are looked up once per
+// device, with that device current, and cached.
+struct NoAllocScratch {
+    float* fisher = nullptr;
+    int* claim = nullptr;
+};
+NoAllocScratch noalloc_scratch() {
     static std::mutex mtx;
-    static float* addr[64] = {nullptr};
+    static NoAllocScratch addr[64];
     int dev = 0;
     PB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw Error("PB200_EstimateCRLBNoAlloc: device index out of range");
     std::lock_guard<std::mutex> g(mtx);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t rc = cudaGetSymbolAddress(&p, g_noallocFisher);
+    if (!addr[dev].fisher) {
+        void *f = nullptr, *c = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress(&f, g_noallocFisher);
+        if (rc == cudaSuccess) rc = cudaGetSymbolAddress(&c, g_noallocClaim);
         if (rc != cudaSuccess)
             throw Error(std::string("PB200_EstimateCRLBNoAlloc: cudaGetSymbolAddress failed: ") +
                         cudaGetErrorString(rc));
-        addr[dev] = static_cast<float*>(p);
+        addr[dev].claim = static_cast<int*>(c);
+        addr[dev].fisher = static_cast<float*>(f);
     }
     return addr[dev];
 }
@@ -1647,7 +1759,7 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
             if (!d_sample || !d_params || !d_crlb) throw Error("PB200_EstimateCRLBNoAlloc: null sample/params/crlb");
             if (e->numconst && !d_constants) throw Error("this estimator needs per-spot constants");
             if (fisher_row_floats(e->K) > kNoAllocRowFloats) throw Error("PB200_EstimateCRLBNoAlloc: too many parameters");
-            float* scratch = noalloc_scratch();
+            const NoAllocScratch scratch = noalloc_scratch();
             FitArgs a{};
             a.smp = d_sample;
             a.consts = d_constants;
@@ -1656,14 +1768,15 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
             a.iterations = d_iterations;
             a.crlb = d_crlb;
             a.chisq = d_chisq;
-            a.fisher = scratch;
+            a.fisher = scratch.fisher;
+            a.claim = scratch.claim;
             a.n = numspots;
             a.maxIter = e->lm.iterations;
             a.lambda = e->lm.lambda;
             a.flags = 0;
             const cudaStream_t s = (cudaStream_t)stream;
             launch_fit_fisher(e, a, s);
-            launch_crlb(e->K, scratch, d_crlb, d_chisq, numspots, s, e->crlbAbs);
+            launch_crlb(e->K, scratch.fisher, d_crlb, d_chisq, numspots, s, e->crlbAbs);
             return 0;
         },
         -1);

@@ -59,6 +59,8 @@ struct FitArgs {
     float lambda;
     int smemStride;        // floats of shared memory per group
     int flags;
+    int* claim;            // null: group g fits ROIs g, g + groups, ...; else (LM launches) a counter, zeroed
+                           // by the launcher, from which each group takes its next ROI when it is done
 };
 
 __host__ __device__ constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
@@ -88,6 +90,14 @@ __device__ __forceinline__ float group_sum(float v, unsigned mask) {
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
     return v;
+}
+
+// First of `count` ROIs taken from a launch's counter by a group of G lanes (lane 0 takes them).
+template <int G>
+__device__ __forceinline__ int group_claim(int* counter, int count, int lane, unsigned mask) {
+    int r = 0;
+    if (lane == 0) r = atomicAdd(counter, count);
+    return __shfl_sync(mask, r, 0, G);
 }
 
 // 1/x for x >= 1e-8 (never denormal): approximate reciprocal + one Newton step, no branch.

@@ -445,8 +445,13 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
     const int lane = threadIdx.x & (G - 1);
     const int gib = threadIdx.x / G;
     const int gpb = blockDim.x / G;
-    gauss_fit_range<M, G, CPL, PASS>(d, a, blockIdx.x * gpb + gib, a.n, gridDim.x * gpb, sm + gib * a.smemStride, lane,
-                               group_mask<G>());
+    // LM launches with a counter: one ROI per claim, so groups (and the warps and blocks they
+    // share) run out of work within one ROI of each other instead of after a fixed list whose
+    // iteration counts differ. The Fisher pass costs the same for every ROI and keeps the fixed
+    // assignment.
+    int* claim = PASS == PASS_LM ? a.claim : nullptr;
+    gauss_fit_range<M, G, CPL, PASS>(d, a, claim ? 0 : blockIdx.x * gpb + gib, a.n, claim ? 1 : gridDim.x * gpb,
+                                     sm + gib * a.smemStride, lane, group_mask<G>(), claim);
 }
 
 }  // namespace pb200

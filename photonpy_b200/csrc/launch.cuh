@@ -33,6 +33,12 @@ inline void check_launch(const char* what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Zeroes the ROI counter of an LM launch (FitArgs::claim) on the launch's stream.
+inline void reset_claim(int* claim, cudaStream_t s) {
+    const cudaError_t e = cudaMemsetAsync(claim, 0, sizeof(int), s);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("ROI counter reset: ") + cudaGetErrorString(e));
+}
+
 // Opt the kernel in to more than 48 KB of dynamic shared memory. Set on every launch: the
 // attribute is per kernel and per device, and the call costs about a microsecond.
 template <class KernelT>
@@ -92,6 +98,7 @@ inline FitArgs fisher_pass_args(const FitArgs& a) {
     fi.trace = nullptr;
     fi.traceLen = 0;
     fi.diag = nullptr;
+    fi.claim = nullptr;
     return fi;
 }
 
@@ -104,6 +111,7 @@ void launch_fit_generic(const ModelDesc& d, FitArgs a, int threads, cudaStream_t
         launch_groups(fit_kernel<M, G, PASS_FISHER>, G, threads, stride, a.n, d, a, s);
         return;
     }
+    if (a.claim && !model_is_spline(M::kId)) reset_claim(a.claim, s);
     launch_groups(fit_kernel<M, G, PASS_LM>, G, threads, stride, a.n, d, lm_pass_args(a), s);
     if (a.crlb || a.glrt) launch_groups(fit_kernel<M, G, PASS_FISHER>, G, threads, stride, a.n, d, fisher_pass_args(a), s);
 }
@@ -177,6 +185,7 @@ void launch_fit_gauss(const ModelDesc& d, FitArgs a, int threads, cudaStream_t s
         launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, a, s);
         return;
     }
+    if (a.claim) reset_claim(a.claim, s);
     launch_groups(gauss_fit_kernel<M, G, CPL, PASS_LM>, G, threads, stride, a.n, d, lm_pass_args(a), s);
     if (a.crlb || a.glrt)
         launch_groups(gauss_fit_kernel<M, G, CPL, PASS_FISHER>, G, threads, stride, a.n, d, fisher_pass_args(a), s);

@@ -2,11 +2,13 @@
 
 photonpy fits one estimator — one model and one ROI size — per call (its EstimationQueue
 holds one estimator per queue, EstimationQueue.h:27-108). A ``MixedBatch`` binds several
-estimators with their device-resident ROIs; one ``run()`` fits all of them with two persistent
-launches (the LM pass, then the Fisher/CRLB pass) in which ROI groups claim ``tile_rois``
-consecutive ROIs at a time from per-bucket counters, and
-``capture()`` records that run into a CUDA graph for replay. ``run_plain()`` is the
-one-launch-per-bucket form of the same work, for comparison.
+estimators with their device-resident ROIs; one ``run()`` fits all of them: buckets of at
+least ``standalone_min()`` ROIs per SM with the single-model launches, each on a stream forked
+from the run's stream, and the others with two persistent launches (the LM pass, then the
+Fisher/CRLB pass) in which ROI groups claim ``tile_rois`` consecutive ROIs at a time from
+per-bucket counters; ``capture()`` records that run into a CUDA graph for replay.
+``run_plain()`` is the one-launch-per-bucket form of the same work, in sequence on one stream,
+for comparison.
 """
 from __future__ import annotations
 
@@ -28,6 +30,12 @@ def _bind(L):
     L.PB200_MixedPlanDestroy.argtypes = [vp]
     L.PB200_MixedPlanLanes.argtypes = [vp, ct.c_int, vp]
     L.PB200_MixedPlanLanes.restype = ct.c_int
+    L.PB200_MixedPlanStandalone.argtypes = [vp, ct.c_int, vp]
+    L.PB200_MixedPlanStandalone.restype = ct.c_int
+    L.PB200_SetMixedStandaloneMin.argtypes = [ct.c_int]
+    L.PB200_SetMixedStandaloneMin.restype = None
+    L.PB200_GetMixedStandaloneMin.argtypes = []
+    L.PB200_GetMixedStandaloneMin.restype = ct.c_int
     return L
 
 
@@ -36,6 +44,18 @@ def _ptr_array(tensors):
     for i, t in enumerate(tensors):
         arr[i] = None if t is None else t.data_ptr()
     return arr
+
+
+def set_standalone_min(rois_per_sm):
+    """ROIs per SM from which a bucket of the MixedBatch objects created afterwards runs as
+    launches of its own, on a stream forked from the run's stream (default 0: every bucket; None
+    restores it; a value above any bucket size keeps every bucket in the persistent kernel).
+    Process-wide."""
+    _bind(load_library()).PB200_SetMixedStandaloneMin(-1 if rois_per_sm is None else int(rois_per_sm))
+
+
+def standalone_min():
+    return int(_bind(load_library()).PB200_GetMixedStandaloneMin())
 
 
 class MixedBatch:
@@ -107,6 +127,14 @@ class MixedBatch:
         if self._L.PB200_MixedPlanLanes(self.plan, len(self.buckets), arr) != 0:
             check_error("MixedPlanLanes")
         return list(arr)
+
+    def standalone(self):
+        """Per bucket: True when it runs as launches of its own (the single-model kernels, at least
+        standalone_min() ROIs per SM), False when the persistent mixed kernel fits it."""
+        arr = (ct.c_int * len(self.buckets))()
+        if self._L.PB200_MixedPlanStandalone(self.plan, len(self.buckets), arr) != 0:
+            check_error("MixedPlanStandalone")
+        return [bool(v) for v in arr]
 
     def run_plain(self, stream=None, lanes="plan"):
         """The same work as single-model launches, bucket by bucket (LM, Fisher and CRLB

@@ -57,9 +57,18 @@ def test_tune_mixed_picks_a_candidate(ctx):
     from photonpy_b200.mixed import MixedBatch
     from test_gpu_mixed import _buckets
     buckets = _buckets(ctx, n=3000, seed=9)
+    from photonpy_b200.mixed import set_standalone_min, standalone_min
     r = tune_mixed(buckets, tiles=(1, 4), budgets=(256, 128), reps=1)
     assert r["tile"] in (1, 4) and r["threads"] in (256, 128) and r["ms"] > 0
-    mb = MixedBatch(buckets, tile_rois=r["tile"], threads=r["threads"]).run()
+    assert r["standalone_min"] in (0, 1 << 30)
+    assert standalone_min() == 0  # restored
+    # every threshold timed; the all-alone plan once, the persistent kernel at each tile and budget
+    assert len(r["timings"]) == 1 + 4
+    set_standalone_min(r["standalone_min"])
+    try:
+        mb = MixedBatch(buckets, tile_rois=r["tile"], threads=r["threads"]).run()
+    finally:
+        set_standalone_min(None)
     torch.cuda.synchronize()
     fused = [{k: v.clone() for k, v in x.items()} for x in mb.results()]
     mb.run_plain()

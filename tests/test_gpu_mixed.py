@@ -1,10 +1,23 @@
-"""One persistent launch over mixed PSF models and ROI sizes gives exactly the results of
-one launch per (model, ROI size) with the lanes per ROI the plan chose (4, or 2 for large 7..10 px
-buckets, as the per-bucket launches' default); a captured CUDA graph replays the same results."""
+"""A mixed batch over several PSF models and ROI sizes gives exactly the results of one launch
+per (model, ROI size) with the lanes per ROI the plan chose, whether its buckets run in the
+persistent mixed kernel (4 lanes, or 2 for large 7..10 px buckets), as launches of their own on
+forked streams (each estimator's default lanes), or split between the two; a captured CUDA graph
+replays the same results."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+NEVER = 1 << 30
+
+
+@pytest.fixture
+def persistent_kernel():
+    """Every bucket of the MixedBatch objects created in the test runs in the persistent kernel."""
+    from photonpy_b200.mixed import set_standalone_min
+    set_standalone_min(NEVER)
+    yield
+    set_standalone_min(None)
 
 
 def _buckets(ctx, n=3000, seed=5):
@@ -26,7 +39,7 @@ def _buckets(ctx, n=3000, seed=5):
 
 
 @pytest.mark.parametrize("tile", [1, 8, 97])
-def test_mixed_launch_equals_plain_launches(ctx, tile):
+def test_mixed_launch_equals_plain_launches(ctx, tile, persistent_kernel):
     import torch
     from photonpy_b200.mixed import MixedBatch
     buckets = _buckets(ctx)
@@ -43,7 +56,7 @@ def test_mixed_launch_equals_plain_launches(ctx, tile):
     mb.close()
 
 
-def test_large_small_roi_buckets_run_two_lanes(ctx):
+def test_large_small_roi_buckets_run_two_lanes(ctx, persistent_kernel):
     """A 9 px bucket of 200k ROIs runs 2 lanes per ROI (two groups per 4-lane slot) beside a
     4-lane 16 px bucket: its results equal the per-bucket launch at the estimator's default
     configuration (2 lanes per ROI) bit for bit."""
@@ -73,7 +86,7 @@ def test_large_small_roi_buckets_run_two_lanes(ctx):
     mb.close()
 
 
-def test_mixed_launch_close_to_default_config_launches(ctx):
+def test_mixed_launch_close_to_default_config_launches(ctx, persistent_kernel):
     """With each estimator's own configuration (2 lanes per ROI for the 7 and 9 px buckets) the
     per-bucket launches sum those buckets' pixels in another order than the plan's 4 lanes: the
     fits agree to within float rounding on the ROIs both sides converge on, and the estimators'
@@ -100,11 +113,25 @@ def test_mixed_launch_close_to_default_config_launches(ctx):
     mb.close()
 
 
-def test_mixed_graph_replay(ctx):
+@pytest.mark.parametrize("standalone_min", [NEVER, 0, 2])
+def test_mixed_graph_replay(ctx, standalone_min):
+    """Graph replay of the persistent kernel, of forked per-bucket launches (threshold 0) and of a
+    plan split between the two (threshold 2 ROIs per SM: the larger buckets alone)."""
     import torch
-    from photonpy_b200.mixed import MixedBatch
+    from photonpy_b200.mixed import MixedBatch, set_standalone_min
     buckets = _buckets(ctx, n=2000, seed=6)
-    mb = MixedBatch(buckets, tile_rois=32).run()
+    set_standalone_min(standalone_min)
+    try:
+        mb = MixedBatch(buckets, tile_rois=32).run()
+    finally:
+        set_standalone_min(None)
+    alone = mb.standalone()
+    if standalone_min == NEVER:
+        assert not any(alone)
+    elif standalone_min == 0:
+        assert all(alone)
+    else:
+        assert any(alone) and not all(alone)
     torch.cuda.synchronize()
     ref = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
     for r in mb.results():
@@ -117,6 +144,38 @@ def test_mixed_graph_replay(ctx):
         mb.run(s)
     s.synchronize()
     for f, p in zip(ref, mb.results()):
+        for k in f:
+            assert torch.equal(f[k], p[k]), k
+    mb.close()
+
+
+@pytest.mark.parametrize("standalone_min", [0, 2])
+def test_standalone_buckets_equal_plain_launches(ctx, standalone_min):
+    """Buckets run as launches of their own on forked streams (all of them, or the larger ones
+    beside the persistent kernel for the others) give the per-bucket launches' results bit for
+    bit, at each estimator's default lanes per ROI (2 for the 7 and 9 px buckets)."""
+    import torch
+    from photonpy_b200.mixed import MixedBatch, set_standalone_min
+    buckets = _buckets(ctx, n=3000, seed=8)
+    set_standalone_min(standalone_min)
+    try:
+        mb = MixedBatch(buckets, tile_rois=1).run()
+    finally:
+        set_standalone_min(None)
+    torch.cuda.synchronize()
+    alone = mb.standalone()
+    assert any(alone)
+    defaults = [b[0].GetKernelConfig()[0] for b in buckets]
+    lanes = mb.lanes()
+    for a, l, dflt in zip(alone, lanes, defaults):
+        assert l == (dflt if a else 4)
+    fused = [{k: v.clone() for k, v in r.items()} for r in mb.results()]
+    for r in mb.results():
+        for v in r.values():
+            v.zero_()
+    mb.run_plain()
+    torch.cuda.synchronize()
+    for f, p in zip(fused, mb.results()):
         for k in f:
             assert torch.equal(f[k], p[k]), k
     mb.close()
