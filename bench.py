@@ -821,6 +821,25 @@ def main():
         d2h = n * (4 * K * 2 + 8)
         e2e = dict(value=world * n / float(et.item()), unit=UNIT, h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                    ms_per_step=1e3 * float(et.item()), api="PB200_EstimateCRLB (C ABI, pinned host buffers)")
+        # The host-to-device copy of the step's ROIs alone (one copy of the same pinned buffer,
+        # CUDA events): with the fits overlapping the copies, an end-to-end step cannot be
+        # shorter than the longer of this copy and the device-resident step.
+        d_copy = torch.empty(h_smp.shape, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            d_copy.copy_(h_smp, non_blocking=True)
+        torch.cuda.synchronize()
+        ev4, ev5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev4.record()
+        for _ in range(3):
+            d_copy.copy_(h_smp, non_blocking=True)
+        ev5.record()
+        ev5.synchronize()
+        copy_ms = ev4.elapsed_time(ev5) / 3
+        del d_copy
+        bound_ms = max(copy_ms, ms)
+        e2e["bound"] = dict(h2d_copy_ms=copy_ms, h2d_gbs=h2d / (copy_ms * 1e-3) / 1e9, device_step_ms=ms,
+                            bound_ms=bound_ms, frac=bound_ms / e2e["ms_per_step"],
+                            what="max(host-to-device copy of the ROIs alone, device-resident step) / e2e step")
         # results through the host path equal the device path
         assert np.array_equal(h_par.numpy(), out["params"].cpu().numpy())
 

@@ -64,3 +64,18 @@ def test_struct_layouts_match_reference_ctypes():
     from photonpy_b200 import spotdetect
     assert ctypes.sizeof(spotdetect.SpotDetector) == 32
     assert spotdetect.SpotDetector.backgroundImagePtr.offset == 24
+
+
+def test_mixed_standalone_threshold_setting():
+    """The mixed plans' standalone threshold is host state: set, read back, restored by a
+    negative value (no GPU call)."""
+    from photonpy_b200 import mixed
+    assert mixed.standalone_min() == 0
+    try:
+        mixed.set_standalone_min(1 << 30)
+        assert mixed.standalone_min() == 1 << 30
+        mixed.set_standalone_min(256)
+        assert mixed.standalone_min() == 256
+    finally:
+        mixed.set_standalone_min(None)
+    assert mixed.standalone_min() == 0
