@@ -236,6 +236,9 @@ struct Slot {
     cudaStream_t stream = nullptr;
     DevBuf smp, consts, initial, params, iters, trace, crlb, chisq, fisher, glrt;
     DevBuf claim;  // ROI counter of the slot's LM launches
+    // copied: the slot's inputs have arrived (recorded on the copy stream); freed: its launches
+    // have read them, so the copy stream may refill them (recorded on the slot's stream)
+    cudaEvent_t copied = nullptr, freed = nullptr;
 };
 
 struct Estimator {
@@ -260,11 +263,16 @@ struct Estimator {
     static constexpr int kMaxSlots = 8;
     int hostSlots = 4;
     Slot slots[kMaxSlots];
+    cudaStream_t copyStream = nullptr;  // the pipeline's host-to-device copies, in chunk order
 
     Estimator() { PB_CUDA(cudaGetDevice(&device)); }
     ~Estimator() {
-        for (auto& s : slots)
+        for (auto& s : slots) {
             if (s.stream) cudaStreamDestroy(s.stream);
+            if (s.copied) cudaEventDestroy(s.copied);
+            if (s.freed) cudaEventDestroy(s.freed);
+        }
+        if (copyStream) cudaStreamDestroy(copyStream);
     }
     int lanes_for() const { return lanes ? lanes : default_lanes(desc.model, desc.roisize); }
     // Lanes per ROI and columns per lane of the fit kernel this configuration launches (cpl 0:
@@ -332,8 +340,15 @@ struct Estimator {
     }
     int npix() const { return desc.roisize * desc.roisize; }
     Slot& slot(int i) {
-        if (!slots[i].stream) PB_CUDA(cudaStreamCreateWithFlags(&slots[i].stream, cudaStreamNonBlocking));
-        return slots[i];
+        Slot& s = slots[i];
+        if (!s.stream) PB_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        if (!s.copied) PB_CUDA(cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming));
+        if (!s.freed) PB_CUDA(cudaEventCreateWithFlags(&s.freed, cudaEventDisableTiming));
+        return s;
+    }
+    cudaStream_t copy_stream() {
+        if (!copyStream) PB_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+        return copyStream;
     }
 };
 
@@ -420,8 +435,13 @@ struct Chunking {
 // more from HBM.
 void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) { e->fit_launch()(e->desc, a, e->threads_for(), s); }
 
-// Host-pointer fit through the slot pipeline: H2D(c) + kernel(c) on slot c % slots are issued
-// before D2H(c - slots + 1), so the copies of one chunk overlap the fits of the others.
+// Host-pointer fit through the slot pipeline. The host-to-device copies of all chunks go, in
+// chunk order, to one copy stream, so that the copy engines deliver the chunk needed next at
+// full bandwidth instead of sharing it with the copies of later chunks (with a copy stream per
+// slot the end-to-end time of 1M 16x16 ROIs varied between 25.5 and 28.6 ms from one chunking
+// to the next). Chunk c's launches and result copies run on the stream of slot c % slots after
+// its inputs have arrived; the copy stream refills a slot once that slot's launches have read
+// their inputs.
 // h_fisher (with FIT_CRLB_ONLY): the packed FP32 Fisher rows [n][K(K+1)/2 + 1] themselves are
 // copied out instead of (or besides) being inverted.
 void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, const float* h_initial,
@@ -436,13 +456,17 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         e->glrtRoi0.ensure(sizeof(float) * npix);
         PB_CUDA(cudaMemcpy(e->glrtRoi0.p, h_smp, sizeof(float) * npix, cudaMemcpyHostToDevice));
     }
-    // Chunks of at most 64 MB of samples (at least 16384 ROIs, an eighth of the call when that is
-    // smaller); the first three are 1/8, 1/4 and 1/2 of that, so the first fit starts early.
+    // Chunks of at most 128 MB of samples (at least 16384 ROIs, an eighth of the call when that is
+    // smaller); the first three are 1/8, 1/4 and 1/2 of that, so the first fit starts early. Every
+    // chunk boundary costs the end of a fit launch, whose last ROIs leave most of the GPU idle
+    // (about 0.18 ms for 16x16 SigmaXY ROIs, even with the next chunk's launch on another
+    // stream): 1M such ROIs took 26.1 ms end to end in chunks of 64 MB, 25.5 ms in chunks of
+    // 128 MB, 26.9 ms in chunks of 256 MB, whose first chunks take longer to arrive.
     int chunk = n;
     if (e->hostChunk > 0) {
         chunk = std::min(n, e->hostChunk);
     } else if (n > 16384) {
-        const int cmax = (int)std::max<long long>(4096, (64LL << 20) / (4LL * npix));
+        const int cmax = (int)std::max<long long>(4096, (128LL << 20) / (4LL * npix));
         chunk = std::min(cmax, std::max(16384, (n + 7) / 8));
     }
     std::vector<std::pair<int, int>> chunks;  // (start, count)
@@ -455,10 +479,11 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
     }
     const int nchunks = (int)chunks.size();
     const int nslots = e->hostSlots;
+    const cudaStream_t cs = e->copy_stream();
+    std::vector<char> slotUsed(nslots, 0);
     struct Pending {
         int slot, start, count;
     };
-    std::vector<Pending> pend;
     auto d2h = [&](const Pending& p) {
         Slot& s = e->slot(p.slot);
         if (h_params && !fisherOnly)
@@ -487,23 +512,25 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
     };
     for (int c = 0; c < nchunks; c++) {
         const int start = chunks[c].first, count = chunks[c].second;
-        Slot& s = e->slot(c % nslots);
-        if (h_smp) {
-            s.smp.ensure(sizeof(float) * (size_t)npix * count);
+        const int k = c % nslots;
+        Slot& s = e->slot(k);
+        if (NC && !h_consts) throw Error("this estimator needs per-spot constants");
+        if (h_smp) s.smp.ensure(sizeof(float) * (size_t)npix * count);
+        if (NC) s.consts.ensure(sizeof(float) * NC * count);
+        if (h_initial) s.initial.ensure(sizeof(float) * K * count);
+        if (slotUsed[k]) PB_CUDA(cudaStreamWaitEvent(cs, s.freed, 0));
+        if (h_smp)
             PB_CUDA(cudaMemcpyAsync(s.smp.p, h_smp + (size_t)start * npix, sizeof(float) * (size_t)npix * count,
-                                    cudaMemcpyHostToDevice, s.stream));
-        }
-        if (NC) {
-            if (!h_consts) throw Error("this estimator needs per-spot constants");
-            s.consts.ensure(sizeof(float) * NC * count);
+                                    cudaMemcpyHostToDevice, cs));
+        if (NC)
             PB_CUDA(cudaMemcpyAsync(s.consts.p, h_consts + (size_t)start * NC, sizeof(float) * NC * count,
-                                    cudaMemcpyHostToDevice, s.stream));
-        }
-        if (h_initial) {
-            s.initial.ensure(sizeof(float) * K * count);
+                                    cudaMemcpyHostToDevice, cs));
+        if (h_initial)
             PB_CUDA(cudaMemcpyAsync(s.initial.p, h_initial + (size_t)start * K, sizeof(float) * K * count,
-                                    cudaMemcpyHostToDevice, s.stream));
-        }
+                                    cudaMemcpyHostToDevice, cs));
+        PB_CUDA(cudaEventRecord(s.copied, cs));
+        PB_CUDA(cudaStreamWaitEvent(s.stream, s.copied, 0));
+        slotUsed[k] = 1;
         s.params.ensure(sizeof(float) * K * count);
         if (h_iters) s.iters.ensure(sizeof(int) * count);
         if (h_trace && traceLen > 0) {
@@ -537,13 +564,10 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         }
         launch_fit_fisher(e, a, s.stream);
         if (h_crlb) launch_crlb(K, a.fisher, a.crlb, a.chisq, count, s.stream, e->crlbAbs);
-        pend.push_back({c % nslots, start, count});
-        if ((int)pend.size() == nslots) {
-            d2h(pend.front());
-            pend.erase(pend.begin());
-        }
+        PB_CUDA(cudaEventRecord(s.freed, s.stream));
+        d2h({k, start, count});
     }
-    for (auto& p : pend) d2h(p);
+    PB_CUDA(cudaStreamSynchronize(cs));
     for (int i = 0; i < Estimator::kMaxSlots; i++)
         if (e->slots[i].stream) PB_CUDA(cudaStreamSynchronize(e->slots[i].stream));
 }
