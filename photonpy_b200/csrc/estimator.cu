@@ -114,6 +114,18 @@ int num_sms() {
 
 void count_launch() { g_launches++; }
 
+// Streamed LM launcher (host calls whose ROIs arrive during the launch), or null.
+StreamLaunch stream_launcher_for(int model, int G, int CPL) {
+    switch (model) {
+    case MODEL_XYIBG: return stream_launcher_xyibg(G, CPL);
+    case MODEL_XYIBG_CONSTSIGMA: return stream_launcher_constsigma(G, CPL);
+    case MODEL_XYIBG_SIGMA: return stream_launcher_sigma(G, CPL);
+    case MODEL_XYIBG_SIGMAXY: return stream_launcher_sigmaxy(G, CPL);
+    case MODEL_XYZIBG: return stream_launcher_astig(G, CPL);
+    }
+    return nullptr;
+}
+
 FitLaunch fit_launcher_for(int model, int G, int CPL, int variant) {
     switch (model) {
     case MODEL_XYIBG: return fit_launcher_xyibg(G, CPL, variant);
@@ -264,6 +276,15 @@ struct Estimator {
     int hostSlots = 4;
     Slot slots[kMaxSlots];
     cudaStream_t copyStream = nullptr;  // the pipeline's host-to-device copies, in chunk order
+    // streamed host calls: buffers of a whole call, the ready flags and a pinned block of ones
+    // from which the copy stream sets them
+    DevBuf stSmp, stConsts, stInitial, stParams, stIters, stCrlb, stChisq, stFisher, stFlags, stClaim;
+    int* hostOnes = nullptr;
+    int hostOnesCount = 0;
+    // 0: not yet known; 1: the streamed path; -1: the slot pipeline (chosen after the first
+    // streamed call from how long its fits ran on after the last copy in)
+    int streamPref = 0;
+    cudaEvent_t stCopyStart = nullptr, stCopyEnd = nullptr, stLmEnd = nullptr;
 
     Estimator() { PB_CUDA(cudaGetDevice(&device)); }
     ~Estimator() {
@@ -273,6 +294,9 @@ struct Estimator {
             if (s.freed) cudaEventDestroy(s.freed);
         }
         if (copyStream) cudaStreamDestroy(copyStream);
+        if (hostOnes) cudaFreeHost(hostOnes);
+        for (cudaEvent_t ev : {stCopyStart, stCopyEnd, stLmEnd})
+            if (ev) cudaEventDestroy(ev);
     }
     int lanes_for() const { return lanes ? lanes : default_lanes(desc.model, desc.roisize); }
     // Lanes per ROI and columns per lane of the fit kernel this configuration launches (cpl 0:
@@ -444,11 +468,148 @@ void launch_fit_fisher(Estimator* e, const FitArgs& a, cudaStream_t s) { e->fit_
 // their inputs.
 // h_fisher (with FIT_CRLB_ONLY): the packed FP32 Fisher rows [n][K(K+1)/2 + 1] themselves are
 // copied out instead of (or besides) being inverted.
+// Largest call (bytes of samples) the streamed path takes; larger calls run through the slots.
+constexpr long long kStreamedMaxBytes = 4LL << 30;
+
+// Streamed host-pointer fit of the column-blocked Gaussian kernel: ONE LM launch for the whole
+// call, started before the ROIs have arrived. The copy stream copies the per-spot constants and
+// start values, then the samples in chunks (in order; after each chunk it sets the ready flag of
+// each of its 1024-ROI blocks from pinned host memory, a copy-engine write that needs no SM),
+// and the launch's groups wait for the block of each ROI they claim (wait_stream_ready, bounded).
+// So the fits run while the ROIs arrive without the end of a launch at every chunk, which in
+// the slot pipeline left the GPU mostly idle for about 0.18 ms per chunk. Then the Fisher
+// launch, the FP64 CRLB and the copies out. Same kernels and arguments per ROI as the other
+// paths: the results are identical.
+void host_fit_streamed(Estimator* e, StreamLaunch streamLaunch, int n, const float* h_smp, const float* h_consts,
+                       const float* h_initial, float* h_params, int* h_iters, float* h_crlb, float* h_chisq) {
+    const int K = e->K, NC = e->numconst, npix = e->npix();
+    const int nblocks = (n + (1 << kStreamBlockShift) - 1) >> kStreamBlockShift;
+    const cudaStream_t cs = e->copy_stream();
+    Slot& ks = e->slot(0);
+    e->stSmp.ensure(sizeof(float) * (size_t)npix * n);
+    if (NC) e->stConsts.ensure(sizeof(float) * (size_t)NC * n);
+    if (h_initial) e->stInitial.ensure(sizeof(float) * (size_t)K * n);
+    e->stParams.ensure(sizeof(float) * (size_t)K * n);
+    if (h_iters) e->stIters.ensure(sizeof(int) * (size_t)n);
+    if (h_crlb) {
+        e->stCrlb.ensure(sizeof(float) * (size_t)K * n);
+        e->stFisher.ensure(sizeof(float) * (size_t)fisher_row_floats(K) * n);
+    }
+    if (h_crlb || h_chisq) e->stChisq.ensure(sizeof(float) * (size_t)n);
+    e->stFlags.ensure(sizeof(int) * (size_t)(1 + nblocks));
+    e->stClaim.ensure(sizeof(int));
+    // chunks of at most 32 MB of samples, whole 1024-ROI blocks; the first three at 1/8, 1/4
+    // and 1/2 size so that the fits start early
+    const int blk = 1 << kStreamBlockShift;
+    int chunk = (int)std::max<long long>(8 * blk, ((32LL << 20) / (4LL * npix)) / (8 * blk) * (8 * blk));
+    std::vector<std::pair<int, int>> chunks;
+    for (int start = 0, k = 0; start < n; k++) {
+        int c = k < 3 ? chunk >> (3 - k) : chunk;
+        c = std::min(c, n - start);
+        chunks.push_back({start, c});
+        start += c;
+    }
+    const int onesNeeded = chunk / blk + 1;
+    if (e->hostOnesCount < onesNeeded) {
+        if (e->hostOnes) PB_CUDA(cudaFreeHost(e->hostOnes));
+        e->hostOnes = nullptr;
+        e->hostOnesCount = 0;
+        PB_CUDA(cudaMallocHost(&e->hostOnes, sizeof(int) * onesNeeded));
+        for (int i = 0; i < onesNeeded; i++) e->hostOnes[i] = 1;
+        e->hostOnesCount = onesNeeded;
+    }
+    int* d_flags = e->stFlags.as<int>();
+    // the flags cleared and the small inputs in place before the launch starts
+    PB_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * (size_t)(1 + nblocks), cs));
+    if (NC)
+        PB_CUDA(cudaMemcpyAsync(e->stConsts.p, h_consts, sizeof(float) * (size_t)NC * n, cudaMemcpyHostToDevice, cs));
+    if (h_initial)
+        PB_CUDA(cudaMemcpyAsync(e->stInitial.p, h_initial, sizeof(float) * (size_t)K * n, cudaMemcpyHostToDevice, cs));
+    PB_CUDA(cudaEventRecord(ks.copied, cs));
+    PB_CUDA(cudaStreamWaitEvent(ks.stream, ks.copied, 0));
+    FitArgs a{};
+    a.smp = e->stSmp.as<float>();
+    a.consts = NC ? e->stConsts.as<float>() : nullptr;
+    a.initial = h_initial ? e->stInitial.as<float>() : nullptr;
+    a.params = e->stParams.as<float>();
+    a.iterations = h_iters ? e->stIters.as<int>() : nullptr;
+    a.crlb = h_crlb ? e->stCrlb.as<float>() : nullptr;
+    a.chisq = (h_crlb || h_chisq) ? e->stChisq.as<float>() : nullptr;
+    a.fisher = h_crlb ? e->stFisher.as<float>() : nullptr;
+    a.n = n;
+    a.maxIter = e->lm.iterations;
+    a.lambda = e->lm.lambda;
+    a.claim = e->stClaim.as<int>();
+    const FitLaunch launch = e->fit_launch();
+    const int threads = e->threads_for();
+    const bool measure = e->streamPref == 0;
+    if (measure && !e->stCopyStart) {
+        PB_CUDA(cudaEventCreate(&e->stCopyStart));
+        PB_CUDA(cudaEventCreate(&e->stCopyEnd));
+        PB_CUDA(cudaEventCreate(&e->stLmEnd));
+    }
+    streamLaunch(e->desc, a, d_flags, threads, ks.stream);  // LM only (no Fisher outputs)
+    if (measure) {
+        PB_CUDA(cudaEventRecord(e->stLmEnd, ks.stream));
+        PB_CUDA(cudaEventRecord(e->stCopyStart, cs));
+    }
+    for (const auto& ch : chunks) {
+        const int start = ch.first, count = ch.second;
+        PB_CUDA(cudaMemcpyAsync(e->stSmp.as<float>() + (size_t)start * npix, h_smp + (size_t)start * npix,
+                                sizeof(float) * (size_t)npix * count, cudaMemcpyHostToDevice, cs));
+        const int b0 = start >> kStreamBlockShift, b1 = (start + count + blk - 1) >> kStreamBlockShift;
+        PB_CUDA(cudaMemcpyAsync(d_flags + 1 + b0, e->hostOnes, sizeof(int) * (size_t)(b1 - b0),
+                                cudaMemcpyHostToDevice, cs));
+    }
+    PB_CUDA(cudaEventRecord(ks.freed, cs));
+    if (measure) PB_CUDA(cudaEventRecord(e->stCopyEnd, cs));
+    PB_CUDA(cudaStreamWaitEvent(ks.stream, ks.freed, 0));  // every ROI in place for the Fisher pass
+    if (h_crlb) {
+        launch(e->desc, fisher_pass_args(a), threads, ks.stream);
+        launch_crlb(K, a.fisher, a.crlb, a.chisq, n, ks.stream, e->crlbAbs);
+    }
+    if (h_params)
+        PB_CUDA(cudaMemcpyAsync(h_params, a.params, sizeof(float) * (size_t)K * n, cudaMemcpyDeviceToHost, ks.stream));
+    if (h_iters)
+        PB_CUDA(cudaMemcpyAsync(h_iters, a.iterations, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ks.stream));
+    if (h_crlb)
+        PB_CUDA(cudaMemcpyAsync(h_crlb, a.crlb, sizeof(float) * (size_t)K * n, cudaMemcpyDeviceToHost, ks.stream));
+    if (h_chisq)
+        PB_CUDA(cudaMemcpyAsync(h_chisq, a.chisq, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, ks.stream));
+    PB_CUDA(cudaStreamSynchronize(cs));
+    PB_CUDA(cudaStreamSynchronize(ks.stream));
+    int err = 0;
+    PB_CUDA(cudaMemcpy(&err, d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) throw Error("streamed fit: ROIs did not arrive in device memory in time");
+    if (measure) {
+        // Fits that end soon after the last ROIs arrived were waiting for the copies: then the
+        // slot pipeline, which also overlaps the copies out, is faster (1M ROIs end to end: XYIBg
+        // 10x10 7.6 against 8.7 ms, astig 12x12 11.5 against 12.9 ms); fits that run on for
+        // longer gain from the single launch (SigmaXY 16x16 24.3 against 26.1 ms).
+        float copyMs = 0.0f, tailMs = 0.0f;
+        PB_CUDA(cudaEventElapsedTime(&copyMs, e->stCopyStart, e->stCopyEnd));
+        PB_CUDA(cudaEventElapsedTime(&tailMs, e->stCopyEnd, e->stLmEnd));
+        e->streamPref = tailMs > 0.1f * copyMs ? 1 : -1;
+    }
+}
+
 void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, const float* h_initial,
               float* h_params, int* h_iters, float* h_trace, int traceLen, float* h_crlb, float* h_chisq,
               int flags, float* h_glrt = nullptr, float* h_fisher = nullptr) {
     std::lock_guard<std::mutex> g(e->mtx);
     PB_CUDA(cudaSetDevice(e->device));
+    {
+        int G = 0, cpl = 0;
+        e->fit_shape(G, cpl);
+        const bool plain = (flags & FIT_CRLB_ONLY) == 0 && !(h_trace && traceLen > 0) && !h_glrt && !h_fisher;
+        const StreamLaunch sl = cpl > 0 ? stream_launcher_for(e->desc.model, G, cpl) : nullptr;
+        if (sl && plain && h_smp && e->hostChunk == 0 && e->streamPref >= 0 && n > 16384 &&
+            4LL * e->npix() * n <= kStreamedMaxBytes) {
+            if (e->numconst && !h_consts) throw Error("this estimator needs per-spot constants");
+            host_fit_streamed(e, sl, n, h_smp, h_consts, h_initial, h_params, h_iters, h_crlb, h_chisq);
+            return;
+        }
+    }
     const int K = e->K, NC = e->numconst, npix = e->npix();
     const bool fisherOnly = (flags & FIT_CRLB_ONLY) != 0;
     const bool wantGlrt = h_glrt && e->glrt && !fisherOnly;
@@ -456,18 +617,19 @@ void host_fit(Estimator* e, int n, const float* h_smp, const float* h_consts, co
         e->glrtRoi0.ensure(sizeof(float) * npix);
         PB_CUDA(cudaMemcpy(e->glrtRoi0.p, h_smp, sizeof(float) * npix, cudaMemcpyHostToDevice));
     }
-    // Chunks of at most 128 MB of samples (at least 16384 ROIs, an eighth of the call when that is
-    // smaller); the first three are 1/8, 1/4 and 1/2 of that, so the first fit starts early. Every
-    // chunk boundary costs the end of a fit launch, whose last ROIs leave most of the GPU idle
-    // (about 0.18 ms for 16x16 SigmaXY ROIs, even with the next chunk's launch on another
-    // stream): 1M such ROIs took 26.1 ms end to end in chunks of 64 MB, 25.5 ms in chunks of
-    // 128 MB, 26.9 ms in chunks of 256 MB, whose first chunks take longer to arrive.
+    // Chunks of at most 64 MB of samples (at least 16384 ROIs, a sixteenth of the call when that
+    // is smaller); the first three are 1/8, 1/4 and 1/2 of that, so the first fit starts early.
+    // Every chunk boundary costs the end of a fit launch, whose last ROIs leave most of the GPU
+    // idle (about 0.18 ms for 16x16 SigmaXY ROIs, even with the next chunk's launch on another
+    // stream); calls whose copies are slower than their fits (which is when this path runs, see
+    // host_fit_streamed) gain from the smaller chunks: 1M ROIs end to end, chunks of 65536 / 131072
+    // ROIs: XYIBg 10x10 7.60 / 7.79 ms, astig 12x12 11.5 / 11.9 ms.
     int chunk = n;
     if (e->hostChunk > 0) {
         chunk = std::min(n, e->hostChunk);
     } else if (n > 16384) {
-        const int cmax = (int)std::max<long long>(4096, (128LL << 20) / (4LL * npix));
-        chunk = std::min(cmax, std::max(16384, (n + 7) / 8));
+        const int cmax = (int)std::max<long long>(4096, (64LL << 20) / (4LL * npix));
+        chunk = std::min(cmax, std::max(16384, (n + 15) / 16));
     }
     std::vector<std::pair<int, int>> chunks;  // (start, count)
     for (int start = 0, k = 0; start < n; k++) {

@@ -92,6 +92,28 @@ __device__ __forceinline__ float group_sum(float v, unsigned mask) {
     return v;
 }
 
+// Streamed input of a fit launch that starts before all of its ROIs have arrived: a copy engine
+// writes the ROIs of block b (1 << kStreamBlockShift ROIs), then sets flags[1 + b]; flags[0] is
+// the error flag. Waits for the block of `roi` with acquire loads and growing sleeps; gives up
+// after about 4 s of polling (or at once when another group already has), sets the error flag
+// and returns false.
+constexpr int kStreamBlockShift = 10;
+__device__ __forceinline__ bool wait_stream_ready(int* flags, int roi) {
+    const int* f = flags + 1 + (roi >> kStreamBlockShift);
+    unsigned ns = 32;
+    for (int i = 0; i < (1 << 22); i++) {
+        int v, err;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+        if (v) return true;
+        asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(err) : "l"(flags) : "memory");
+        if (err) return false;
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+    atomicExch(flags, 1);
+    return false;
+}
+
 // First of `count` ROIs taken from a launch's counter by a group of G lanes (lane 0 takes them).
 template <int G>
 __device__ __forceinline__ int group_claim(int* counter, int count, int lane, unsigned mask) {

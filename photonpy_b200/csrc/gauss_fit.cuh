@@ -188,15 +188,22 @@ __device__ __forceinline__ void map_virtual(const float (&av)[NV], float (&acc)[
 // lanes (`lane`, `mask`) and its shared-memory area `spix` (gauss_group_base_floats floats). With
 // `claim` set, the group instead takes its ROIs, the first included, from that counter, roiStep
 // consecutive ROIs per atomicAdd of the group's first lane, so groups refill from a shared pool
-// until it runs out.
-template <class M, int G, int CPL, int PASS = PASS_BOTH>
+// until it runs out. STREAM: the ROIs are still arriving (streamFlags, see wait_stream_ready);
+// a group waits for each claimed ROI and reads its samples from L2.
+template <class M, int G, int CPL, int PASS = PASS_BOTH, bool STREAM = false>
 __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArgs& a, int roi, const int roiEnd,
                                                 const int roiStep, float* spix, const int lane, const unsigned mask,
-                                                int* claim = nullptr) {
+                                                int* claim = nullptr, int* streamFlags = nullptr) {
     int claimEnd = 0;
     auto claim_next = [&]() -> int {
         int r = 0;
-        if (lane == 0) r = atomicAdd(claim, roiStep);
+        if (lane == 0) {
+            r = atomicAdd(claim, roiStep);
+            if constexpr (STREAM) {
+                // a group that gives up waiting ends; the host reads the error flag
+                if (r < roiEnd && !wait_stream_ready(streamFlags, min(r + roiStep, roiEnd) - 1)) r = roiEnd;
+            }
+        }
         r = __shfl_sync(mask, r, 0, G);
         claimEnd = r + roiStep;
         return r;
@@ -237,9 +244,9 @@ __device__ __forceinline__ void gauss_fit_range(const ModelDesc& d, const FitArg
                 if (vec4) {
                     const float4* s4 = reinterpret_cast<const float4*>(src);
                     float4* d4 = reinterpret_cast<float4*>(spix);
-                    for (int i = lane; i < (npix >> 2); i += G) d4[i] = __ldcs(s4 + i);
+                    for (int i = lane; i < (npix >> 2); i += G) d4[i] = STREAM ? __ldcg(s4 + i) : __ldcs(s4 + i);
                 } else {
-                    for (int i = lane; i < npix; i += G) spix[i] = __ldcs(src + i);
+                    for (int i = lane; i < npix; i += G) spix[i] = STREAM ? __ldcg(src + i) : __ldcs(src + i);
                 }
             }
 #pragma unroll
@@ -452,6 +459,18 @@ __global__ void __launch_bounds__(256) gauss_fit_kernel(const ModelDesc d, const
     int* claim = PASS == PASS_LM ? a.claim : nullptr;
     gauss_fit_range<M, G, CPL, PASS>(d, a, claim ? 0 : blockIdx.x * gpb + gib, a.n, claim ? 1 : gridDim.x * gpb,
                                      sm + gib * a.smemStride, lane, group_mask<G>(), claim);
+}
+
+// LM launch over ROIs that a copy engine is still bringing in (host calls, see host_fit_streamed
+// in estimator.cu): flags[1 + b] is set once ROI block b has arrived, flags[0] reports a wait
+// that ran out. Groups take ROIs from the counter a.claim as in gauss_fit_kernel.
+template <class M, int G, int CPL>
+__global__ void __launch_bounds__(256) gauss_fit_stream_kernel(const ModelDesc d, const FitArgs a, int* flags) {
+    extern __shared__ __align__(16) float sm[];
+    const int lane = threadIdx.x & (G - 1);
+    const int gib = threadIdx.x / G;
+    gauss_fit_range<M, G, CPL, PASS_LM, true>(d, a, 0, a.n, 1, sm + gib * a.smemStride, lane, group_mask<G>(), a.claim,
+                                              flags);
 }
 
 }  // namespace pb200

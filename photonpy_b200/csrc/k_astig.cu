@@ -8,6 +8,8 @@ FitLaunch fit_launcher_astig(int G, int CPL, int variant) {
     return generic_fit_table<GaussModel<MODEL_XYZIBG>>(G);
 }
 
+StreamLaunch stream_launcher_astig(int G, int CPL) { return gauss_stream_table<GaussModel<MODEL_XYZIBG>>(G, CPL); }
+
 EvalLaunch eval_launcher_astig(int G) { return eval_table<GaussModel<MODEL_XYZIBG>>(G); }
 
 AdjointLaunch adjoint_launcher_astig() { return launch_adjoint<GaussModel<MODEL_XYZIBG>, 8>; }

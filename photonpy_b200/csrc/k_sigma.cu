@@ -8,6 +8,8 @@ FitLaunch fit_launcher_sigma(int G, int CPL, int variant) {
     return generic_fit_table<GaussModel<MODEL_XYIBG_SIGMA>>(G);
 }
 
+StreamLaunch stream_launcher_sigma(int G, int CPL) { return gauss_stream_table<GaussModel<MODEL_XYIBG_SIGMA>>(G, CPL); }
+
 EvalLaunch eval_launcher_sigma(int G) { return eval_table<GaussModel<MODEL_XYIBG_SIGMA>>(G); }
 
 AdjointLaunch adjoint_launcher_sigma() { return launch_adjoint<GaussModel<MODEL_XYIBG_SIGMA>, 8>; }

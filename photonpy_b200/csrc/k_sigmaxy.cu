@@ -8,6 +8,8 @@ FitLaunch fit_launcher_sigmaxy(int G, int CPL, int variant) {
     return generic_fit_table<GaussModel<MODEL_XYIBG_SIGMAXY>>(G);
 }
 
+StreamLaunch stream_launcher_sigmaxy(int G, int CPL) { return gauss_stream_table<GaussModel<MODEL_XYIBG_SIGMAXY>>(G, CPL); }
+
 EvalLaunch eval_launcher_sigmaxy(int G) { return eval_table<GaussModel<MODEL_XYIBG_SIGMAXY>>(G); }
 
 AdjointLaunch adjoint_launcher_sigmaxy() { return launch_adjoint<GaussModel<MODEL_XYIBG_SIGMAXY>, 8>; }

@@ -6,6 +6,8 @@ namespace pb200 {
 
 FitLaunch fit_launcher_spline(int G, int, int) { return spline_fit_table<0>(G); }
 
+StreamLaunch stream_launcher_spline(int, int) { return nullptr; }  // spline host calls use the slot pipeline
+
 EvalLaunch eval_launcher_spline(int G) { return spline_eval_table<0>(G); }
 
 static void launch_adjoint_spline(const ModelDesc& d, AdjointArgs a, cudaStream_t s) {

@@ -19,6 +19,8 @@
 namespace pb200 {
 
 using FitLaunch = void (*)(const ModelDesc&, FitArgs, int threads, cudaStream_t);
+// LM launch over ROIs still arriving (gauss_fit_stream_kernel): FitArgs with a.claim set, the ready flags
+using StreamLaunch = void (*)(const ModelDesc&, FitArgs, int* flags, int threads, cudaStream_t);
 using AdjointLaunch = void (*)(const ModelDesc&, AdjointArgs, cudaStream_t);
 using EvalLaunch = void (*)(const ModelDesc&, const float*, const float*, float*, float*, int, int threads,
                             cudaStream_t);
@@ -58,9 +60,9 @@ inline int launched_threads(int threads, int G, int strideFloats) {
 }
 
 // Launch a persistent group kernel: `strideFloats` of shared memory per group of G lanes.
-template <class KernelT>
+template <class KernelT, class... Extra>
 inline void launch_groups(KernelT kern, int G, int threads, int strideFloats, int n, const ModelDesc& d, FitArgs a,
-                          cudaStream_t s) {
+                          cudaStream_t s, Extra... extra) {
     threads = launched_threads(threads, G, strideFloats);
     const int gpb = threads / G;
     const size_t smem = (size_t)gpb * strideFloats * sizeof(float);
@@ -73,7 +75,7 @@ inline void launch_groups(KernelT kern, int G, int threads, int strideFloats, in
     const long long cap = (long long)num_sms() * perSM;
     const int grid = (int)(needed < cap ? needed : cap);
     a.smemStride = strideFloats;
-    kern<<<grid, threads, smem, s>>>(d, a);
+    kern<<<grid, threads, smem, s>>>(d, a, extra...);
     check_launch("fit kernel launch");
     count_launch();
 }
@@ -264,6 +266,38 @@ FitLaunch gauss_fit_table(int G, int CPL) {
 #undef PB_CASE
 }
 
+template <class M, int G, int CPL>
+void launch_fit_gauss_stream(const ModelDesc& d, FitArgs a, int* flags, int threads, cudaStream_t s) {
+    if (a.n <= 0 || !a.claim) return;
+    const int stride = gauss_group_stride<M::K>(d.roisize, G, CPL);
+    reset_claim(a.claim, s);
+    launch_groups(gauss_fit_stream_kernel<M, G, CPL>, G, threads, stride, a.n, d, lm_pass_args(a), s, flags);
+}
+
+// Streamed LM launchers of the 2- and 4-lane shapes (the default configurations up to 16 px);
+// null for the others, whose host calls use the slot pipeline.
+template <class M>
+StreamLaunch gauss_stream_table(int G, int CPL) {
+    if (G == 2) {
+        switch (CPL) {
+        case 1: return launch_fit_gauss_stream<M, 2, 1>;
+        case 2: return launch_fit_gauss_stream<M, 2, 2>;
+        case 3: return launch_fit_gauss_stream<M, 2, 3>;
+        case 4: return launch_fit_gauss_stream<M, 2, 4>;
+        default: return launch_fit_gauss_stream<M, 2, 5>;
+        }
+    }
+    if (G == 4) {
+        switch (CPL) {
+        case 1: return launch_fit_gauss_stream<M, 4, 1>;
+        case 2: return launch_fit_gauss_stream<M, 4, 2>;
+        case 3: return launch_fit_gauss_stream<M, 4, 3>;
+        default: return launch_fit_gauss_stream<M, 4, 4>;
+        }
+    }
+    return nullptr;
+}
+
 template <class M>
 FitLaunch generic_fit_table(int G) {
     switch (G) {
@@ -356,6 +390,7 @@ EvalLaunch eval_launcher_for(int model, int G);
 
 #define PB_DECLARE_MODEL_LAUNCHERS(name)                               \
     FitLaunch fit_launcher_##name(int G, int CPL, int variant);        \
+    StreamLaunch stream_launcher_##name(int G, int CPL);               \
     EvalLaunch eval_launcher_##name(int G);                            \
     AdjointLaunch adjoint_launcher_##name();
 PB_DECLARE_MODEL_LAUNCHERS(xyibg)
