@@ -335,8 +335,11 @@ const char* PB200_GetLastError(void);
 void PB200_ClearError(void);
 /* Localization in one call: LM fit, Fisher/CRLB + chi-square at the fitted parameters (what
  * photonpy's EstimationQueue runs as Estimate followed by ChiSquareAndCRLB,
- * EstimationQueue.cpp:285-289), as three launches per chunk (LM, Fisher pass, FP64 inverse) on
- * one stream. Host pointers; large batches are pipelined in chunks over four CUDA streams. */
+ * EstimationQueue.cpp:285-289): LM launch, Fisher pass, FP64 inverse. Host pointers; large
+ * batches of the flat-background Gaussian models at their default configuration are fitted by
+ * one LM launch while a copy stream brings the ROIs in (when the fits outlast the copies,
+ * which each estimator's first large call measures), others in chunks pipelined over four
+ * CUDA streams. */
 void PB200_EstimateCRLB(Estimator* e, int numspots, const float* sample, const float* constants,
                         const float* initial, float* params, int* iterations, float* crlb, float* chisq);
 /* Device-pointer variants on a caller stream (cudaStream_t as void*; NULL = legacy default).
@@ -447,8 +450,10 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
  * Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
 /* Extension: the host-pointer pipeline of the Estimate/CRLB calls. The ROIs are fitted in chunks of
- * roisPerChunk (0: automatic), with `slots` chunks (2..8) in flight: while one chunk is fitted
- * the next ones are copied in and the previous ones copied out. Returns 0 or -1. */
+ * roisPerChunk (0: automatic, which also lets large calls of the flat-background Gaussian models
+ * run the streamed path, one fit launch while the ROIs arrive), with `slots` chunks (2..8) in
+ * flight: while one chunk is fitted the next ones are copied in and the previous ones copied
+ * out. Returns 0 or -1. */
 int PB200_SetHostPipeline(Estimator* e, int roisPerChunk, int slots);
 /* Lanes per ROI and threads per block the fit kernel of this estimator launches with (for large
  * ROIs the block is smaller than the configured threads per block, so that its groups' shared

@@ -341,7 +341,8 @@ class Estimator:
 
     def SetHostPipeline(self, rois_per_chunk=0, slots=4):
         """Chunking of the host-array calls (Estimate, EstimateWithCRLB, ...): ROIs per chunk
-        (0 = automatic: up to 128 MB of samples, ramped up over the first three chunks) and the
+        (0 = automatic: up to 64 MB of samples, ramped up over the first three chunks, and the
+        streamed path where it is faster; an explicit size always takes the chunked path) and the
         number of chunks in flight (2..8), whose copies overlap the fits of the others."""
         if self._lib.PB200_SetHostPipeline(self.inst, int(rois_per_chunk), int(slots)) != 0:
             raise ValueError("invalid host pipeline configuration")
