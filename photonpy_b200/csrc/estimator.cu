@@ -563,15 +563,19 @@ void host_fit_streamed(Estimator* e, StreamLaunch streamLaunch, int n, const flo
     }
     PB_CUDA(cudaEventRecord(ks.freed, cs));
     if (measure) PB_CUDA(cudaEventRecord(e->stCopyEnd, cs));
+    // the parameters and iteration counts go out on the copy stream while the Fisher and CRLB
+    // launches run
+    PB_CUDA(cudaEventRecord(ks.copied, ks.stream));
+    PB_CUDA(cudaStreamWaitEvent(cs, ks.copied, 0));
+    if (h_params)
+        PB_CUDA(cudaMemcpyAsync(h_params, a.params, sizeof(float) * (size_t)K * n, cudaMemcpyDeviceToHost, cs));
+    if (h_iters)
+        PB_CUDA(cudaMemcpyAsync(h_iters, a.iterations, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, cs));
     PB_CUDA(cudaStreamWaitEvent(ks.stream, ks.freed, 0));  // every ROI in place for the Fisher pass
     if (h_crlb) {
         launch(e->desc, fisher_pass_args(a), threads, ks.stream);
         launch_crlb(K, a.fisher, a.crlb, a.chisq, n, ks.stream, e->crlbAbs);
     }
-    if (h_params)
-        PB_CUDA(cudaMemcpyAsync(h_params, a.params, sizeof(float) * (size_t)K * n, cudaMemcpyDeviceToHost, ks.stream));
-    if (h_iters)
-        PB_CUDA(cudaMemcpyAsync(h_iters, a.iterations, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ks.stream));
     if (h_crlb)
         PB_CUDA(cudaMemcpyAsync(h_crlb, a.crlb, sizeof(float) * (size_t)K * n, cudaMemcpyDeviceToHost, ks.stream));
     if (h_chisq)
