@@ -449,6 +449,14 @@ int PB200_EstimateCRLBNoAlloc(Estimator* e, int numspots, const float* d_sample,
  * supported count is used) and threads per block (64..256, a multiple of 32; 0 = automatic).
  * Returns 0 on success. */
 int PB200_SetKernelConfig(Estimator* e, int lanesPerRoi, int threadsPerBlock);
+/* No counterpart in the reference; diagnostic. Runs the streamed LM launch (the one that host
+ * calls use while their ROIs are still being copied in) on device-resident ROIs: with markReady
+ * = 1 every ROI block is marked as arrived beforehand, and the results equal PB200_EstimateDevice's;
+ * with markReady = 0 none is, so every wait runs out (after about 1-2 s) and the launch ends.
+ * Returns 0 (no wait ran out), 1 (a wait ran out; the context stays usable) or -1 on a bad
+ * argument. Column-blocked Gaussian estimators without per-spot constants at 2 or 4 lanes per ROI. */
+int PB200_StreamedFitProbe(Estimator* e, int numspots, const float* d_sample, float* d_params, int* d_iterations,
+                           int markReady);
 /* Extension: the host-pointer pipeline of the Estimate/CRLB calls. The ROIs are fitted in chunks of
  * roisPerChunk (0: automatic, which also lets large calls of the flat-background Gaussian models
  * run the streamed path, one fit launch while the ROIs arrive), with `slots` chunks (2..8) in

@@ -475,17 +475,37 @@ constexpr long long kStreamedMaxBytes = 4LL << 30;
 // call, started before the ROIs have arrived. The copy stream copies the per-spot constants and
 // start values, then the samples in chunks (in order; after each chunk it sets the ready flag of
 // each of its 1024-ROI blocks from pinned host memory, a copy-engine write that needs no SM),
-// and the launch's groups wait for the block of each ROI they claim (wait_stream_ready, bounded).
+// and the launch's groups wait for the block of each ROI they claim (wait_stream_ready, bounded
+// to 1-2 s, after which the call reports an error).
 // So the fits run while the ROIs arrive without the end of a launch at every chunk, which in
 // the slot pipeline left the GPU mostly idle for about 0.18 ms per chunk. Then the Fisher
 // launch, the FP64 CRLB and the copies out. Same kernels and arguments per ROI as the other
 // paths: the results are identical.
+void host_fit_streamed_body(Estimator* e, StreamLaunch streamLaunch, int n, const float* h_smp,
+                            const float* h_consts, const float* h_initial, float* h_params, int* h_iters,
+                            float* h_crlb, float* h_chisq, cudaStream_t cs, Slot& ks);
+
 void host_fit_streamed(Estimator* e, StreamLaunch streamLaunch, int n, const float* h_smp, const float* h_consts,
                        const float* h_initial, float* h_params, int* h_iters, float* h_crlb, float* h_chisq) {
-    const int K = e->K, NC = e->numconst, npix = e->npix();
-    const int nblocks = (n + (1 << kStreamBlockShift) - 1) >> kStreamBlockShift;
     const cudaStream_t cs = e->copy_stream();
     Slot& ks = e->slot(0);
+    try {
+        host_fit_streamed_body(e, streamLaunch, n, h_smp, h_consts, h_initial, h_params, h_iters, h_crlb, h_chisq, cs,
+                               ks);
+    } catch (...) {
+        // a launch that is still waiting for ROIs ends by its bounded wait; let it end before the
+        // buffers and flags are used again
+        cudaStreamSynchronize(cs);
+        cudaStreamSynchronize(ks.stream);
+        throw;
+    }
+}
+
+void host_fit_streamed_body(Estimator* e, StreamLaunch streamLaunch, int n, const float* h_smp,
+                            const float* h_consts, const float* h_initial, float* h_params, int* h_iters,
+                            float* h_crlb, float* h_chisq, cudaStream_t cs, Slot& ks) {
+    const int K = e->K, NC = e->numconst, npix = e->npix();
+    const int nblocks = (n + (1 << kStreamBlockShift) - 1) >> kStreamBlockShift;
     e->stSmp.ensure(sizeof(float) * (size_t)npix * n);
     if (NC) e->stConsts.ensure(sizeof(float) * (size_t)NC * n);
     if (h_initial) e->stInitial.ensure(sizeof(float) * (size_t)K * n);
@@ -1878,6 +1898,42 @@ int PB200_MixedPlanLanes(MixedPlan* p, int nbuckets, int* lanes) {
 
 void PB200_SetMixedStandaloneMin(int roisPerSM) { g_aloneMinRoisPerSM.store(roisPerSM < 0 ? 0 : roisPerSM); }
 int PB200_GetMixedStandaloneMin(void) { return g_aloneMinRoisPerSM.load(); }
+
+int PB200_StreamedFitProbe(Estimator* e, int numspots, const float* d_sample, float* d_params, int* d_iterations,
+                           int markReady) {
+    return guarded(
+        [&]() -> int {
+            check_estimator(e);
+            if (numspots <= 0 || !d_sample || !d_params) throw Error("StreamedFitProbe: bad arguments");
+            int G = 0, cpl = 0;
+            e->fit_shape(G, cpl);
+            const StreamLaunch sl = cpl > 0 ? stream_launcher_for(e->desc.model, G, cpl) : nullptr;
+            if (!sl) throw Error("StreamedFitProbe: no streamed kernel for this estimator's configuration");
+            if (e->numconst) throw Error("StreamedFitProbe: estimators with per-spot constants are not supported");
+            std::lock_guard<std::mutex> g(e->mtx);
+            const int nblocks = (numspots + (1 << kStreamBlockShift) - 1) >> kStreamBlockShift;
+            Slot& ks = e->slot(0);
+            e->stFlags.ensure(sizeof(int) * (size_t)(1 + nblocks));
+            e->stClaim.ensure(sizeof(int));
+            int* flags = e->stFlags.as<int>();
+            PB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), ks.stream));
+            PB_CUDA(cudaMemsetAsync(flags + 1, markReady ? 1 : 0, sizeof(int) * (size_t)nblocks, ks.stream));
+            FitArgs a{};
+            a.smp = d_sample;
+            a.params = d_params;
+            a.iterations = d_iterations;
+            a.n = numspots;
+            a.maxIter = e->lm.iterations;
+            a.lambda = e->lm.lambda;
+            a.claim = e->stClaim.as<int>();
+            sl(e->desc, a, flags, e->threads_for(), ks.stream);
+            PB_CUDA(cudaStreamSynchronize(ks.stream));
+            int err = 0;
+            PB_CUDA(cudaMemcpy(&err, flags, sizeof(int), cudaMemcpyDeviceToHost));
+            return err ? 1 : 0;
+        },
+        -1);
+}
 
 int PB200_MixedPlanStandalone(MixedPlan* p, int nbuckets, int* standalone) {
     if (!p || !standalone || nbuckets != (int)p->bucketAlone.size()) return -1;

@@ -95,13 +95,13 @@ __device__ __forceinline__ float group_sum(float v, unsigned mask) {
 // Streamed input of a fit launch that starts before all of its ROIs have arrived: a copy engine
 // writes the ROIs of block b (1 << kStreamBlockShift ROIs), then sets flags[1 + b]; flags[0] is
 // the error flag. Waits for the block of `roi` with acquire loads and growing sleeps; gives up
-// after about 4 s of polling (or at once when another group already has), sets the error flag
-// and returns false.
+// after about 1-2 s of polling (2^20 polls; a chunk's copy takes milliseconds), or at once when
+// another group already has, sets the error flag and returns false.
 constexpr int kStreamBlockShift = 10;
 __device__ __forceinline__ bool wait_stream_ready(int* flags, int roi) {
     const int* f = flags + 1 + (roi >> kStreamBlockShift);
     unsigned ns = 32;
-    for (int i = 0; i < (1 << 22); i++) {
+    for (int i = 0; i < (1 << 20); i++) {
         int v, err;
         asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
         if (v) return true;
