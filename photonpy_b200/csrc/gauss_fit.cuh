@@ -10,7 +10,8 @@
 //
 // The loop is flat: one trip = one LM iteration (or the Fisher pass) of every group in the
 // warp; a group whose ROI has finished loads the next one at the top of the next trip, so
-// groups never wait for their warp-mates to converge. ROIs are assigned statically:
+// groups never wait for their warp-mates to converge. The LM launches take ROIs one at a time
+// from a per-launch counter (FitArgs::claim); the Fisher launches assign them statically:
 // group g processes ROIs g, g + total_groups, ...
 //
 // Semantics follow photonpy's LevMarOptimize (Estimators/Estimation.h:104-134, 194-251);

@@ -1,4 +1,4 @@
-"""Mixed batches: several (model, ROI size) buckets fitted in persistent launches.
+"""Mixed batches: several (model, ROI size) buckets fitted in one run (a CUDA-graph replay).
 
 photonpy fits one estimator — one model and one ROI size — per call (its EstimationQueue
 holds one estimator per queue, EstimationQueue.h:27-108). A ``MixedBatch`` binds several
